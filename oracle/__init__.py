@@ -1,0 +1,203 @@
+"""Oracle loader (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this
+package.  It binds two CPU implementations of the reference's propagation:
+
+* ``port``      -- oracle/fwi2d_oracle.c, the C restatement (liborc32/64.so);
+* ``reference`` -- the reference's own sources compiled by oracle/build_ref.sh
+                   (oracle/_ref/libfwi2d_ref32/64.so), present only where the
+                   reference tree was available at build time.
+
+Both take the same parameter struct (``Par``) and model/trace layouts as the
+reference's ``propagate`` (src/cpp/we_op.cpp:564): model ``[npar][nx][nz]``
+already converted, sources ``[ncomp][ns][nt]``, receivers ``[ncomp][nr][nt]``,
+snapshots ``[nt/sub+1][ncomp][nx][nz]``, gradient ``[3][nx][nz]``.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+KIND_ELASTIC, KIND_VTI, KIND_ACOUSTIC, KIND_AE = 0, 1, 2, 3
+
+
+class Par(ctypes.Structure):
+    _fields_ = [
+        ("nt", ctypes.c_int), ("sub", ctypes.c_int), ("dt", ctypes.c_double),
+        ("ns", ctypes.c_int), ("nr", ctypes.c_int),
+        ("bc_top", ctypes.c_int), ("bc_bottom", ctypes.c_int), ("bc_left", ctypes.c_int), ("bc_right", ctypes.c_int),
+        ("taper_top", ctypes.c_int), ("taper_bottom", ctypes.c_int), ("taper_left", ctypes.c_int), ("taper_right", ctypes.c_int),
+        ("taper_strength", ctypes.c_double), ("free_surface_stiffness", ctypes.c_double),
+        ("mt", ctypes.c_int),
+        ("gdamp_tmin", ctypes.c_double), ("gdamp_tmax", ctypes.c_double), ("gdamp_power", ctypes.c_double),
+        ("nza", ctypes.c_int),
+        ("water_velocity", ctypes.c_double), ("water_density", ctypes.c_double),
+        ("acoustic_source", ctypes.c_int),
+    ]
+
+
+def make_par(**kw):
+    d = dict(nt=100, sub=1, dt=4e-4, ns=1, nr=1, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2,
+             taper_top=0, taper_bottom=0, taper_left=0, taper_right=0, taper_strength=0.05,
+             free_surface_stiffness=1.05, mt=0, gdamp_tmin=0.0, gdamp_tmax=0.0, gdamp_power=1.0,
+             nza=0, water_velocity=1.5, water_density=1.0, acoustic_source=1)
+    d.update(kw)
+    p = Par()
+    for k, v in d.items():
+        if isinstance(getattr(p, k), float):
+            # every real parameter of the reference is data_t: round through float32
+            v = float(np.float32(v))
+        setattr(p, k, v)
+    return p
+
+
+class Injector(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int), ("ntr", ctypes.c_int),
+                ("xind", ctypes.c_void_p), ("zind", ctypes.c_void_p),
+                ("xw", ctypes.c_void_p), ("zw", ctypes.c_void_p)]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Lib:
+    def __init__(self, path, prec, kind):
+        self.lib = ctypes.CDLL(path)
+        self.prec = prec
+        self.kind = kind
+        self.dtype = np.float32 if prec == 32 else np.float64
+
+    def arr(self, a):
+        return np.ascontiguousarray(a, dtype=self.dtype)
+
+
+def port_path(prec=32):
+    return os.path.join(HERE, "liborc%d.so" % prec)
+
+
+def reference_path(prec=32):
+    return os.path.join(HERE, "_ref", "libfwi2d_ref%d.so" % prec)
+
+
+def have_reference(prec=32):
+    return os.path.exists(reference_path(prec))
+
+
+class Port(_Lib):
+    """The C restatement."""
+
+    def __init__(self, prec=32):
+        path = port_path(prec)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " (build with `make -C oracle`)")
+        super().__init__(path, prec, "port")
+        pre = "orc%d_" % prec
+        self._weights = getattr(self.lib, pre + "injector_weights")
+        self._prop = getattr(self.lib, pre + "propagate")
+        self._conv = getattr(self.lib, pre + "convert_model")
+        self._weights.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        self._prop.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Par),
+                               ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        self._conv.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+
+    def injector_weights(self, itype, lx, lz, nx, nz, dx, dz, ox, oz):
+        lx, lz = self.arr(lx), self.arr(lz)
+        n = len(lx)
+        w = 3 if itype == 0 else 6
+        xind = np.zeros((n, 3), np.int32)
+        zind = np.zeros((n, 3), np.int32)
+        xw = np.zeros((n, 2, w), self.dtype)
+        zw = np.zeros((n, 2, w), self.dtype)
+        self._weights(itype, n, _ptr(lx), _ptr(lz), nx, nz, dx, dz, ox, oz, _ptr(xind), _ptr(zind), _ptr(xw), _ptr(zw))
+        return xind, zind, xw, zw
+
+    def _inj(self, itype, tabs):
+        xind, zind, xw, zw = tabs
+        j = Injector(itype, len(xind), _ptr(xind), _ptr(zind), _ptr(xw), _ptr(zw))
+        j._keep = tabs
+        return j
+
+    def convert_model(self, kind, m, forward=True):
+        m = self.arr(m).copy()
+        self._conv(kind, _ptr(m), m.shape[-1] * m.shape[-2] if m.ndim == 3 else m.size // m.shape[0], 1 if forward else 0)
+        return m
+
+    def propagate(self, kind, adj, model, src, rcv, par, nx, nz, dx, dz, ox, oz, inj_locs, ext_locs,
+                  inj_type=0, full=None, grad=None, water_inj_locs=None, water_ext_locs=None):
+        """Run one shot.  inj_locs / ext_locs: (x array, z array) on the grid
+        whose origin is (ox, oz); water locations on the water grid (origin
+        (ox, 0)) for the acoustic-elastic propagator."""
+        inj = self._inj(inj_type, self.injector_weights(inj_type, inj_locs[0], inj_locs[1], nx, nz, dx, dz, ox, oz)) if inj_locs is not None else None
+        ext = self._inj(0, self.injector_weights(0, ext_locs[0], ext_locs[1], nx, nz, dx, dz, ox, oz)) if ext_locs is not None else None
+        inja = exta = None
+        if kind == KIND_AE:
+            nza = par.nza
+            wi, we = (water_inj_locs, water_ext_locs)
+            if adj:
+                wi, we = water_ext_locs, water_inj_locs
+            if wi is not None:
+                inja = self._inj(0, self.injector_weights(0, wi[0], wi[1], nx, nza, dx, dz, ox, 0.0))
+            if we is not None:
+                exta = self._inj(0, self.injector_weights(0, we[0], we[1], nx, nza, dx, dz, ox, 0.0))
+        rc = self._prop(kind, adj, _ptr(model), _ptr(src), _ptr(rcv),
+                        ctypes.byref(inj) if inj else None, ctypes.byref(ext) if ext else None,
+                        ctypes.byref(inja) if inja else None, ctypes.byref(exta) if exta else None,
+                        _ptr(full), _ptr(grad), ctypes.byref(par), nx, nz, dx, dz)
+        if rc != 0:
+            raise RuntimeError("oracle propagate failed with status %d" % rc)
+
+
+class Reference(_Lib):
+    """The reference's own sources, compiled by oracle/build_ref.sh."""
+
+    def __init__(self, prec=32):
+        path = reference_path(prec)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " (built by oracle/build_ref.sh where the reference is present)")
+        super().__init__(path, prec, "reference")
+        self._weights = self.lib.ref_injector_weights
+        self._weights.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        self._prop = self.lib.ref_propagate
+        self._prop.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int,
+                               ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+
+    def injector_weights(self, itype, lx, lz, nx, nz, dx, dz, ox, oz):
+        lx, lz = self.arr(lx), self.arr(lz)
+        n = len(lx)
+        w = 3 if itype == 0 else 6
+        xind = np.zeros((n, 3), np.int32)
+        zind = np.zeros((n, 3), np.int32)
+        xw = np.zeros((n, 2, w), self.dtype)
+        zw = np.zeros((n, 2, w), self.dtype)
+        self._weights(itype, n, _ptr(lx), _ptr(lz), nx, nz, dx, dz, ox, oz, _ptr(xind), _ptr(zind), _ptr(xw), _ptr(zw))
+        return xind, zind, xw, zw
+
+    def propagate(self, kind, adj, model, src, rcv, par, nx, nz, dx, dz, ox, oz, inj_locs, ext_locs,
+                  inj_type=0, full=None, grad=None, water_inj_locs=None, water_ext_locs=None):
+        def loc(l):
+            if l is None:
+                return 0, None, None
+            x, z = self.arr(l[0]), self.arr(l[1])
+            return len(x), x, z
+        ni, ix, iz = loc(inj_locs)
+        ne, ex, ez = loc(ext_locs)
+        nsa, sax, saz = loc(water_inj_locs)
+        nra, rax, raz = loc(water_ext_locs)
+        rc = self._prop(kind, adj, _ptr(model), _ptr(src), _ptr(rcv), inj_type, ni, _ptr(ix), _ptr(iz),
+                        ne, _ptr(ex), _ptr(ez), nsa, _ptr(sax), _ptr(saz), nra, _ptr(rax), _ptr(raz),
+                        _ptr(full), _ptr(grad), ctypes.byref(par), nx, nz, dx, dz, ox, oz)
+        if rc != 0:
+            raise RuntimeError("reference propagate failed with status %d" % rc)

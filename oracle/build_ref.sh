@@ -1,0 +1,35 @@
+#!/bin/sh
+# Compile the reference's own CPU propagation sources (read in place under
+# /root/reference, never copied) into oracle/_ref/ with the shims in
+# oracle/ref_shim/: libfwi2d_ref32.so (FP32, the reference's default build)
+# and libfwi2d_ref64.so (FP64, as ENABLE_DOUBLE_PRECISION).
+# Flags follow the reference's CMakeLists.txt: -O3 -fopenmp, no MPI, no CUDA.
+set -e
+REF=${FWI2D_REFERENCE:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+if [ ! -d "$REF/src/cpp" ]; then
+    echo "reference sources not found at $REF; skipping the reference build" >&2
+    exit 0
+fi
+mkdir -p "$OUT"
+SRCS="we_op.cpp spatial_operators.cpp injector.cpp misc.cpp operator.cpp dummy.cpp"
+for prec in 32 64; do
+    B="$OUT/obj$prec"
+    mkdir -p "$B"
+    DEF=""
+    [ "$prec" = 64 ] && DEF="-DDOUBLE_PRECISION"
+    OBJS=""
+    for s in $SRCS; do
+        o="$B/${s%.cpp}.o"
+        g++ -std=c++11 -O3 -fopenmp -fPIC -fpermissive -w $DEF -I"$HERE/ref_shim" -I"$REF/src/include" -c "$REF/src/cpp/$s" -o "$o"
+        OBJS="$OBJS $o"
+    done
+    for s in ispc_loops.cpp stubs.cpp ref_driver.cpp; do
+        o="$B/${s%.cpp}.o"
+        g++ -std=c++11 -O3 -fopenmp -fPIC -w $DEF -I"$HERE/ref_shim" -I"$REF/src/include" -c "$HERE/ref_shim/$s" -o "$o"
+        OBJS="$OBJS $o"
+    done
+    g++ -shared -fopenmp -o "$OUT/libfwi2d_ref$prec.so" $OBJS -Wl,--no-undefined
+done
+echo "reference oracle built in $OUT"

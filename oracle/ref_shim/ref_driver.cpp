@@ -1,0 +1,112 @@
+// C entry points over the reference's own propagation code, for the oracle
+// build only.  Compiled together with the reference sources (src/cpp/we_op.cpp,
+// spatial_operators.cpp, injector.cpp, misc.cpp, operator.cpp, dummy.cpp) by
+// oracle/build_ref.sh into oracle/_ref/.  Used to generate tests/golden/ and
+// to pin the restatement in oracle/fwi2d_oracle.c.
+#include <vector>
+#include <cstring>
+#include "we_op.hpp"
+
+struct ref_param {
+    int nt, sub;
+    double dt;
+    int ns, nr;
+    int bc_top, bc_bottom, bc_left, bc_right;
+    int taper_top, taper_bottom, taper_left, taper_right;
+    double taper_strength, free_surface_stiffness;
+    int mt;
+    double gdamp_tmin, gdamp_tmax, gdamp_power;
+    int nza;
+    double water_velocity, water_density;
+    int acoustic_source;
+};
+
+static param to_param(const ref_param *p)
+{
+    param par;
+    par.nt = p->nt; par.sub = p->sub; par.dt = (data_t)p->dt;
+    par.ns = p->ns; par.nr = p->nr;
+    par.bc_top = p->bc_top; par.bc_bottom = p->bc_bottom; par.bc_left = p->bc_left; par.bc_right = p->bc_right;
+    par.taper_top = p->taper_top; par.taper_bottom = p->taper_bottom;
+    par.taper_left = p->taper_left; par.taper_right = p->taper_right;
+    par.taper_strength = (data_t)p->taper_strength;
+    par.free_surface_stiffness = (data_t)p->free_surface_stiffness;
+    par.mt = p->mt != 0;
+    par.gdamp_tmin = (data_t)p->gdamp_tmin; par.gdamp_tmax = (data_t)p->gdamp_tmax; par.gdamp_power = (data_t)p->gdamp_power;
+    par.nza = p->nza;
+    par.water_velocity = (data_t)p->water_velocity; par.water_density = (data_t)p->water_density;
+    par.acoustic_source = p->acoustic_source != 0;
+    par.acoustic_elastic = p->nza > 0;
+    par.version = 2;
+    par.pml = false; par.pml_T = par.pml_B = par.pml_L = par.pml_R = false;
+    par.verbose = 0;
+    return par;
+}
+
+static std::vector<std::vector<data_t> > locs(int n, const data_t *x, const data_t *z)
+{
+    std::vector<std::vector<data_t> > v(n);
+    for (int i = 0; i < n; i++) v[i] = {x[i], z[i], 0};
+    return v;
+}
+
+static hypercube<data_t> grid(int nx, int nz, double dx, double dz, double ox, double oz)
+{
+    return hypercube<data_t>(axis<data_t>(nz, (data_t)oz, (data_t)dz), axis<data_t>(nx, (data_t)ox, (data_t)dx));
+}
+
+extern "C" {
+
+int ref_real_size(void) { return (int)sizeof(data_t); }
+
+// injector tables built by the reference's delta_m3 / ddelta_m3.
+int ref_injector_weights(int type, int ntr, const data_t *lx, const data_t *lz, int nx, int nz,
+                         double dx, double dz, double ox, double oz, int *xind, int *zind, data_t *xw, data_t *zw)
+{
+    hypercube<data_t> g = grid(nx, nz, dx, dz, ox, oz);
+    injector *J;
+    if (type == 0) J = new delta_m3(g, locs(ntr, lx, lz));
+    else J = new ddelta_m3(g, locs(ntr, lx, lz));
+    std::memcpy(xind, J->_xind.data(), J->_xind.size() * sizeof(int));
+    std::memcpy(zind, J->_zind.data(), J->_zind.size() * sizeof(int));
+    std::memcpy(xw, J->_xw.data(), J->_xw.size() * sizeof(data_t));
+    std::memcpy(zw, J->_zw.data(), J->_zw.size() * sizeof(data_t));
+    delete J;
+    return 0;
+}
+
+// kind: 0 elastic, 1 VTI, 2 acoustic, 3 acoustic-elastic.
+// inj/ext locations are on the (elastic) grid; for kind 3 the water-layer
+// source (sa) and receiver (ra) locations are passed too.
+int ref_propagate(int kind, int adj, const data_t *model, const data_t *allsrc, data_t *allrcv,
+                  int inj_type, int ninj, const data_t *ix, const data_t *iz,
+                  int next, const data_t *ex, const data_t *ez,
+                  int nsa, const data_t *sax, const data_t *saz, int nra, const data_t *rax, const data_t *raz,
+                  data_t *full, data_t *grad, const ref_param *rp, int nx, int nz,
+                  double dx, double dz, double ox, double oz)
+{
+    try {
+        param par = to_param(rp);
+        hypercube<data_t> g = grid(nx, nz, dx, dz, ox, oz);
+        injector *inj = nullptr, *ext = nullptr;
+        if (ninj > 0) inj = inj_type == 0 ? (injector *)new delta_m3(g, locs(ninj, ix, iz)) : (injector *)new ddelta_m3(g, locs(ninj, ix, iz));
+        if (next > 0) ext = new delta_m3(g, locs(next, ex, ez));
+        if (kind == 3) {
+            par.sxz = locs(nsa, sax, saz);
+            par.rxza = {locs(nra, rax, raz)};
+            par.rxz = {locs(next, ex, ez)};
+        }
+        if (kind == 0) { nl_we_op_e op; op.propagate(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, (data_t)ox, (data_t)oz, 0); }
+        else if (kind == 1) { nl_we_op_vti op; op.propagate(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, (data_t)ox, (data_t)oz, 0); }
+        else if (kind == 2) { nl_we_op_a op; op.propagate(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, (data_t)ox, (data_t)oz, 0); }
+        else if (kind == 3) { nl_we_op_ae op; op.propagate(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, (data_t)ox, (data_t)oz, 0); }
+        delete inj;
+        delete ext;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_propagate: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+}
