@@ -1,0 +1,1156 @@
+// Host engine and C ABI of fwi2d_b200.
+//
+// A context owns one device stream, one model and one batch plan.  The plan
+// holds every per-shot device buffer (two field buffers, time-major traces,
+// injection / extraction tables, boundary and taper tables, snapshots and the
+// gradient accumulator) and two CUDA graphs: the forward time loop and the
+// adjoint time loop, each a chain of one fused kernel per time step.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "host_tables.h"
+#include "launch.h"
+#include "../../include/fwi2d_b200.h"
+
+namespace fwi2d {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                              \
+    do {                                                                                                   \
+        cudaError_t e_ = (x);                                                                              \
+        if (e_ != cudaSuccess) {                                                                           \
+            (void)cudaGetLastError();                                                                      \
+            throw Error(e_ == cudaErrorMemoryAllocation ? FWI2D_ERR_OOM : FWI2D_ERR_CUDA,                  \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                                  \
+        }                                                                                                  \
+    } while (0)
+#define REQ(c, msg)                                      \
+    do {                                                 \
+        if (!(c)) throw Error(FWI2D_ERR_ARG, (msg));     \
+    } while (0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t bytes)
+    {
+        release();
+        if (bytes) {
+            CK(cudaMalloc(&p, bytes));
+            n = bytes;
+        }
+    }
+    template <class T> T *as() const { return (T *)p; }
+    template <class T> void upload(const std::vector<T> &v, cudaStream_t st)
+    {
+        alloc(std::max<size_t>(v.size(), 1) * sizeof(T));
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    }
+};
+
+static int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// ---------------------------------------------------------------------------
+// layout kernels
+// ---------------------------------------------------------------------------
+__global__ void k_to_time_major(const float *__restrict__ in, float *__restrict__ out, int rows, int nt)
+{
+    __shared__ float t[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < rows && c < nt) t[j][threadIdx.x] = in[(long long)r * nt + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        int c = c0 + j, r = r0 + threadIdx.x;
+        if (r < rows && c < nt) out[(long long)c * rows + r] = t[threadIdx.x][j];
+    }
+}
+__global__ void k_from_time_major(const float *__restrict__ in, float *__restrict__ out, int rows, int nt)
+{
+    __shared__ float t[32][33];
+    const int c0 = blockIdx.y * 32, r0 = blockIdx.x * 32;   // in is [nt][rows]
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        int c = c0 + j, r = r0 + threadIdx.x;
+        if (r < rows && c < nt) t[j][threadIdx.x] = in[(long long)c * rows + r];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < rows && c < nt) out[(long long)r * nt + c] = t[threadIdx.x][j];
+    }
+}
+__global__ void k_add_subgrid(float *__restrict__ full, const float *__restrict__ part, int ncomp, int x0, int nx,
+                              int ldz, long long full_comp)
+{
+    const long long n = (long long)ncomp * nx * ldz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long c = i / ((long long)nx * ldz);
+        const long long r = i - c * nx * ldz;
+        full[c * full_comp + (long long)x0 * ldz + r] += part[i];
+    }
+}
+__global__ void k_pitch(const float *__restrict__ in, float *__restrict__ out, long long rows, int nz, int ldz)
+{
+    const long long n = rows * ldz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / ldz;
+        const int z = (int)(i - r * ldz);
+        out[i] = z < nz ? in[r * nz + z] : 0.f;
+    }
+}
+__global__ void k_unpitch(const float *__restrict__ in, float *__restrict__ out, long long rows, int nz, int ldz)
+{
+    const long long n = rows * nz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / nz;
+        const int z = (int)(i - r * nz);
+        out[i] = in[r * ldz + z];
+    }
+}
+
+void launch_to_time_major(const float *in, float *out, int rows, int nt, cudaStream_t st)
+{
+    dim3 g((nt + 31) / 32, (rows + 31) / 32), b(32, 8);
+    k_to_time_major<<<g, b, 0, st>>>(in, out, rows, nt);
+}
+void launch_from_time_major(const float *in, float *out, int rows, int nt, cudaStream_t st)
+{
+    dim3 g((rows + 31) / 32, (nt + 31) / 32), b(32, 8);
+    k_from_time_major<<<g, b, 0, st>>>(in, out, rows, nt);
+}
+void launch_add_subgrid(float *full, const float *part, int ncomp, int x0, int nx, int ldz, long long full_comp,
+                        cudaStream_t st)
+{
+    k_add_subgrid<<<592, 256, 0, st>>>(full, part, ncomp, x0, nx, ldz, full_comp);
+}
+
+// ---------------------------------------------------------------------------
+// model
+// ---------------------------------------------------------------------------
+struct ModelState {
+    int kind = -1, nx = 0, nz = 0, ldz = 0, npar = 0;
+    float dx = 0, dz = 0;
+    std::vector<float> host;   // converted model as given, [npar][nx][nz]
+    DevBuf p0, p1, p2, c13, eps, fxx, lbis, gv2, gv3;
+    ModelDev dev() const
+    {
+        ModelDev m;
+        m.nx = nx;
+        m.nz = nz;
+        m.ldz = ldz;
+        m.p0 = p0.as<float>();
+        m.p1 = p1.as<float>();
+        m.p2 = p2.as<float>();
+        m.c13 = c13.as<float>();
+        m.eps = eps.as<float>();
+        m.fxx = fxx.as<float>();
+        m.lbis = lbis.as<float>();
+        m.gv2 = gv2.as<float>();
+        m.gv3 = gv3.as<float>();
+        return m;
+    }
+    const float *hp(int i) const { return host.data() + (size_t)i * nx * nz; }
+};
+
+static int npar_of(int kind)
+{
+    switch (kind) {
+    case KIND_ELASTIC: return 3;
+    case KIND_VTI: return 5;
+    case KIND_ACOUSTIC: return 2;
+    case KIND_AE: return 3;
+    }
+    return -1;
+}
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+struct ShotPlan {
+    int x0 = 0, nx = 0, nt = 0, tiles_x = 0, tiles_z = 0;
+    int ncomp = 2;                 // field components
+    int ncomp_src = 2, ntr_src = 0, nr = 0;
+    int nsrc_rows = 0, nrcv_rows = 0;
+    int nslot = 0;
+    std::vector<InjEntry> inj_f, inj_a;
+    std::vector<int> inj_f_off, inj_a_off;
+    std::vector<ExtEntry> ext_f;
+    std::vector<int> ext_f_off, ext_none_off;
+    DevBuf u0, u1, src_f, rcv_f, src_a;
+    DevBuf d_inj_f, d_inj_f_off, d_inj_a, d_inj_a_off, d_ext_f, d_ext_f_off, d_ext_none_off;
+    DevBuf den, tz, tx, snap, amax, grad, gwt;
+};
+
+struct Plan {
+    fwi2d_params par;
+    int kind = 0;
+    int shape = 0, TZ = 32, TX = 16;
+    int nt_max = 0;
+    int ncompg = 3;
+    std::vector<std::unique_ptr<ShotPlan>> shots;
+    std::vector<TileRef> tiles;
+    DevBuf d_tiles, d_shots_f, d_shots_a;
+    DevBuf d_init, d_init_off;
+    size_t init_cap = 0;
+    DevBuf d_grad_full, d_stage;
+    StepConst C;
+    float dtg = 0;
+    bool have_snapshots = false;
+    bool snapshots_valid = false;
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};   // forward, forward+store, adjoint
+    long long launches[3] = {0, 0, 0};
+    long long snap_bytes = 0;
+    ~Plan()
+    {
+        for (auto &g : graph)
+            if (g) cudaGraphExecDestroy(g);
+    }
+};
+
+}  // namespace fwi2d
+
+struct fwi2d_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    fwi2d::ModelState M;
+    std::unique_ptr<fwi2d::Plan> plan;
+};
+
+namespace fwi2d {
+
+static void set_device(fwi2d_ctx *ctx) { CK(cudaSetDevice(ctx->device)); }
+
+// ---- model upload -----------------------------------------------------------
+static void set_model(fwi2d_ctx *ctx, int kind, int nx, int nz, float dx, float dz, const float *model)
+{
+    REQ(kind >= 0 && kind <= 3, "unknown propagator kind");
+    REQ(nx >= 12 && nz >= 12, "the model must have at least 12 samples along each axis");
+    REQ(dx > 0 && dz > 0, "grid spacings must be positive");
+    REQ(model != nullptr, "null model");
+    set_device(ctx);
+    ModelState &M = ctx->M;
+    ctx->plan.reset();
+    M.kind = kind;
+    M.nx = nx;
+    M.nz = nz;
+    M.ldz = round_up(nz, 32);
+    M.dx = dx;
+    M.dz = dz;
+    M.npar = npar_of(kind);
+    const size_t nxz = (size_t)nx * nz;
+    M.host.assign(model, model + nxz * M.npar);
+    for (size_t i = 0; i < M.host.size(); i++) REQ(std::isfinite(M.host[i]), "model holds a non-finite value");
+    const size_t pitched = (size_t)nx * M.ldz;
+    DevBuf stage;
+    stage.alloc(nxz * sizeof(float));
+    auto up = [&](DevBuf &dst, const float *src) {
+        dst.alloc(pitched * sizeof(float));
+        CK(cudaMemcpyAsync(stage.p, src, nxz * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        k_pitch<<<592, 256, 0, ctx->st>>>(stage.as<float>(), dst.as<float>(), nx, nz, M.ldz);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->st));
+    };
+    up(M.p0, M.hp(0));
+    up(M.p1, M.hp(1));
+    if (kind != KIND_ACOUSTIC) up(M.p2, M.hp(2));
+    else M.p2.release();
+    M.c13.release();
+    M.eps.release();
+    M.fxx.release();
+    M.lbis.release();
+    M.gv2.release();
+    M.gv3.release();
+    if (kind == KIND_VTI) {
+        const float *lam = M.hp(0), *mu = M.hp(1), *c13 = M.hp(3), *eps = M.hp(4);
+        std::vector<float> fxx(nxz), lbis(nxz), v2(nxz), v3(nxz);
+        for (size_t i = 0; i < nxz; i++) {
+            fxx[i] = (1 + 2 * eps[i]) * 2 * mu[i];           // vtiexpr7b, we_op.cpp:1473
+            lbis[i] = (1 + 2 * eps[i]) * lam[i];             // mod_bis, we_op.cpp:1590
+            const float l = lam[i], m = mu[i], c = c13[i];   // we_op.cpp:1499-1504
+            const float del = ((c + m) * (c + m) - (l + m) * (l + m)) / (2 * (l + m) * (l + 2 * m));
+            const float val1 = std::sqrt(2 * (l + 2 * m) * (l + m) * del + (l + m) * (l + m));
+            v2[i] = ((1 + 2 * del) * l + (1 + 3 * del) * m) / val1;
+            v3[i] = ((1 + 3 * del) * l + (1 + 4 * del) * m) / val1 - 1;
+        }
+        up(M.c13, c13);
+        up(M.eps, eps);
+        up(M.fxx, fxx.data());
+        up(M.lbis, lbis.data());
+        up(M.gv2, v2.data());
+        up(M.gv3, v3.data());
+    }
+}
+
+// ---- plan construction -------------------------------------------------------
+static int owner_tile(int g, int n, int T)
+{
+    if (g >= n - T) return (n + T - 1) / T - 1;
+    return g / T;
+}
+
+static void check_injector(const fwi2d_injector &J, int nx, int nz, const char *what)
+{
+    if (J.ntr == 0) return;
+    REQ(J.ntr > 0 && J.xind && J.zind && J.xw && J.zw, std::string(what) + ": incomplete injector tables");
+    REQ(J.type == FWI2D_INJ_DELTA || J.type == FWI2D_INJ_DDELTA, std::string(what) + ": unknown injector type");
+    for (int t = 0; t < J.ntr; t++)
+        for (int k = 0; k < 3; k++) {
+            REQ(J.xind[t * 3 + k] >= 0 && J.xind[t * 3 + k] < nx, std::string(what) + ": x index outside the shot grid");
+            REQ(J.zind[t * 3 + k] >= 0 && J.zind[t * 3 + k] < nz, std::string(what) + ": z index outside the shot grid");
+        }
+}
+
+// Injection entries of one injector into a field, in the reference's order
+// (trace, x, z), then stably grouped by owning tile.  rows(c, itr, which)
+// gives the trace row of component c.
+static void build_inj(const fwi2d_injector &J, int ncomp, const int *rowbase_a, const int *rowbase_b, int nx, int nz,
+                      int TX, int TZ, int tiles_x, int ntiles, std::vector<InjEntry> &out, std::vector<int> &off)
+{
+    std::vector<InjEntry> ent;
+    const int w = J.type == FWI2D_INJ_DELTA ? 3 : 6;
+    for (int c = 0; c < ncomp; c++)
+        for (int t = 0; t < J.ntr; t++) {
+            const float *xi = J.xw + (size_t)t * 2 * w, *zi = J.zw + (size_t)t * 2 * w;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) {
+                    InjEntry e;
+                    e.gx = J.xind[t * 3 + a];
+                    e.gz = J.zind[t * 3 + b];
+                    e.comp = c;
+                    if (J.type == FWI2D_INJ_DELTA) {
+                        e.mt = 0;
+                        e.ia = rowbase_a[c] + t;
+                        e.ib = 0;
+                        e.wa = xi[a] * zi[b];
+                        e.wb = 0.f;
+                    } else {
+                        e.mt = 1;
+                        e.ia = rowbase_a[c] + t;
+                        e.ib = rowbase_b[c] + t;
+                        e.wa = -xi[a + 3] * zi[b];
+                        e.wb = xi[a] * zi[b + 3];
+                    }
+                    ent.push_back(e);
+                }
+        }
+    std::vector<int> tile_of(ent.size());
+    for (size_t i = 0; i < ent.size(); i++)
+        tile_of[i] = owner_tile(ent[i].gz, nz, TZ) * tiles_x + owner_tile(ent[i].gx, nx, TX);
+    std::vector<size_t> idx(ent.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return tile_of[a] < tile_of[b]; });
+    out.clear();
+    off.assign(ntiles + 1, 0);
+    for (size_t i : idx) {
+        out.push_back(ent[i]);
+        off[tile_of[i] + 1]++;
+    }
+    for (int t = 0; t < ntiles; t++) off[t + 1] += off[t];
+}
+
+static void build_ext(const fwi2d_injector &J, int ncomp, int nx, int nz, int TX, int TZ, int tiles_x, int ntiles,
+                      std::vector<ExtEntry> &out, std::vector<int> &off)
+{
+    std::vector<ExtEntry> ent;
+    std::vector<int> tile_of;
+    for (int c = 0; c < ncomp; c++)
+        for (int t = 0; t < J.ntr; t++) {
+            ExtEntry e;
+            e.row = c * J.ntr + t;
+            e.comp = c;
+            e.gx0 = J.xind[t * 3];
+            e.gz0 = J.zind[t * 3];
+            const float *xe = J.xw + (size_t)t * 6 + 3, *ze = J.zw + (size_t)t * 6 + 3;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) e.w[a * 3 + b] = xe[a] * ze[b];
+            ent.push_back(e);
+            tile_of.push_back(owner_tile(J.zind[t * 3 + 1], nz, TZ) * tiles_x + owner_tile(J.xind[t * 3 + 1], nx, TX));
+        }
+    std::vector<size_t> idx(ent.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return tile_of[a] < tile_of[b]; });
+    out.clear();
+    off.assign(ntiles + 1, 0);
+    for (size_t i : idx) {
+        out.push_back(ent[i]);
+        off[tile_of[i] + 1]++;
+    }
+    for (int t = 0; t < ntiles; t++) off[t + 1] += off[t];
+}
+
+static StepConst make_const(const fwi2d_params &p, float dx, float dz)
+{
+    StepConst C;
+    std::memset(&C, 0, sizeof(C));
+    const float h0 = sbp_tables().h0;
+    C.dt = p.dt;
+    C.dt2 = p.dt * p.dt;
+    C.dx = dx;
+    C.dz = dz;
+    C.d2x = dx * dx;
+    C.d2z = dz * dz;
+    C.inv_d2x = 1.f / C.d2x;
+    C.inv_d2z = 1.f / C.d2z;
+    C.adx = 1.f / dx;
+    C.adz = 1.f / dz;
+    C.sdx = (float)(1.0 / (double)dx);
+    C.sdz = (float)(1.0 / (double)dz);
+    C.sat_x = 1.f / (dx * h0);
+    C.sat_z = 1.f / (dz * h0);
+    C.nsat_x = 1.f / (dx * dx * h0);
+    C.nsat_z = 1.f / (dz * dz * h0);
+    C.alpha = (float)(0.2508560249 / p.free_surface_stiffness);
+    C.bc[0] = p.bc_top;
+    C.bc[1] = p.bc_bottom;
+    C.bc[2] = p.bc_left;
+    C.bc[3] = p.bc_right;
+    C.sub = p.sub > 0 ? p.sub : 1;
+    C.snap_prec = p.snapshot_precision;
+    C.kahan = p.compensated;
+    return C;
+}
+
+static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool adjoint, ShotDev &d)
+{
+    std::memset(&d, 0, sizeof(d));
+    d.nx = s.nx;
+    d.nz = M.nz;
+    d.ldz = M.ldz;
+    d.x0 = s.x0;
+    d.nt = s.nt;
+    d.tiles_x = s.tiles_x;
+    d.tiles_z = s.tiles_z;
+    d.u[0] = s.u0.as<float>();
+    d.u[1] = s.u1.as<float>();
+    if (!adjoint) {
+        d.src = s.src_f.as<float>();
+        d.nsrc = s.nsrc_rows;
+        d.rcv = s.rcv_f.as<float>();
+        d.nrcv = s.nrcv_rows;
+        d.inj = s.d_inj_f.as<InjEntry>();
+        d.inj_off = s.d_inj_f_off.as<int>();
+        d.ext = s.d_ext_f.as<ExtEntry>();
+        d.ext_off = s.d_ext_f_off.as<int>();
+    } else {
+        d.src = s.src_a.as<float>();
+        d.nsrc = s.nrcv_rows;
+        d.rcv = nullptr;
+        d.nrcv = 0;
+        d.inj = s.d_inj_a.as<InjEntry>();
+        d.inj_off = s.d_inj_a_off.as<int>();
+        d.ext = nullptr;
+        d.ext_off = s.d_ext_none_off.as<int>();
+    }
+    d.den = s.den.as<float>();
+    d.tz = s.tz.as<float>();
+    d.tx = s.tx.as<float>();
+    d.snap = s.snap.p;
+    d.snap_slot = (long long)s.ncomp * s.nx * M.ldz;
+    d.snap_amax = s.amax.as<unsigned>();
+    d.grad = s.grad.as<float>();
+    d.gwt = s.gwt.as<float>();
+    (void)P;
+}
+
+static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
+{
+    ModelState &M = ctx->M;
+    if (M.kind < 0) throw Error(FWI2D_ERR_STATE, "fwi2d_set_model must be called first");
+    REQ(par != nullptr && shots != nullptr && nshots > 0, "no shots");
+    const fwi2d_params &p = *par;
+    REQ(p.nt >= 2, "nt must be at least 2");
+    REQ(p.dt > 0, "dt must be positive");
+    REQ(p.sub >= 0, "sub must be >= 0");
+    REQ(p.snapshot_precision >= 0 && p.snapshot_precision <= 2, "unknown snapshot precision");
+    REQ(p.taper_top >= 0 && p.taper_bottom >= 0 && p.taper_left >= 0 && p.taper_right >= 0, "negative taper");
+    REQ(p.taper_top + p.taper_bottom <= M.nz, "top and bottom tapers overlap");
+    for (int i = 0; i < 4; i++) {
+        int bc = (&p.bc_top)[i];
+        REQ(bc >= 1 && bc <= 3, "boundary condition must be 1, 2 or 3");
+        if (M.kind != KIND_ACOUSTIC) REQ(bc <= 2, "the elastic propagators take boundary conditions 1 or 2");
+    }
+    if (M.kind == KIND_ACOUSTIC || M.kind == KIND_AE)
+        throw Error(FWI2D_ERR_UNSUPPORTED, "this propagator is not built yet");
+    REQ(p.checkpoint_every == 0, "checkpointing is not available in this build");
+    set_device(ctx);
+
+    auto P = std::make_unique<Plan>();
+    P->par = p;
+    P->kind = M.kind;
+    P->ncompg = M.kind == KIND_ACOUSTIC ? 2 : 3;
+    P->C = make_const(p, M.dx, M.dz);
+    P->dtg = (float)(P->C.sub) * p.dt;
+
+    // tile shape: the requested one, else the first that tiles every shot
+    // grid.  An axis of n samples takes tiles of T when n == T or n >= T + 8,
+    // so that each SBP boundary band lies in a window that reaches its boundary.
+    auto fits = [&](int T, int n) { return n == T || n >= T + 8; };
+    auto shape_ok = [&](int i) {
+        int tz, tx;
+        elastic_tile_shape(i, &tz, &tx);
+        if (!fits(tz, M.nz)) return false;
+        for (int s = 0; s < nshots; s++)
+            if (!fits(tx, shots[s].nx)) return false;
+        return true;
+    };
+    const int nshapes = elastic_tile_count();
+    int shape = p.tile_shape;
+    if (shape < 0 || shape >= nshapes) {
+        shape = -1;
+        for (int i = 0; i < nshapes && shape < 0; i++)
+            if (shape_ok(i)) shape = i;
+        REQ(shape >= 0, "no tile shape fits the grid (an axis needs n == T or n >= T + 8)");
+    }
+    REQ(shape_ok(shape), "the requested tile shape does not fit a shot grid");
+    P->shape = shape;
+    elastic_tile_shape(shape, &P->TZ, &P->TX);
+
+    const bool vti = M.kind == KIND_VTI;
+    long long total_bytes = 0;
+    for (int s = 0; s < nshots; s++) {
+        const fwi2d_shot &sh = shots[s];
+        REQ(sh.x0 >= 0 && sh.nx >= 12 && sh.x0 + sh.nx <= M.nx, "shot grid outside the model");
+        REQ(sh.nt >= 2 && sh.nt <= p.nt, "shot nt must be in [2, params.nt]");
+        REQ(p.taper_left + p.taper_right <= sh.nx, "left and right tapers overlap");
+        REQ(sh.src.ntr > 0, "shot without source");
+        REQ(sh.rcv.ntr > 0 && sh.rcv.type == FWI2D_INJ_DELTA, "shot receivers must be a delta injector");
+        REQ((sh.src.type == FWI2D_INJ_DDELTA) == (p.mt != 0), "source injector type must match params.mt");
+        check_injector(sh.src, sh.nx, M.nz, "source");
+        check_injector(sh.rcv, sh.nx, M.nz, "receivers");
+        auto S = std::make_unique<ShotPlan>();
+        S->x0 = sh.x0;
+        S->nx = sh.nx;
+        S->nt = sh.nt;
+        S->ncomp = 2;
+        S->tiles_x = (sh.nx + P->TX - 1) / P->TX;
+        S->tiles_z = (M.nz + P->TZ - 1) / P->TZ;
+        const int ntiles = S->tiles_x * S->tiles_z;
+        S->ntr_src = sh.src.ntr;
+        S->ncomp_src = p.mt ? 3 : 2;
+        S->nr = sh.rcv.ntr;
+        S->nsrc_rows = S->ncomp_src * S->ntr_src;
+        S->nrcv_rows = 2 * S->nr;
+        // forward sources: force -> rows c*ntr ; moment tensor blocks (mxx, mzz, mxz)
+        int ra[2], rb[2];
+        if (!p.mt) {
+            ra[0] = 0;
+            ra[1] = S->ntr_src;
+            rb[0] = rb[1] = 0;
+        } else {
+            ra[0] = 0;                  // next0: inx = mxx, inz = mxz  (we_op.cpp:618-621)
+            rb[0] = 2 * S->ntr_src;
+            ra[1] = 2 * S->ntr_src;     // next1: inx = mxz, inz = mzz
+            rb[1] = S->ntr_src;
+        }
+        build_inj(sh.src, 2, ra, rb, sh.nx, M.nz, P->TX, P->TZ, S->tiles_x, ntiles, S->inj_f, S->inj_f_off);
+        int qa[2] = {0, S->nr}, qb[2] = {0, 0};
+        build_inj(sh.rcv, 2, qa, qb, sh.nx, M.nz, P->TX, P->TZ, S->tiles_x, ntiles, S->inj_a, S->inj_a_off);
+        build_ext(sh.rcv, 2, sh.nx, M.nz, P->TX, P->TZ, S->tiles_x, ntiles, S->ext_f, S->ext_f_off);
+        S->ext_none_off.assign(ntiles + 1, 0);
+
+        // boundary divisors and taper on this shot's window of the model
+        std::vector<float> den, tz, tx;
+        const float *lam = M.hp(0) + (size_t)sh.x0 * M.nz, *mu = M.hp(1) + (size_t)sh.x0 * M.nz,
+                    *rho = M.hp(2) + (size_t)sh.x0 * M.nz;
+        const float *eps = vti ? M.hp(4) + (size_t)sh.x0 * M.nz : nullptr;
+        elastic_scale_divisors(sh.nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, p.bc_top == 2,
+                               p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
+        taper_factors(sh.nx, M.nz, p.taper_top, p.taper_bottom, p.taper_left, p.taper_right, p.taper_strength,
+                      true, true, true, true, tz, tx);
+        S->nslot = p.sub > 0 ? 1 + sh.nt / p.sub : 0;
+        std::vector<float> gw(std::max(S->nslot, 1), 1.f);
+        for (int i = 0; i < S->nslot; i++) {
+            float t = i * P->dtg;
+            float w = 1;
+            if (p.gdamp_tmax - t > 0 && t - p.gdamp_tmin >= 0)
+                w = (float)std::cos(p.gdamp_power * M_PI * (t - p.gdamp_tmin) / (p.gdamp_tmax - p.gdamp_tmin));
+            w *= w;
+            gw[i] = w;
+        }
+
+        const size_t field = (size_t)S->ncomp * sh.nx * M.ldz;
+        S->u0.alloc(field * sizeof(float));
+        S->u1.alloc(field * sizeof(float));
+        S->src_f.alloc((size_t)sh.nt * S->nsrc_rows * sizeof(float));
+        S->rcv_f.alloc((size_t)sh.nt * S->nrcv_rows * sizeof(float));
+        S->src_a.alloc((size_t)sh.nt * S->nrcv_rows * sizeof(float));
+        S->d_inj_f.upload(S->inj_f, ctx->st);
+        S->d_inj_f_off.upload(S->inj_f_off, ctx->st);
+        S->d_inj_a.upload(S->inj_a, ctx->st);
+        S->d_inj_a_off.upload(S->inj_a_off, ctx->st);
+        S->d_ext_f.upload(S->ext_f, ctx->st);
+        S->d_ext_f_off.upload(S->ext_f_off, ctx->st);
+        S->d_ext_none_off.upload(S->ext_none_off, ctx->st);
+        S->den.upload(den, ctx->st);
+        S->tz.upload(tz, ctx->st);
+        S->tx.upload(tx, ctx->st);
+        S->gwt.upload(gw, ctx->st);
+        S->grad.alloc((size_t)P->ncompg * sh.nx * M.ldz * sizeof(float));
+        if (S->nslot > 0) {
+            const size_t esz = p.snapshot_precision == FWI2D_SNAP_FP32 ? 4 : 2;
+            const size_t bytes = (size_t)S->nslot * field * esz;
+            S->snap.alloc(bytes);
+            S->amax.alloc((size_t)S->nslot * sizeof(unsigned));
+            P->snap_bytes += bytes;
+            total_bytes += bytes;
+        }
+        P->nt_max = std::max(P->nt_max, sh.nt);
+        for (int tzi = 0; tzi < S->tiles_z; tzi++)
+            for (int txi = 0; txi < S->tiles_x; txi++) P->tiles.push_back(TileRef{s, txi, tzi, 0});
+        P->shots.push_back(std::move(S));
+    }
+    P->have_snapshots = p.sub > 0;
+    P->d_tiles.upload(P->tiles, ctx->st);
+    std::vector<ShotDev> sf(nshots), sa(nshots);
+    for (int s = 0; s < nshots; s++) {
+        shot_dev(*P, *P->shots[s], M, false, sf[s]);
+        shot_dev(*P, *P->shots[s], M, true, sa[s]);
+    }
+    P->d_shots_f.upload(sf, ctx->st);
+    P->d_shots_a.upload(sa, ctx->st);
+    // initial-state scatter buffers: at most one entry per injection sample
+    size_t cap = 0;
+    for (auto &S : P->shots) cap += std::max(S->inj_f.size(), S->inj_a.size());
+    P->init_cap = std::max<size_t>(cap, 1);
+    P->d_init.alloc(P->init_cap * sizeof(InitEntry));
+    P->d_init_off.alloc((nshots + 1) * sizeof(int));
+    P->d_grad_full.alloc((size_t)P->ncompg * M.nx * M.ldz * sizeof(float));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->plan = std::move(P);
+}
+
+// Initial "prev" of the leapfrog (we_op.cpp:657-663): inject sample 0 with
+// add=false, then scale by dt^2/(2 rho) in double.
+static void compute_init(const ModelState &M, const Plan &P, bool adjoint, const float *const *trace_blocks,
+                         std::vector<InitEntry> &ent, std::vector<int> &off)
+{
+    ent.clear();
+    off.assign(P.shots.size() + 1, 0);
+    for (size_t s = 0; s < P.shots.size(); s++) {
+        const ShotPlan &S = *P.shots[s];
+        const std::vector<InjEntry> &inj = adjoint ? S.inj_a : S.inj_f;
+        const float *tr = trace_blocks[s];   // [rows][nt]
+        // accumulate per cell in entry order (entries of one cell keep the reference's trace order)
+        std::vector<InitEntry> cells;
+        for (const InjEntry &e : inj) {
+            const float a = tr[(size_t)e.ia * S.nt];
+            const float c = e.mt ? (e.wa * a - e.wb * tr[(size_t)e.ib * S.nt]) : e.wa * a;
+            bool found = false;
+            for (InitEntry &q : cells)
+                if (q.gx == e.gx && q.gz == e.gz && q.comp == e.comp) {
+                    q.val += c;
+                    found = true;
+                    break;
+                }
+            if (!found) cells.push_back(InitEntry{e.gx, e.gz, e.comp, 0.f + c});
+        }
+        for (InitEntry &q : cells) {
+            const size_t mi = (size_t)(S.x0 + q.gx) * M.nz + q.gz;
+            const double rho = M.host[2 * (size_t)M.nx * M.nz + mi];
+            q.val = (float)((double)q.val * (0.5 * (double)P.par.dt * (double)P.par.dt / rho));
+            ent.push_back(q);
+        }
+        off[s + 1] = (int)ent.size();
+    }
+}
+
+static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
+{
+    const ModelState &M = ctx->M;
+    const bool adj = mode == 2;
+    const bool store = mode == 1;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+    long long n = 0;
+    for (auto &S : P.shots) {
+        CK(cudaMemsetAsync(S->u0.p, 0, S->u0.n, ctx->st));
+        CK(cudaMemsetAsync(S->u1.p, 0, S->u1.n, ctx->st));
+        if (adj) CK(cudaMemsetAsync(S->grad.p, 0, S->grad.n, ctx->st));
+        if (store && S->amax.p) CK(cudaMemsetAsync(S->amax.p, 0, S->amax.n, ctx->st));
+    }
+    const ShotDev *shots = (adj ? P.d_shots_a : P.d_shots_f).as<ShotDev>();
+    const int nshots = (int)P.shots.size();
+    launch_scatter_init(shots, nshots, P.d_init.as<InitEntry>(), P.d_init_off.as<int>(), ctx->st);
+    n++;
+    int flags = 0;
+    if (adj) flags = STEP_GRAD;
+    else {
+        flags = STEP_EXTRACT;
+        if (store) {
+            flags |= STEP_STORE;
+            if (P.par.snapshot_precision != FWI2D_SNAP_FP32) flags |= STEP_AMAX;
+        }
+    }
+    const ModelDev md = M.dev();
+    for (int it = 0; it < P.nt_max - 1; it++) {
+        launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
+                            it, flags, P.dtg, ctx->st);
+        n++;
+    }
+    if (!adj) {
+        launch_finalize(shots, nshots, P.C, 2, STEP_EXTRACT | (store ? STEP_STORE : 0), ctx->st);
+        n++;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamEndCapture(ctx->st, &g));
+    cudaGraphExec_t ge;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    P.graph[mode] = ge;
+    P.launches[mode] = n;
+}
+
+static Plan &need_plan(fwi2d_ctx *ctx)
+{
+    if (!ctx->plan) throw Error(FWI2D_ERR_STATE, "fwi2d_set_shots must be called first");
+    return *ctx->plan;
+}
+
+// traces: concatenated per-shot blocks [rows][nt]
+static void upload_traces(fwi2d_ctx *ctx, const float *traces, bool adjoint)
+{
+    Plan &P = need_plan(ctx);
+    REQ(traces != nullptr, "null trace array");
+    set_device(ctx);
+    size_t maxn = 0;
+    for (auto &S : P.shots) maxn = std::max(maxn, (size_t)S->nt * (adjoint ? S->nrcv_rows : S->nsrc_rows));
+    if (P.d_stage.n < maxn * sizeof(float)) P.d_stage.alloc(maxn * sizeof(float));
+    std::vector<const float *> blocks;
+    const float *p = traces;
+    for (auto &S : P.shots) {
+        const int rows = adjoint ? S->nrcv_rows : S->nsrc_rows;
+        const size_t n = (size_t)rows * S->nt;
+        for (size_t i = 0; i < n; i++)
+            if (!std::isfinite(p[i])) throw Error(FWI2D_ERR_ARG, "trace array holds a non-finite value");
+        CK(cudaMemcpyAsync(P.d_stage.p, p, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        launch_to_time_major(P.d_stage.as<float>(), (adjoint ? S->src_a : S->src_f).as<float>(), rows, S->nt, ctx->st);
+        CK(cudaGetLastError());
+        blocks.push_back(p);
+        p += n;
+    }
+    std::vector<InitEntry> ent;
+    std::vector<int> off;
+    compute_init(ctx->M, P, adjoint, blocks.data(), ent, off);
+    REQ(ent.size() <= P.init_cap, "internal: initial-state table overflow");
+    if (!ent.empty())
+        CK(cudaMemcpyAsync(P.d_init.p, ent.data(), ent.size() * sizeof(InitEntry), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(P.d_init_off.p, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));   // host arrays above are temporaries
+}
+
+static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
+{
+    Plan &P = need_plan(ctx);
+    set_device(ctx);
+    if (adjoint) {
+        if (!P.have_snapshots || !P.snapshots_valid)
+            throw Error(FWI2D_ERR_STATE, "the adjoint needs a forward pass that stored snapshots (sub > 0)");
+    }
+    if (store && !P.have_snapshots) throw Error(FWI2D_ERR_ARG, "snapshots requested with sub = 0");
+    const int mode = adjoint ? 2 : (store ? 1 : 0);
+    if (!P.graph[mode]) capture(ctx, P, mode);
+    CK(cudaGraphLaunch(P.graph[mode], ctx->st));
+    if (adjoint) {
+        CK(cudaMemsetAsync(P.d_grad_full.p, 0, P.d_grad_full.n, ctx->st));
+        for (auto &S : P.shots)
+            launch_add_subgrid(P.d_grad_full.as<float>(), S->grad.as<float>(), P.ncompg, S->x0, S->nx, ctx->M.ldz,
+                               (long long)ctx->M.nx * ctx->M.ldz, ctx->st);
+        CK(cudaGetLastError());
+    } else if (store) {
+        P.snapshots_valid = true;
+    }
+}
+
+static void download_rcv(fwi2d_ctx *ctx, float *rcv)
+{
+    Plan &P = need_plan(ctx);
+    size_t maxn = 0;
+    for (auto &S : P.shots) maxn = std::max(maxn, (size_t)S->nt * S->nrcv_rows);
+    if (P.d_stage.n < maxn * sizeof(float)) P.d_stage.alloc(maxn * sizeof(float));
+    float *p = rcv;
+    for (auto &S : P.shots) {
+        const size_t n = (size_t)S->nrcv_rows * S->nt;
+        launch_from_time_major(S->rcv_f.as<float>(), P.d_stage.as<float>(), S->nrcv_rows, S->nt, ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(p, P.d_stage.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        p += n;
+    }
+}
+
+static void download_grad(fwi2d_ctx *ctx, float *grad)
+{
+    Plan &P = need_plan(ctx);
+    const ModelState &M = ctx->M;
+    const size_t n = (size_t)P.ncompg * M.nx * M.nz;
+    if (P.d_stage.n < n * sizeof(float)) P.d_stage.alloc(n * sizeof(float));
+    k_unpitch<<<592, 256, 0, ctx->st>>>(P.d_grad_full.as<float>(), P.d_stage.as<float>(), (long long)P.ncompg * M.nx,
+                                        M.nz, M.ldz);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(grad, P.d_stage.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+}
+
+
+// Host snapshots [nslot][ncomp][nx][nz] (fp32) -> the device store of shot 0.
+static void load_host_snapshots(fwi2d_ctx *ctx, const float *full)
+{
+    Plan &P = need_plan(ctx);
+    REQ(P.par.snapshot_precision == FWI2D_SNAP_FP32, "host snapshots are fp32");
+    ShotPlan &S = *P.shots[0];
+    const ModelState &M = ctx->M;
+    const size_t rows = (size_t)S.ncomp * S.nx;
+    const size_t slot_in = rows * M.nz, slot_out = rows * M.ldz;
+    if (P.d_stage.n < slot_in * sizeof(float)) P.d_stage.alloc(slot_in * sizeof(float));
+    for (int k = 0; k < S.nslot; k++) {
+        CK(cudaMemcpyAsync(P.d_stage.p, full + (size_t)k * slot_in, slot_in * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->st));
+        k_pitch<<<592, 256, 0, ctx->st>>>(P.d_stage.as<float>(), S.snap.as<float>() + (size_t)k * slot_out,
+                                          (long long)rows, M.nz, M.ldz);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    P.snapshots_valid = true;
+}
+
+static void store_host_snapshots(fwi2d_ctx *ctx, float *full)
+{
+    Plan &P = need_plan(ctx);
+    ShotPlan &S = *P.shots[0];
+    const ModelState &M = ctx->M;
+    const size_t rows = (size_t)S.ncomp * S.nx;
+    const size_t slot_in = rows * M.ldz, slot_out = rows * M.nz;
+    if (P.d_stage.n < slot_out * sizeof(float)) P.d_stage.alloc(slot_out * sizeof(float));
+    // the reference writes slots it/sub for it in [0, nt-1]; later slots stay untouched
+    const int written = (S.nt - 1) / P.C.sub + 1;
+    for (int k = 0; k < std::min(written, S.nslot); k++) {
+        k_unpitch<<<592, 256, 0, ctx->st>>>(S.snap.as<float>() + (size_t)k * slot_in, P.d_stage.as<float>(),
+                                            (long long)rows, M.nz, M.ldz);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(full + (size_t)k * slot_out, P.d_stage.p, slot_out * sizeof(float), cudaMemcpyDeviceToHost,
+                           ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+}
+
+static fwi2d_ctx *thread_ctx(int device)
+{
+    static thread_local std::vector<std::unique_ptr<fwi2d_ctx, int (*)(fwi2d_ctx *)>> pool;
+    for (auto &c : pool)
+        if (c->device == device) return c.get();
+    fwi2d_ctx *c = nullptr;
+    int rc = fwi2d_ctx_create(device, &c);
+    if (rc != FWI2D_OK) throw Error(rc, g_err);
+    pool.emplace_back(c, fwi2d_ctx_destroy);
+    return c;
+}
+
+}  // namespace fwi2d
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace fwi2d;
+
+#define ABI_TRY try {
+#define ABI_END                                   \
+    }                                             \
+    catch (const Error &e)                        \
+    {                                             \
+        g_err = e.what();                         \
+        return e.code;                            \
+    }                                             \
+    catch (const std::bad_alloc &)                \
+    {                                             \
+        g_err = "host memory exhausted";          \
+        return FWI2D_ERR_OOM;                     \
+    }                                             \
+    catch (const std::exception &e)               \
+    {                                             \
+        g_err = e.what();                         \
+        return FWI2D_ERR_ARG;                     \
+    }                                             \
+    return FWI2D_OK;
+
+extern "C" {
+
+const char *fwi2d_last_error(void) { return g_err.c_str(); }
+
+int fwi2d_version(void) { return 100; }
+
+int fwi2d_injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz, float dx,
+                           float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw)
+{
+    ABI_TRY
+    REQ(type == FWI2D_INJ_DELTA || type == FWI2D_INJ_DDELTA, "unknown injector type");
+    REQ(ntr >= 0 && nx >= 3 && nz >= 3 && dx > 0 && dz > 0, "invalid grid");
+    REQ(ntr == 0 || (locx && locz && xind && zind && xw && zw), "null array");
+    injector_weights(type, ntr, locx, locz, nx, nz, dx, dz, ox, oz, xind, zind, xw, zw);
+    ABI_END
+}
+
+int fwi2d_ctx_create(int device, fwi2d_ctx **out)
+{
+    ABI_TRY
+    REQ(out != nullptr, "null output pointer");
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    REQ(device >= 0 && device < n, "no such CUDA device");
+    auto c = std::make_unique<fwi2d_ctx>();
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    const SbpTables &t = sbp_tables();
+    upload_sbp_tables(&t.b1[0][0], &t.b2[0][0][0], t.c2, t.c1, t.sc, t.hc);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = c.release();
+    ABI_END
+}
+
+int fwi2d_ctx_destroy(fwi2d_ctx *ctx)
+{
+    ABI_TRY
+    if (!ctx) return FWI2D_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->st);
+    ctx->plan.reset();
+    cudaStreamDestroy(ctx->st);
+    delete ctx;
+    ABI_END
+}
+
+int fwi2d_set_model(fwi2d_ctx *ctx, int kind, int nx, int nz, float dx, float dz, const float *model)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    set_model(ctx, kind, nx, nz, dx, dz, model);
+    ABI_END
+}
+
+int fwi2d_set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    set_shots(ctx, par, nshots, shots);
+    ABI_END
+}
+
+int fwi2d_forward(fwi2d_ctx *ctx, const float *src, float *rcv, int store_snapshots)
+{
+    ABI_TRY
+    REQ(ctx && rcv, "null argument");
+    upload_traces(ctx, src, false);
+    run(ctx, false, store_snapshots != 0);
+    download_rcv(ctx, rcv);
+    ABI_END
+}
+
+int fwi2d_adjoint(fwi2d_ctx *ctx, const float *adj, float *grad)
+{
+    ABI_TRY
+    REQ(ctx && grad, "null argument");
+    upload_traces(ctx, adj, true);
+    run(ctx, true, false);
+    download_grad(ctx, grad);
+    ABI_END
+}
+
+int fwi2d_upload_traces(fwi2d_ctx *ctx, const float *traces, int adjoint)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    upload_traces(ctx, traces, adjoint != 0);
+    ABI_END
+}
+
+int fwi2d_run(fwi2d_ctx *ctx, int adjoint, int store_snapshots)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    run(ctx, adjoint != 0, store_snapshots != 0);
+    ABI_END
+}
+
+int fwi2d_sync(fwi2d_ctx *ctx)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    set_device(ctx);
+    CK(cudaStreamSynchronize(ctx->st));
+    ABI_END
+}
+
+int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out)
+{
+    ABI_TRY
+    REQ(ctx && out, "null argument");
+    Plan &P = need_plan(ctx);
+    REQ(shot >= 0 && shot < (int)P.shots.size(), "no such shot");
+    ShotPlan &S = *P.shots[shot];
+    REQ(P.have_snapshots && slot >= 0 && slot < S.nslot, "no such snapshot");
+    set_device(ctx);
+    const ModelState &M = ctx->M;
+    const size_t field = (size_t)S.ncomp * S.nx * M.ldz;
+    const int prec = P.par.snapshot_precision;
+    const size_t esz = prec == FWI2D_SNAP_FP32 ? 4 : 2;
+    std::vector<unsigned char> raw(field * esz);
+    CK(cudaMemcpyAsync(raw.data(), (const char *)S.snap.p + (size_t)slot * field * esz, field * esz,
+                       cudaMemcpyDeviceToHost, ctx->st));
+    unsigned amax = 0;
+    if (prec != FWI2D_SNAP_FP32)
+        CK(cudaMemcpyAsync(&amax, S.amax.as<unsigned>() + slot, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    float inv = 1.f;
+    if (prec != FWI2D_SNAP_FP32) {
+        float m;
+        std::memcpy(&m, &amax, 4);
+        if (m > 0.f) inv = 1.f / std::ldexp(1.f, 14 - (std::ilogb(m) + 1));
+    }
+    for (int c = 0; c < S.ncomp; c++)
+        for (int ix = 0; ix < S.nx; ix++)
+            for (int iz = 0; iz < M.nz; iz++) {
+                const size_t i = ((size_t)c * S.nx + ix) * M.ldz + iz;
+                float v;
+                if (prec == FWI2D_SNAP_FP32) std::memcpy(&v, &raw[i * 4], 4);
+                else {
+                    unsigned short h;
+                    std::memcpy(&h, &raw[i * 2], 2);
+                    if (prec == FWI2D_SNAP_BF16) {
+                        unsigned b = (unsigned)h << 16;
+                        std::memcpy(&v, &b, 4);
+                    } else {
+                        // IEEE half -> float
+                        const unsigned sgn = (h >> 15) & 1, ex = (h >> 10) & 31, man = h & 1023;
+                        float f;
+                        if (ex == 0) f = std::ldexp((float)man, -24);
+                        else if (ex == 31) f = man ? NAN : INFINITY;
+                        else f = std::ldexp((float)(man + 1024), (int)ex - 25);
+                        v = sgn ? -f : f;
+                    }
+                    v *= inv;
+                }
+                out[((size_t)c * S.nx + ix) * M.nz + iz] = v;
+            }
+    ABI_END
+}
+
+int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, long long *snap_bytes)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    Plan &P = need_plan(ctx);
+    const long long steps = P.nt_max - 1;
+    if (lf) *lf = steps + 2;
+    if (la) *la = steps + 1 + (long long)P.shots.size();
+    if (shape) *shape = P.shape;
+    if (snap_bytes) *snap_bytes = P.snap_bytes;
+    ABI_END
+}
+
+int fwi2d_tile_shape_count(void) { return elastic_tile_count(); }
+
+int fwi2d_tile_shape(int index, int *tz, int *tx)
+{
+    ABI_TRY
+    REQ(index >= 0 && index < elastic_tile_count() && tz && tx, "no such tile shape");
+    elastic_tile_shape(index, tz, tx);
+    ABI_END
+}
+
+int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, float *allrcv,
+                    const fwi2d_injector *inj, const fwi2d_injector *ext, const fwi2d_injector *inja,
+                    const fwi2d_injector *exta, float *full_wfld, float *grad, const fwi2d_params *par, int ns, int nr,
+                    int nx, int nz, float dx, float dz)
+{
+    ABI_TRY
+    REQ(par && model && inj && ext, "null argument");
+    REQ(kind == FWI2D_ELASTIC || kind == FWI2D_VTI, "fwi2d_propagate: this propagator is not built yet");
+    (void)inja;
+    (void)exta;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    fwi2d_ctx *ctx = thread_ctx(dev);
+    fwi2d_params p = *par;
+    p.snapshot_precision = FWI2D_SNAP_FP32;
+    p.checkpoint_every = 0;
+    const int nt = p.nt;
+    if (adj) REQ(p.sub > 0 && full_wfld && grad, "the adjoint needs snapshots (sub > 0) and a gradient buffer");
+    set_model(ctx, kind, nx, nz, dx, dz, model);
+    // forward: inject the sources, extract the receivers; adjoint: inject the receivers
+    fwi2d_shot sh;
+    std::memset(&sh, 0, sizeof(sh));
+    sh.x0 = 0;
+    sh.nx = nx;
+    sh.nt = nt;
+    sh.src = adj ? *ext : *inj;
+    sh.rcv = adj ? *inj : *ext;
+    if (adj) p.mt = sh.src.type == FWI2D_INJ_DDELTA;
+    const bool store = !adj && p.sub > 0 && full_wfld != nullptr;
+    fwi2d_params pp = p;
+    if (!store && !adj) pp.sub = 0;
+    set_shots(ctx, &pp, 1, &sh);
+    Plan &P = *ctx->plan;
+    ShotPlan &S = *P.shots[0];
+    // gather the component blocks (stride ns*nt / nr*nt in the reference's buffers)
+    const int in_ntr = adj ? S.nr : S.ntr_src;
+    const int in_comp = adj ? 2 : S.ncomp_src;
+    const int stride = adj ? nr : ns;
+    std::vector<float> in((size_t)in_comp * in_ntr * nt);
+    for (int c = 0; c < in_comp; c++)
+        for (int t = 0; t < in_ntr; t++)
+            std::memcpy(&in[((size_t)c * in_ntr + t) * nt], allsrc + ((size_t)c * stride + t) * nt, nt * sizeof(float));
+    if (!adj) {
+        std::vector<float> out((size_t)2 * S.nr * nt);
+        upload_traces(ctx, in.data(), false);
+        run(ctx, false, store);
+        download_rcv(ctx, out.data());
+        for (int c = 0; c < 2; c++)
+            for (int t = 0; t < S.nr; t++) {
+                float *dst = allrcv + ((size_t)c * nr + t) * nt;
+                const float *src = &out[((size_t)c * S.nr + t) * nt];
+                for (int k = 0; k < nt; k++) dst[k] += src[k];
+            }
+        if (store) store_host_snapshots(ctx, full_wfld);
+    } else {
+        load_host_snapshots(ctx, full_wfld);
+        std::vector<float> g((size_t)3 * nx * nz);
+        upload_traces(ctx, in.data(), true);
+        run(ctx, true, false);
+        download_grad(ctx, g.data());
+        for (size_t i = 0; i < g.size(); i++) grad[i] += g[i];
+    }
+    ABI_END
+}
+
+}  // extern "C"

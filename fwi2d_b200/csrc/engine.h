@@ -1,0 +1,100 @@
+// Device-side data structures shared by the propagation kernels and the host
+// engine.  Layouts follow the reference (src/cpp/we_op.cpp:564-902): every
+// 2-D array is x-major with z contiguous, a[ix*ldz + iz]; ldz is nz rounded
+// up to a multiple of 32 so that each x-row starts on a 128-byte boundary.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fwi2d {
+
+enum Kind { KIND_ELASTIC = 0, KIND_VTI = 1, KIND_ACOUSTIC = 2, KIND_AE = 3 };
+enum SnapPrec { SNAP_FP32 = 0, SNAP_BF16 = 1, SNAP_FP16 = 2 };
+
+// One injection contribution to one cell.  delta_m3: out += wa*S[ia];
+// ddelta_m3 (moment tensor): out += wa*S[ia] - wb*S[ib]  (injector.cpp:91-112, 214-239).
+struct InjEntry {
+    int gx, gz;       // cell on the shot's grid
+    int comp;         // field component (0: x / potential, 1: z)
+    int mt;           // 1 for the moment-tensor form
+    int ia, ib;       // rows of the time-major source block
+    float wa, wb;     // xw*zw products (reference order)
+};
+
+// One receiver sample: o = sum_{i,k} w[3i+k] * u[gx0+i][gz0+k]  (injector.cpp:68-89).
+struct ExtEntry {
+    int row;          // output row in the time-major trace block
+    int comp;         // field component read
+    int gx0, gz0;     // first of the 3x3 cells
+    float w[9];
+};
+
+// Initial-state scatter: u[comp][gx][gz] = val (precomputed on the host in the
+// reference's double arithmetic, we_op.cpp:657-663).
+struct InitEntry {
+    int gx, gz, comp;
+    float val;
+};
+
+struct ShotDev {
+    int nx, nz, ldz;      // shot grid (nz == model nz)
+    int x0;               // first model column of this shot's grid
+    int nt;               // time samples of this shot
+    int tiles_x, tiles_z;
+    float *u[2];          // two field buffers, each [ncomp][nx][ldz]
+    const float *src;     // time-major injection traces [nt][nsrc]
+    int nsrc;
+    float *rcv;           // time-major extraction output [nt][nrcv]
+    int nrcv;
+    const InjEntry *inj;  // sorted by (tile, cell, trace)
+    const int *inj_off;   // [tiles+1]
+    const ExtEntry *ext;
+    const int *ext_off;   // [tiles+1]
+    const float *den;     // absorbing-boundary divisors: [ncomp][2*nx + 2*nz] (top, bottom, left, right)
+    const float *tz;      // taper factor along z [nz]
+    const float *tx;      // taper factor along x [nx]
+    void *snap;           // snapshots [nslot][ncomp][nx][ldz] in fp32/bf16/fp16
+    long long snap_slot;  // elements per slot
+    float *snap_inv;      // per-slot dequantisation factor (16-bit snapshots)
+    unsigned *snap_amax;  // per-slot max |u| bits (16-bit snapshots)
+    float *grad;          // [3 or 2][nx][ldz] gradient accumulator of this shot
+    float *gcomp;         // compensation terms (compensated accumulation) or nullptr
+    float *halo_save;     // interface scratch (acoustic-elastic) or nullptr
+    const float *gwt;     // gradient time-damping weight per snapshot index
+};
+
+// Model on the full grid; shots index it at column x0 + ix.
+struct ModelDev {
+    int nx, nz, ldz;
+    const float *p0, *p1, *p2;   // elastic: lambda, mu, rho.  acoustic: K, 1/rho
+    const float *c13, *eps;      // VTI
+    const float *fxx;            // VTI: (1+2eps)*2mu ; elastic: unused
+    const float *lbis;           // VTI: (1+2eps)*lambda
+    const float *gv2, *gv3;      // VTI gradient: dC13/dlambda, dC13/dmu
+};
+
+// Scalars of one propagation, each computed on the host exactly as the
+// reference computes it (float arithmetic unless noted).
+struct StepConst {
+    float dt, dt2;               // dt, dt*dt
+    float inv_d2x, inv_d2z;      // 1/(dx*dx), 1/(dz*dz)       (Dxx_var/Dzz_var a/d2)
+    float adx, adz;              // 1/dx, 1/dz                 (mult_Dx/mult_Dz a/d)
+    float sdx, sdz;              // (float)(1.0/(double)d)     (Dx/Dz interior scale)
+    float dx, dz;
+    float d2x, d2z;              // dx*dx, dz*dz
+    float sat_x, sat_z;          // 1/(dx*h0), 1/(dz*h0)       (esat_* a/(d*h0))
+    float nsat_x, nsat_z;        // 1/(dx*dx*h0), 1/(dz*dz*h0) (esat_D* a/(d*d*h0))
+    float alpha;                 // acoustic free-surface stiffness factor
+    int bc[4];                   // top, bottom, left, right
+    int sub;
+    int snap_prec;
+    int nslot;
+    int kahan;                   // compensated gradient accumulation
+};
+
+// Per-launch tile table entry.
+struct TileRef {
+    int shot, tx, tz, pad;
+};
+
+}  // namespace fwi2d

@@ -1,0 +1,33 @@
+// Host entry points of the kernels in kernels.cu / acoustic.cu.
+#pragma once
+#include "engine.h"
+
+namespace fwi2d {
+
+enum StepFlagBits { STEP_STORE = 1, STEP_EXTRACT = 2, STEP_AMAX = 4, STEP_GRAD = 8 };
+
+void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const float *c1, const float *sc,
+                       const float *hc);
+
+int elastic_tile_count();
+void elastic_tile_shape(int i, int *tz, int *tx);
+void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
+                         const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+void launch_scatter_init(const ShotDev *shots, int nshots, const InitEntry *ent, const int *off, cudaStream_t st);
+void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st);
+
+// acoustic.cu
+int acoustic_tile_count();
+void acoustic_tile_shape(int i, int *tz, int *tx);
+void launch_acoustic_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+void launch_acoustic_final_grad(const ShotDev *shots, int nshots, const ModelDev &M, const StepConst &C, float dtg,
+                                cudaStream_t st);
+
+// layout helpers (engine.cu)
+void launch_to_time_major(const float *in, float *out, int rows, int nt, cudaStream_t st);
+void launch_from_time_major(const float *in, float *out, int rows, int nt, cudaStream_t st);
+void launch_add_subgrid(float *full, const float *part, int ncomp, int x0, int nx, int ldz, long long full_comp,
+                        cudaStream_t st);
+
+}  // namespace fwi2d

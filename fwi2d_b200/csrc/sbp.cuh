@@ -1,0 +1,139 @@
+// SBP operator building blocks on shared-memory tiles.
+//
+// Every routine restates one reference operator at a single sample, in the
+// same single-precision operation order (this library is compiled with
+// --fmad=false so that no multiply-add is contracted):
+//   d1    Dx/Dz              src/cpp/spatial_operators.cpp:100-154 + .ispc:7-25
+//   md1   mult_Dx/mult_Dz    src/cpp/spatial_operators.cpp:156-210 + .ispc:27-45
+//   d2acc Dxx_var/Dzz_var    src/include/spatial_operators.hpp:31-156
+//   tsum / nsum              the boundary sums of esat_* (spatial_operators.hpp:160-727)
+// A pointer `p` addresses the sample being evaluated inside a tile, `st` is
+// the tile stride along the derivative axis, `g` the global index of the
+// sample on that axis and `n` the axis length.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace fwi2d {
+
+// Coefficient tables, one copy in the single translation unit that holds the
+// kernels (kernels.cu); upload_sbp_tables() fills them per device from the
+// same rationals as the reference's initialisers.
+static __constant__ float kB1[4][6];      // first-derivative boundary closure
+static __constant__ float kB2[6][8][8];   // variable-coefficient second-derivative closure
+static __constant__ float kC2[10];        // its interior weights
+static __constant__ float kC1[2];         // 2/3, -1/12
+static __constant__ float kSC[4];         // one-sided boundary derivative 11/6, -3, 3/2, -1/3
+static __constant__ float kHC[4];         // H-norm boundary weights 17/48, 59/48, 43/48, 49/48
+
+__device__ __forceinline__ float d1(const float *p, int st, int g, int n, float d, float scale)
+{
+    if (g < 4) {
+        const float *b = p - g * st;
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) s += kB1[g][k] * b[k * st];
+        return s / d;
+    }
+    if (g >= n - 4) {
+        const int r = n - 1 - g;
+        const float *b = p + r * st;
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) s -= kB1[r][k] * b[-k * st];
+        return s / d;
+    }
+    return scale * (kC1[0] * (p[st] - p[-st]) + kC1[1] * (p[2 * st] - p[-2 * st]));
+}
+
+__device__ __forceinline__ float md1(const float *p, const float *q, int st, int g, int n, float ad)
+{
+    if (g < 4) {
+        const float *b = p - g * st, *c = q - g * st;
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) s += kB1[g][k] * b[k * st] * c[k * st];
+        return ad * s;
+    }
+    if (g >= n - 4) {
+        const int r = n - 1 - g;
+        const float *b = p + r * st, *c = q + r * st;
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) s -= kB1[r][k] * b[-k * st] * c[-k * st];
+        return ad * s;
+    }
+    return ad * (kC1[0] * (p[st] * q[st] - p[-st] * q[-st]) + kC1[1] * (p[2 * st] * q[2 * st] - p[-2 * st] * q[-2 * st]));
+}
+
+// acc += D2(f, u) at one sample.  fs scales every coefficient sample
+// (1 or exactly 2: the reference's expr4b = 2*mu is an exact doubling).
+__device__ __forceinline__ void d2acc(float &acc, const float *pu, int su, const float *pf, int sf, float fs,
+                                      int g, int n, float invd2, float d2)
+{
+    if (g < 6 || g >= n - 6) {
+        const bool top = g < 6;
+        const int r = top ? g : n - 1 - g;
+        const int dir = top ? 1 : -1;
+        const float *bu = top ? pu - g * su : pu + r * su;
+        const float *bf = top ? pf - g * sf : pf + r * sf;
+        float fk[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) fk[k] = fs * bf[dir * k * sf];
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+            float val = 0.f;
+#pragma unroll
+            for (int k = 0; k < 8; k++) val += kB2[r][jj][k] * fk[k];
+            acc += val * bu[dir * jj * su] / d2;
+        }
+        return;
+    }
+    const float fm2 = fs * pf[-2 * sf], fm1 = fs * pf[-sf], f0 = fs * pf[0], fp1 = fs * pf[sf], fp2 = fs * pf[2 * sf];
+    const float um2 = pu[-2 * su], um1 = pu[-su], u0 = pu[0], up1 = pu[su], up2 = pu[2 * su];
+    acc = acc + invd2 * ((kC2[0] * f0 + kC2[1] * (fm1 + fp1) + kC2[2] * (fm2 + fp2)) * u0
+                       + (kC2[3] * fm2 + kC2[4] * fm1 + kC2[5] * f0 + kC2[6] * fp1) * um1
+                       + (kC2[3] * fp2 + kC2[4] * fp1 + kC2[5] * f0 + kC2[6] * fm1) * up1
+                       + (kC2[7] * fm2 + kC2[8] * fm1 + kC2[9] * f0) * um2
+                       + (kC2[7] * fp2 + kC2[8] * fp1 + kC2[9] * f0) * up2);
+}
+
+// Tangential first-derivative sum along a boundary line (no division by d).
+__device__ __forceinline__ float tsum(const float *p, int st, int g, int n)
+{
+    float s = 0.f;
+    if (g < 4) {
+        const float *b = p - g * st;
+#pragma unroll
+        for (int j = 0; j < 6; j++) s += kB1[g][j] * b[j * st];
+    } else if (g >= n - 4) {
+        const int r = n - 1 - g;
+        const float *b = p + r * st;
+#pragma unroll
+        for (int j = 0; j < 6; j++) s -= kB1[r][j] * b[-j * st];
+    } else {
+        s += kC1[0] * (p[st] - p[-st]);
+        s += kC1[1] * (p[2 * st] - p[-2 * st]);
+    }
+    return s;
+}
+
+// One-sided outward derivative sum S.u at a boundary sample; `in` is the
+// stride pointing into the domain.
+__device__ __forceinline__ float nsum(const float *p, int in)
+{
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) s += kSC[k] * p[k * in];
+    return s;
+}
+
+// -(D u)_0 at a boundary sample: the sum of esat_Dz_top & co.
+__device__ __forceinline__ float ndsum(const float *p, int in)
+{
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 6; j++) s -= kB1[0][j] * p[j * in];
+    return s;
+}
+
+}  // namespace fwi2d

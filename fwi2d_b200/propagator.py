@@ -1,0 +1,172 @@
+"""Python front end of the C ABI: a batch of shots on one device.
+
+Mirrors the per-shot contract of the reference's ``propagate``
+(src/cpp/we_op.cpp:564): the model is already converted (``convert_model``),
+traces are ``[ncomp][ntr][nt]`` per shot, gradients are the raw imaging
+condition before the H quadrature and the chain rule.
+"""
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _capi as C
+
+PARAM_DEFAULTS = dict(
+    nt=0, sub=1, dt=0.0, bc_top=1, bc_bottom=1, bc_left=1, bc_right=1,
+    taper_top=0, taper_bottom=0, taper_left=0, taper_right=0, taper_strength=0.05,
+    free_surface_stiffness=1.05, mt=0, gdamp_tmin=0.0, gdamp_tmax=0.0, gdamp_power=1.0,
+    nza=0, water_velocity=1.5, water_density=1.0, acoustic_source=1,
+    snapshot_precision=C.SNAP_FP32, checkpoint_every=0, compensated=0, tile_shape=-1,
+)
+
+
+def make_params(**kw):
+    d = dict(PARAM_DEFAULTS)
+    unknown = set(kw) - set(d)
+    if unknown:
+        raise KeyError("unknown parameters: %s" % sorted(unknown))
+    d.update(kw)
+    p = C.Params()
+    for k, v in d.items():
+        setattr(p, k, v)
+    return p
+
+
+def injector_tables(itype, locx, locz, nx, nz, dx, dz, ox, oz):
+    """delta_m3 / ddelta_m3 tables computed by the library (host side)."""
+    L = C.load()
+    locx = np.ascontiguousarray(locx, np.float32)
+    locz = np.ascontiguousarray(locz, np.float32)
+    n = len(locx)
+    w = 3 if itype == C.INJ_DELTA else 6
+    xind = np.zeros((n, 3), np.int32)
+    zind = np.zeros((n, 3), np.int32)
+    xw = np.zeros((n, 2, w), np.float32)
+    zw = np.zeros((n, 2, w), np.float32)
+    C.check(L.fwi2d_injector_weights(itype, n, C.ptr(locx), C.ptr(locz), nx, nz, float(dx), float(dz), float(ox),
+                                     float(oz), C.ptr(xind), C.ptr(zind), C.ptr(xw), C.ptr(zw)))
+    return xind, zind, xw, zw
+
+
+def _injector(itype, tabs):
+    if tabs is None:
+        return C.Injector(0, 0, None, None, None, None)
+    xind, zind, xw, zw = tabs
+    return C.Injector(itype, len(xind), C.ptr(xind), C.ptr(zind), C.ptr(xw), C.ptr(zw))
+
+
+@dataclass
+class ShotSpec:
+    """One shot: its grid is model columns [x0, x0+nx); locations in km
+    relative to the model origin (ox, oz)."""
+    x0: int
+    nx: int
+    nt: int
+    src_x: Sequence[float]
+    src_z: Sequence[float]
+    rcv_x: Sequence[float]
+    rcv_z: Sequence[float]
+    mt: bool = False
+
+
+class Propagator:
+    """One device context: model, batch plan, forward and adjoint passes."""
+
+    def __init__(self, device=0):
+        self.L = C.load()
+        h = ctypes.c_void_p()
+        C.check(self.L.fwi2d_ctx_create(int(device), ctypes.byref(h)))
+        self.h = h
+        self.kind = None
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            self.L.fwi2d_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_model(self, kind, model, dx, dz, ox=0.0, oz=0.0):
+        m = np.ascontiguousarray(model, np.float32)
+        npar, nx, nz = m.shape
+        C.check(self.L.fwi2d_set_model(self.h, kind, nx, nz, float(dx), float(dz), C.ptr(m)))
+        self.kind, self.nx, self.nz, self.dx, self.dz, self.ox, self.oz = kind, nx, nz, dx, dz, ox, oz
+
+    def set_shots(self, params, shots: List[ShotSpec]):
+        self.params = params
+        self.shots = shots
+        arr = (C.Shot * len(shots))()
+        keep = []
+        self.src_rows, self.rcv_rows = [], []
+        for i, s in enumerate(shots):
+            ox = self.ox + s.x0 * self.dx
+            st = C.INJ_DDELTA if s.mt else C.INJ_DELTA
+            src = injector_tables(st, s.src_x, s.src_z, s.nx, self.nz, self.dx, self.dz, ox, self.oz)
+            rcv = injector_tables(C.INJ_DELTA, s.rcv_x, s.rcv_z, s.nx, self.nz, self.dx, self.dz, ox, self.oz)
+            keep += [src, rcv]
+            arr[i] = C.Shot(s.x0, s.nx, s.nt, _injector(st, src), _injector(C.INJ_DELTA, rcv),
+                            _injector(0, None), _injector(0, None))
+            nsrc = len(s.src_x)
+            self.src_rows.append((3 if s.mt else 2) * nsrc)
+            self.rcv_rows.append(2 * len(s.rcv_x))
+        C.check(self.L.fwi2d_set_shots(self.h, ctypes.byref(params), len(shots), arr))
+        self._keep = keep
+
+    # -- host API ---------------------------------------------------------
+    def _concat(self, blocks, rows):
+        parts = []
+        for b, r, s in zip(blocks, rows, self.shots):
+            b = np.asarray(b, np.float32).reshape(r, s.nt)
+            parts.append(b.ravel())
+        return np.ascontiguousarray(np.concatenate(parts))
+
+    def forward(self, src_blocks, store=True):
+        """src_blocks[s]: [ncomp][ntr][nt] traces of shot s.  Returns the
+        receiver blocks [2][nr][nt] per shot."""
+        src = self._concat(src_blocks, self.src_rows)
+        out = np.zeros(sum(r * s.nt for r, s in zip(self.rcv_rows, self.shots)), np.float32)
+        C.check(self.L.fwi2d_forward(self.h, C.ptr(src), C.ptr(out), 1 if store else 0))
+        res, o = [], 0
+        for r, s in zip(self.rcv_rows, self.shots):
+            res.append(out[o:o + r * s.nt].reshape(2, r // 2, s.nt))
+            o += r * s.nt
+        return res
+
+    def adjoint(self, adj_blocks):
+        """adj_blocks[s]: [2][nr][nt] adjoint sources of shot s.  Returns the
+        raw (lambda, mu, rho) imaging condition summed over shots."""
+        adj = self._concat(adj_blocks, self.rcv_rows)
+        g = np.zeros((3, self.nx, self.nz), np.float32)
+        C.check(self.L.fwi2d_adjoint(self.h, C.ptr(adj), C.ptr(g)))
+        return g
+
+    def snapshot(self, shot, slot):
+        s = self.shots[shot]
+        out = np.zeros((2, s.nx, self.nz), np.float32)
+        C.check(self.L.fwi2d_snapshot(self.h, shot, slot, C.ptr(out)))
+        return out
+
+    # -- device-resident API ----------------------------------------------
+    def upload(self, blocks, adjoint):
+        rows = self.rcv_rows if adjoint else self.src_rows
+        buf = self._concat(blocks, rows)
+        C.check(self.L.fwi2d_upload_traces(self.h, C.ptr(buf), 1 if adjoint else 0))
+
+    def run(self, adjoint, store=True):
+        C.check(self.L.fwi2d_run(self.h, 1 if adjoint else 0, 1 if store else 0))
+
+    def sync(self):
+        C.check(self.L.fwi2d_sync(self.h))
+
+    def plan_info(self):
+        lf, la, sh, sb = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int(), ctypes.c_longlong()
+        C.check(self.L.fwi2d_plan_info(self.h, ctypes.byref(lf), ctypes.byref(la), ctypes.byref(sh), ctypes.byref(sb)))
+        return dict(launches_forward=lf.value, launches_adjoint=la.value, tile_shape=sh.value,
+                    snapshot_bytes=sb.value)

@@ -1,0 +1,156 @@
+/*
+ * fwi2d_b200 -- C ABI of the B200 (sm_100a) SBP propagation library.
+ *
+ * The library replaces the GPU hook of the reference's wave-equation
+ * operators: nl_we_op_e::propagate_gpu / nl_we_op_vti::propagate_gpu
+ * (src/include/we_op.hpp:82, :174, implemented by src/cuda/cudaWeOp.cpp:10-433,
+ * :436-876) and the hooks the acoustic and acoustic-elastic operators declare
+ * but leave commented out (we_op.hpp:259-260, :339).  Plain pointers and sizes
+ * only; no exception crosses this boundary.  Every function returns
+ * FWI2D_OK (0) or a negative status; fwi2d_last_error() gives the message.
+ *
+ * Array layouts are the reference's (x-major, z fastest, "[ix*nz+iz]"):
+ *   converted model  [npar][nx][nz]   elastic (lambda, mu, rho), VTI (lambda, mu,
+ *                                     rho, c13, eps), acoustic (K, 1/rho)
+ *   traces           [ncomp][ntr][nt] time fastest
+ *   snapshots        [nt/sub+1][ncomp][nx][nz]
+ *   gradient         [3][nx][nz] (lambda, mu, rho) or [2][nx][nz] (K, 1/rho)
+ * Units are the reference's: km, s, km/s, g/cm^3.
+ */
+#ifndef FWI2D_B200_H
+#define FWI2D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FWI2D_OK 0
+#define FWI2D_ERR_ARG (-1)          /* invalid argument, geometry or parameter */
+#define FWI2D_ERR_CUDA (-2)         /* CUDA runtime error */
+#define FWI2D_ERR_OOM (-3)          /* device memory exhausted */
+#define FWI2D_ERR_STATE (-4)        /* call out of order (no model / no shots) */
+#define FWI2D_ERR_UNSUPPORTED (-5)  /* option the kernels do not implement */
+#define FWI2D_ERR_TIMEOUT (-6)      /* a bounded device wait gave up */
+
+/* propagators: nl_we_op_e, nl_we_op_vti, nl_we_op_a, nl_we_op_ae */
+#define FWI2D_ELASTIC 0
+#define FWI2D_VTI 1
+#define FWI2D_ACOUSTIC 2
+#define FWI2D_ACOUSTIC_ELASTIC 3
+
+/* snapshot storage */
+#define FWI2D_SNAP_FP32 0
+#define FWI2D_SNAP_BF16 1
+#define FWI2D_SNAP_FP16 2
+
+/* injector types (src/include/injector.hpp:39, :69) */
+#define FWI2D_INJ_DELTA 0   /* delta_m3: 3x3 discrete delta */
+#define FWI2D_INJ_DDELTA 1  /* ddelta_m3: moment tensor */
+
+/* The fields of the reference's `param` (src/include/param.hpp:8-83) that the
+ * propagation reads, plus the storage options of this library. */
+typedef struct fwi2d_params {
+    int nt, sub;
+    float dt;
+    int bc_top, bc_bottom, bc_left, bc_right;              /* 1 free/rigid, 2 absorbing, 3 Neumann (acoustic) */
+    int taper_top, taper_bottom, taper_left, taper_right;
+    float taper_strength, free_surface_stiffness;
+    int mt;                                                /* moment-tensor source */
+    float gdamp_tmin, gdamp_tmax, gdamp_power;
+    int nza;                                               /* acoustic-elastic: water rows */
+    float water_velocity, water_density;
+    int acoustic_source;                                   /* acoustic-elastic: source in the water */
+    /* library options */
+    int snapshot_precision;                                /* FWI2D_SNAP_* */
+    int checkpoint_every;                                  /* 0: keep snapshots; k>0: recompute from checkpoints every k steps */
+    int compensated;                                       /* compensated (two-level) gradient accumulation */
+    int tile_shape;                                        /* -1: autotuned; else fwi2d_tile_shape index */
+} fwi2d_params;
+
+/* Public tables of the reference's injector (src/include/injector.hpp:9-13). */
+typedef struct fwi2d_injector {
+    int type;           /* FWI2D_INJ_* */
+    int ntr;
+    const int *xind;    /* [ntr][3] */
+    const int *zind;    /* [ntr][3] */
+    const float *xw;    /* [ntr][2][3] (delta) or [ntr][2][6] (moment tensor) */
+    const float *zw;
+} fwi2d_injector;
+
+/* One shot of a batch: its own grid is the model columns [x0, x0+nx). */
+typedef struct fwi2d_shot {
+    int x0, nx;
+    int nt;                     /* time samples of this shot, <= params.nt */
+    fwi2d_injector src;         /* sources on the shot grid */
+    fwi2d_injector rcv;         /* receivers on the shot grid */
+    fwi2d_injector src_water;   /* acoustic-elastic: water-layer source (ntr = 0 if none) */
+    fwi2d_injector rcv_water;   /* acoustic-elastic: water-layer receivers */
+} fwi2d_shot;
+
+typedef struct fwi2d_ctx fwi2d_ctx;
+
+const char *fwi2d_last_error(void);
+int fwi2d_version(void);
+
+/* delta_m3 / ddelta_m3::findIndicesWeights (src/cpp/injector.cpp:3-64, 114-187). */
+int fwi2d_injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz,
+                           float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw);
+
+/* Context: one device, one stream, one model, one batch plan.  Calls on one
+ * context must be serialised by the caller. */
+int fwi2d_ctx_create(int device, fwi2d_ctx **out);
+int fwi2d_ctx_destroy(fwi2d_ctx *ctx);
+
+/* Upload a converted model (host [npar][nx][nz]); the model grid is dx x dz. */
+int fwi2d_set_model(fwi2d_ctx *ctx, int kind, int nx, int nz, float dx, float dz, const float *model);
+
+/* Build the batch plan: per-shot device buffers, tables and CUDA graphs. */
+int fwi2d_set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots);
+
+/* Forward propagation of every shot of the plan (nl_we_op_*::propagate with
+ * adj=false, we_op.cpp:564).  src: concatenated per-shot blocks [ncomp][ntr][nt];
+ * rcv: concatenated per-shot blocks [ncomp][nr][nt], overwritten.  With
+ * store_snapshots the forward wavefields stay on the device for fwi2d_adjoint. */
+int fwi2d_forward(fwi2d_ctx *ctx, const float *src, float *rcv, int store_snapshots);
+
+/* Adjoint propagation with the zero-lag imaging condition (propagate with
+ * adj=true).  adj: concatenated per-shot blocks in the receiver layout;
+ * grad: model-grid gradient [3 or 2][nx][nz], the sum over shots, overwritten. */
+int fwi2d_adjoint(fwi2d_ctx *ctx, const float *adj, float *grad);
+
+/* Device-resident variants: upload traces once (adjoint=0 sources, 1 adjoint
+ * sources), then run the propagation with inputs and outputs left on the
+ * device.  fwi2d_run returns when the work is queued; fwi2d_sync waits. */
+int fwi2d_upload_traces(fwi2d_ctx *ctx, const float *traces, int adjoint);
+int fwi2d_run(fwi2d_ctx *ctx, int adjoint, int store_snapshots);
+int fwi2d_sync(fwi2d_ctx *ctx);
+
+/* Read back one stored snapshot [ncomp][nx][nz] of one shot (dequantised). */
+int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out);
+
+/* Per-plan facts: number of kernel launches of one forward / adjoint pass,
+ * the tile shape in use, snapshot bytes held. */
+int fwi2d_plan_info(fwi2d_ctx *ctx, long long *launches_fwd, long long *launches_adj, int *tile_shape,
+                    long long *snapshot_bytes);
+
+/* Tile shapes offered to the autotuner. */
+int fwi2d_tile_shape_count(void);
+int fwi2d_tile_shape(int index, int *tz, int *tx);
+
+/* Drop-in for propagate_gpu: one shot, host buffers, the reference's argument
+ * meaning (we_op.hpp:82).  ns / nr are the trace counts that separate the
+ * component blocks of allsrc / allrcv (par.ns and par.nr of the reference).
+ * Forward accumulates into allrcv and writes full_wfld when sub > 0; adjoint
+ * reads full_wfld and accumulates the imaging condition into grad.  inja /
+ * exta are the water-layer injector and extractor of the acoustic-elastic
+ * propagator (NULL otherwise). */
+int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, float *allrcv,
+                    const fwi2d_injector *inj, const fwi2d_injector *ext,
+                    const fwi2d_injector *inja, const fwi2d_injector *exta,
+                    float *full_wfld, float *grad, const fwi2d_params *par, int ns, int nr,
+                    int nx, int nz, float dx, float dz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
