@@ -967,7 +967,7 @@ static void propagate_elastic(int vti, int adj, const real *model, const real *a
     }
 
     for (int it = 0; it < nt - 1; it++) {
-        if (sub > 0 && it % sub == 0 && !grad) memcpy(full + (long)(it / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
+        if (full && sub > 0 && it % sub == 0 && !grad) memcpy(full + (long)(it / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
         if (!grad) {
             extract(ext, curr, rcvx, nz, nt, it);
             extract(ext, curr + nxz, rcvz, nz, nt, it);
@@ -1032,7 +1032,7 @@ static void propagate_elastic(int vti, int adj, const real *model, const real *a
         real *b = prev; prev = curr; curr = next; next = b;
     }
 
-    if (sub > 0 && (nt - 1) % sub == 0 && !grad) memcpy(full + (long)((nt - 1) / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
+    if (full && sub > 0 && (nt - 1) % sub == 0 && !grad) memcpy(full + (long)((nt - 1) / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
     if (!grad) {
         extract(ext, curr, rcvx, nz, nt, nt - 1);
         extract(ext, curr + nxz, rcvz, nz, nt, nt - 1);
@@ -1065,7 +1065,7 @@ static void propagate_acoustic(int adj, const real *model, const real *allsrc, r
     for (long i = 0; i < nxz; i++) prev[i] = (real)((double)prev[i] * (0.5 * (double)K[i] * (double)dt * (double)dt));
 
     for (int it = 0; it < nt - 1; it++) {
-        if (sub > 0 && it % sub == 0 && !grad) memcpy(full + (long)(it / sub) * nxz, curr, nxz * sizeof(real));
+        if (full && sub > 0 && it % sub == 0 && !grad) memcpy(full + (long)(it / sub) * nxz, curr, nxz * sizeof(real));
         if (!grad) extract(ext, curr, allrcv, nz, nt, it);
         if (grad && (nt - 1 - it) % sub == 0 && it != 0)
             grad_acoustic(model, full, curr, tmp, grad, par, nx, nz, (nt - 1 - it) / sub, dx, dz, sub * dt);
@@ -1087,7 +1087,7 @@ static void propagate_acoustic(int adj, const real *model, const real *allsrc, r
         taper_all(next, nx, nz, par, 1, 1, 1, 1);
         real *b = prev; prev = curr; curr = next; next = b;
     }
-    if (sub > 0 && (nt - 1) % sub == 0 && !grad) memcpy(full + (long)((nt - 1) / sub) * nxz, curr, nxz * sizeof(real));
+    if (full && sub > 0 && (nt - 1) % sub == 0 && !grad) memcpy(full + (long)((nt - 1) / sub) * nxz, curr, nxz * sizeof(real));
     if (!grad) extract(ext, curr, allrcv, nz, nt, nt - 1);
     if (grad) grad_acoustic(model, full, curr, tmp, grad, par, nx, nz, 0, dx, dz, sub * dt);
     free(u); free(tmp);
@@ -1162,7 +1162,7 @@ static void propagate_ae(int adj, const real *model, const real *allsrc, real *a
     }
 
     for (int it = 0; it < nt - 1; it++) {
-        if (sub > 0 && it % sub == 0 && !grad) memcpy(full + (long)(it / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
+        if (full && sub > 0 && it % sub == 0 && !grad) memcpy(full + (long)(it / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
         if (!grad) {
             if (!adj) {
                 extract(ext, curr, rcvx, nz, nt, it);
@@ -1272,7 +1272,7 @@ static void propagate_ae(int adj, const real *model, const real *allsrc, real *a
         real *ba = preva; preva = curra; curra = nexta; nexta = ba;
         real *b = prev; prev = curr; curr = next; next = b;
     }
-    if (sub > 0 && (nt - 1) % sub == 0 && !grad) memcpy(full + (long)((nt - 1) / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
+    if (full && sub > 0 && (nt - 1) % sub == 0 && !grad) memcpy(full + (long)((nt - 1) / sub) * 2 * nxz, curr, 2 * nxz * sizeof(real));
     if (!grad) {
         if (!adj) {
             extract(ext, curr, rcvx, nz, nt, nt - 1);
