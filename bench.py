@@ -1,0 +1,418 @@
+#!/usr/bin/env python
+"""Benchmark: elastic FWI gradient on B200 (fwi2d_b200) vs the reference CPU path.
+
+One step = one full FWI gradient evaluation of the elastic single-shot
+workload (401 x 801 grid at 5 m, nt = 5001, 400 two-component receivers,
+FP32 snapshots of every time step kept in HBM): forward propagation with
+snapshot storage, residual against observed data, adjoint sources, adjoint
+propagation with the zero-lag imaging condition, H quadrature and chain rule.
+Cell-updates per step: (nt-1) * nx * nz forward + the same adjoint.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config single|batch]
+
+N > 1 runs one process per GPU (torchrun); each rank computes its own shot
+(weak scaling) and the model gradient is summed over ranks with NCCL.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "elastic FWI gradient shots/s + Gcell-updates/s, batched vs plain, 1 B200"
+BYTES_FWD = 36 + 8      # algorithmic bytes per forward cell-update (fields, model, fp32 snapshot store)
+BYTES_ADJ = 68          # adjoint + imaging: fields, model, snapshot read, gradient read-modify-write
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="single", choices=["single", "batch"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx = float(c[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for n, v in zip(names, c[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def build_workload(name, rank, world):
+    from fwi2d_b200 import workloads as W
+    if name == "single":
+        wl = W.elastic_single()
+        if world > 1:   # one shot per rank, sources 60 m apart
+            sh = dict(wl["shots"][0])
+            sh["sx"] = [2.0 + 0.06 * rank]
+            wl["shots"] = [sh]
+    else:
+        wl = W.vti_batch()
+        if world > 1:
+            wl["shots"] = wl["shots"][rank::world]
+    return wl
+
+
+def make_prop(wl, device):
+    import fwi2d_b200 as F
+    from fwi2d_b200 import workloads as W
+    P = F.Propagator(device)
+    kind = wl["kind"]
+    start = W.convert(kind, wl["start"])
+    P.set_model(kind, start, wl["d"], wl["d"])
+    shots = [F.ShotSpec(s["x0"], s["nx"], s["nt"], s["sx"], s["sz"], s["rx"], s["rz"]) for s in wl["shots"]]
+    P.set_shots(F.make_params(**wl["params"]), shots)
+    srcs = [np.ascontiguousarray(wl["src"][:, :, :s["nt"]]) for s in wl["shots"]]
+    return P, start, srcs
+
+
+def observed(wl, device, srcs):
+    """Observed data: the forward of the true model through the same library
+    (seismotype 1: particle velocity)."""
+    import fwi2d_b200 as F
+    from fwi2d_b200 import workloads as W
+    P = F.Propagator(device)
+    kind = wl["kind"]
+    P.set_model(kind, W.convert(kind, wl["true"]), wl["d"], wl["d"])
+    shots = [F.ShotSpec(s["x0"], s["nx"], s["nt"], s["sx"], s["sz"], s["rx"], s["rz"]) for s in wl["shots"]]
+    prm = dict(wl["params"])
+    prm["sub"] = 0
+    P.set_shots(F.make_params(**prm), shots)
+    out = P.forward(srcs, store=False)
+    P.close()
+    obs = []
+    dt = wl["dt"]
+    for u in out:
+        v = np.empty_like(u)
+        v[..., 0] = (u[..., 1] - u[..., 0]) / np.float32(dt)
+        v[..., -1] = (u[..., -1] - u[..., -2]) / np.float32(dt)
+        v[..., 1:-1] = (u[..., 2:] - u[..., :-2]) / np.float32(2 * dt)
+        obs.append(v.astype(np.float32))
+    return obs
+
+
+def cells_per_step(wl):
+    nz = wl["nz"]
+    return sum(2 * (s["nt"] - 1) * s["nx"] * nz for s in wl["shots"])
+
+
+# ---------------------------------------------------------------------------
+# CPU reference timing (reference sources built in oracle/_ref, else the port)
+# ---------------------------------------------------------------------------
+def cpu_sample(wl, nt_sample):
+    """Forward with snapshots + adjoint with imaging on the full grid of the
+    first shot, nt_sample time samples.  Returns (seconds, cell-updates, kind)."""
+    import oracle as O
+    from fwi2d_b200 import workloads as W
+    kind = "reference" if O.have_reference(32) else "port"
+    lib = O.Reference(32) if kind == "reference" else O.Port(32)
+    s = wl["shots"][0]
+    nx, nz, d = s["nx"], wl["nz"], wl["d"]
+    k = wl["kind"]
+    model = W.convert(k, wl["start"])[:, s["x0"]:s["x0"] + nx].copy()
+    p = dict(wl["params"])
+    p.update(nt=nt_sample, ns=1, nr=len(s["rx"]))
+    par = O.make_par(**{kk: v for kk, v in p.items() if kk in dict(O.Par._fields_)})
+    src = np.ascontiguousarray(wl["src"][:, :, :nt_sample])
+    ox = s["x0"] * d
+    sl = (np.array(s["sx"], np.float32) - ox, np.array(s["sz"], np.float32))
+    rl = (np.asarray(s["rx"], np.float32) - ox, np.asarray(s["rz"], np.float32))
+    rcv = np.zeros((2, len(s["rx"]), nt_sample), np.float32)
+    full = np.zeros((1 + nt_sample, 2, nx, nz), np.float32)
+    full[...] = 0.0   # first touch outside the timed region
+    g = np.zeros((5 if k == 1 else 3, nx, nz), np.float32)
+    t0 = time.perf_counter()
+    lib.propagate(k, 0, model, src, rcv, par, nx, nz, d, d, 0.0, 0.0, sl, rl, full=full)
+    adj = np.ascontiguousarray(-rcv[:, :, ::-1])
+    srcb = np.zeros((2, 1, nt_sample), np.float32)
+    lib.propagate(k, 1, model, adj, srcb, par, nx, nz, d, d, 0.0, 0.0, rl, sl, full=full, grad=g)
+    dtime = time.perf_counter() - t0
+    return dtime, 2 * (nt_sample - 1) * nx * nz, kind
+
+
+def cpu_cores():
+    n = os.environ.get("OMP_NUM_THREADS")
+    return int(n) if n else (os.cpu_count() or 1)
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    wl = build_workload(args.config, 0, 1)
+    nt_sample = 301
+    for _ in range(args.warmup):
+        cpu_sample(wl, nt_sample)
+    times, kind, cells = [], None, 0
+    for _ in range(args.steps):
+        dtime, cells, kind = cpu_sample(wl, nt_sample)
+        times.append(dtime)
+    tot = sum(times)
+    gcell = cells * args.steps / tot / 1e9
+    shots = gcell * 1e9 / cells_per_step(wl) * len(wl["shots"])
+    sample = "forward+adjoint gradient of shot 0 on its full grid, %d of %d time samples" % (nt_sample, wl["nt"])
+    line = {"metric": METRIC, "value": gcell, "unit": "Gcell-updates/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "shots_per_s": shots,
+            "config": {"workload": workload_name(args.config), "sample_nt": nt_sample},
+            "cpu_baseline": {"value": gcell, "unit": "Gcell-updates/s", "cores": cpu_cores(), "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": gcell, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(cfg):
+    if cfg == "single":
+        return "elastic isotropic FWI gradient, 1 shot, 401x801 grid at 5 m, nt=5001, 400 2-C receivers, FP32 snapshots"
+    return "VTI FWI gradient, 64 shots on cropped grids (1.0-3.5 km apertures, 1.2-2.0 s records), 401x801 at 5 m"
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import fwi2d_b200 as F
+    F.load()
+    wl = build_workload(args.config, rank, world)
+    P, start, srcs = make_prop(wl, local)
+    obs = observed(wl, local, srcs)
+    stream = torch.cuda.Stream()
+    P.set_stream(stream.cuda_stream)
+    P.set_observed(obs)
+    P.upload(srcs, adjoint=False)
+    L = F.load()
+    from fwi2d_b200 import _capi as C
+    ng = 3
+    gdev = torch.zeros((ng, wl["nx"], wl["nz"]), dtype=torch.float32, device="cuda")
+
+    def grad_step():
+        C.check(L.fwi2d_fwi_gradient(P.h, None, None, None, wl["seismotype"], None, None))
+        if world > 1:
+            P.copy_gradient(gdev.data_ptr())
+            with torch.cuda.stream(stream):
+                torch.distributed.all_reduce(gdev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # warm-up (graph capture happens on the first call)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            grad_step()
+    torch.cuda.synchronize()
+    barrier()
+    clk = Clocks(local)
+    clk.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(args.steps):
+            grad_step()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    fwd_ms, adj_ms = P.last_timing()
+    clocks = clk.stop()
+
+    # end to end through the public call with host buffers (pinned)
+    kind = wl["kind"]
+    model_h = torch.from_numpy(start).pin_memory().numpy()
+    src_h = torch.from_numpy(np.concatenate([s.ravel() for s in srcs])).pin_memory().numpy()
+    obs_h = torch.from_numpy(np.concatenate([o.ravel() for o in obs])).pin_memory().numpy()
+    grad_pin = torch.empty((ng, wl["nx"], wl["nz"]), dtype=torch.float32).pin_memory()
+    import ctypes
+    mis = ctypes.c_double(0.0)
+
+    def e2e_step():
+        # host inputs in, gradient (summed over ranks) and misfit out to host
+        C.check(L.fwi2d_fwi_gradient(P.h, C.ptr(model_h), C.ptr(src_h), C.ptr(obs_h), wl["seismotype"], None,
+                                     ctypes.byref(mis)))
+        P.copy_gradient(gdev.data_ptr())
+        if world > 1:
+            torch.distributed.all_reduce(gdev)
+        grad_pin.copy_(gdev, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    n_e2e = max(1, args.steps // 2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(n_e2e):
+            e2e_step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / n_e2e
+
+    # max over ranks
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    info = P.plan_info()
+    cells_rank = cells_per_step(wl)
+    nshots_rank = len(wl["shots"])
+    total_cells = cells_rank * world
+    total_shots = nshots_rank * world
+    ms_step = ms / args.steps
+    value = total_cells / (ms_step / 1e3) / 1e9
+    shots_s = total_shots / (ms_step / 1e3)
+
+    # dominant kernel: the adjoint step (imaging condition fused)
+    steps_adj = max(s["nt"] for s in wl["shots"]) - 1
+    cells_launch = sum(s["nx"] * wl["nz"] for s in wl["shots"])
+    adj_launch_s = adj_ms / 1e3 / steps_adj
+    fwd_launch_s = fwd_ms / 1e3 / steps_adj
+    achieved = BYTES_ADJ * cells_launch / adj_launch_s / 1e9
+    peak, peak_kind = peaks()
+    tr = traffic_per_launch()
+    launches = (info["launches_forward"] + info["launches_adjoint"] + 2 * nshots_rank + 1) * args.steps
+    if rank == 0:
+        h2d = model_h.nbytes + src_h.nbytes + obs_h.nbytes
+        d2h = grad_pin.numel() * 4 + 8
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "shots_per_s": shots_s,
+            "config": {"workload": workload_name(args.config), "nx": wl["nx"], "nz": wl["nz"], "nt": wl["nt"],
+                       "shots_per_gpu": nshots_rank, "snapshots": "fp32 every step, in HBM",
+                       "cell_updates_per_step": total_cells, "tile_shape": info["tile_shape"],
+                       "l2": "inputs larger than L2: %.1f GB of snapshots written and read per step"
+                             % (info["snapshot_bytes"] / 1e9),
+                       "parallelism": "shots over %d GPU(s), NCCL all-reduce of the gradient" % world},
+            "e2e": {"value": total_cells / (e2e_ms / 1e3) / 1e9, "unit": "Gcell-updates/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "shots_per_s": total_shots / (e2e_ms / 1e3)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "elastic_step (adjoint + imaging)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": (tr or {}).get("adjoint_bytes_per_launch"),
+                         "algorithmic_bytes_per_launch": BYTES_ADJ * cells_launch,
+                         "launch_ms": adj_launch_s * 1e3,
+                         "forward_launch_ms": fwd_launch_s * 1e3,
+                         "forward_achieved": BYTES_FWD * cells_launch / fwd_launch_s / 1e9},
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                nt_s = 301
+                dtime, cells, kind = cpu_sample(wl, nt_s)
+                g = cells / dtime / 1e9
+                line["cpu_baseline"] = {"value": g, "unit": "Gcell-updates/s", "cores": cpu_cores(), "kind": kind,
+                                        "sample": "forward+adjoint gradient of shot 0, %d of %d time samples"
+                                                  % (nt_s, wl["nt"]),
+                                        "shots_per_s": g * 1e9 / cells_per_step(wl) * nshots_rank}
+            except Exception as e:   # the baseline never blocks the GPU line
+                line["cpu_baseline"] = {"value": None, "unit": "Gcell-updates/s", "cores": cpu_cores(),
+                                        "kind": "port", "sample": "failed: %s" % e}
+        print(json.dumps(line), flush=True)
+    P.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

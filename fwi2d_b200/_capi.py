@@ -18,7 +18,7 @@ SYMBOLS = [
     "fwi2d_last_error", "fwi2d_version", "fwi2d_injector_weights", "fwi2d_ctx_create", "fwi2d_ctx_destroy",
     "fwi2d_set_model", "fwi2d_set_shots", "fwi2d_forward", "fwi2d_adjoint", "fwi2d_upload_traces", "fwi2d_run",
     "fwi2d_sync", "fwi2d_snapshot", "fwi2d_plan_info", "fwi2d_tile_shape_count", "fwi2d_tile_shape",
-    "fwi2d_propagate",
+    "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing", "fwi2d_set_stream", "fwi2d_copy_gradient",
 ]
 
 
@@ -91,6 +91,12 @@ def load(build_if_missing=False):
     L.fwi2d_plan_info.argtypes = [vp, vp, vp, vp, vp]
     L.fwi2d_tile_shape.argtypes = [i, vp, vp]
     L.fwi2d_propagate.argtypes = [i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(Params), i, i, i, i, f, f]
+    L.fwi2d_update_model.argtypes = [vp, vp]
+    L.fwi2d_set_observed.argtypes = [vp, vp]
+    L.fwi2d_fwi_gradient.argtypes = [vp, vp, vp, vp, i, vp, ctypes.POINTER(ctypes.c_double)]
+    L.fwi2d_last_timing.argtypes = [vp, vp, vp]
+    L.fwi2d_set_stream.argtypes = [vp, vp]
+    L.fwi2d_copy_gradient.argtypes = [vp, vp]
     _lib = L
     return L
 

@@ -68,9 +68,15 @@ struct DevBuf {
         }
     }
     template <class T> T *as() const { return (T *)p; }
+    // (re)allocates only when the size changes, so device pointers captured
+    // in a CUDA graph stay valid across same-size updates
+    void ensure(size_t bytes)
+    {
+        if (bytes != n || !p) alloc(bytes);
+    }
     template <class T> void upload(const std::vector<T> &v, cudaStream_t st)
     {
-        alloc(std::max<size_t>(v.size(), 1) * sizeof(T));
+        ensure(std::max<size_t>(v.size(), 1) * sizeof(T));
         if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     }
 };
@@ -219,20 +225,29 @@ struct Plan {
     std::vector<std::unique_ptr<ShotPlan>> shots;
     std::vector<TileRef> tiles;
     DevBuf d_tiles, d_shots_f, d_shots_a;
-    DevBuf d_init, d_init_off;
-    size_t init_cap = 0;
+    // initial-state cells per mode (0 forward, 1 adjoint)
+    std::vector<InitCell> icells[2];
+    std::vector<int> ioff[2], iidx[2];
+    DevBuf d_icells[2], d_ioff[2], d_iidx[2];
+    // FWI gradient: observed data, misfit partial sums
+    DevBuf d_obs, d_misfit;
     DevBuf d_grad_full, d_stage;
     StepConst C;
     float dtg = 0;
     bool have_snapshots = false;
     bool snapshots_valid = false;
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};   // forward, forward+store, adjoint
+    cudaEvent_t ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [forward|adjoint][start|end]
+    bool timed[2] = {false, false};
     long long launches[3] = {0, 0, 0};
     long long snap_bytes = 0;
     ~Plan()
     {
         for (auto &g : graph)
             if (g) cudaGraphExecDestroy(g);
+        for (auto &a : ev)
+            for (auto &e : a)
+                if (e) cudaEventDestroy(e);
     }
 };
 
@@ -240,7 +255,8 @@ struct Plan {
 
 struct fwi2d_ctx {
     int device = 0;
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr;      // stream all work is ordered on
+    cudaStream_t own = nullptr;     // the context's own stream
     fwi2d::ModelState M;
     std::unique_ptr<fwi2d::Plan> plan;
 };
@@ -250,6 +266,8 @@ namespace fwi2d {
 static void set_device(fwi2d_ctx *ctx) { CK(cudaSetDevice(ctx->device)); }
 
 // ---- model upload -----------------------------------------------------------
+static void upload_model_values(fwi2d_ctx *ctx, const float *model);
+
 static void set_model(fwi2d_ctx *ctx, int kind, int nx, int nz, float dx, float dz, const float *model)
 {
     REQ(kind >= 0 && kind <= 3, "unknown propagator kind");
@@ -266,6 +284,14 @@ static void set_model(fwi2d_ctx *ctx, int kind, int nx, int nz, float dx, float 
     M.dx = dx;
     M.dz = dz;
     M.npar = npar_of(kind);
+    upload_model_values(ctx, model);
+}
+
+// New values for the current model geometry (device arrays, host copy).
+static void upload_model_values(fwi2d_ctx *ctx, const float *model)
+{
+    ModelState &M = ctx->M;
+    const int kind = M.kind, nx = M.nx, nz = M.nz;
     const size_t nxz = (size_t)nx * nz;
     M.host.assign(model, model + nxz * M.npar);
     for (size_t i = 0; i < M.host.size(); i++) REQ(std::isfinite(M.host[i]), "model holds a non-finite value");
@@ -273,7 +299,7 @@ static void set_model(fwi2d_ctx *ctx, int kind, int nx, int nz, float dx, float 
     DevBuf stage;
     stage.alloc(nxz * sizeof(float));
     auto up = [&](DevBuf &dst, const float *src) {
-        dst.alloc(pitched * sizeof(float));
+        dst.ensure(pitched * sizeof(float));
         CK(cudaMemcpyAsync(stage.p, src, nxz * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
         k_pitch<<<592, 256, 0, ctx->st>>>(stage.as<float>(), dst.as<float>(), nx, nz, M.ldz);
         CK(cudaGetLastError());
@@ -481,7 +507,71 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
     (void)P;
 }
 
-static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
+// Cells touched by the injection at time sample 0, with their entries in
+// the reference's order and the double-precision scale of we_op.cpp:657-663.
+static void init_factors(const ModelState &M, Plan &P)
+{
+    const double dt = P.par.dt;
+    for (int mode = 0; mode < 2; mode++)
+        for (size_t s = 0; s < P.shots.size(); s++) {
+            const ShotPlan &S = *P.shots[s];
+            for (int c = P.ioff[mode][s]; c < P.ioff[mode][s + 1]; c++) {
+                InitCell &q = P.icells[mode][c];
+                const size_t mi = (size_t)(S.x0 + q.gx) * M.nz + q.gz;
+                if (M.kind == KIND_ACOUSTIC) q.factor = 0.5 * (double)M.host[mi] * dt * dt;
+                else q.factor = 0.5 * dt * dt / (double)M.host[2 * (size_t)M.nx * M.nz + mi];
+            }
+        }
+}
+
+static void build_init_cells(const ModelState &M, Plan &P)
+{
+    for (int mode = 0; mode < 2; mode++) {
+        P.icells[mode].clear();
+        P.iidx[mode].clear();
+        P.ioff[mode].assign(P.shots.size() + 1, 0);
+        for (size_t s = 0; s < P.shots.size(); s++) {
+            const std::vector<InjEntry> &inj = mode ? P.shots[s]->inj_a : P.shots[s]->inj_f;
+            std::vector<std::vector<int>> lists;
+            std::vector<InitCell> cells;
+            for (size_t i = 0; i < inj.size(); i++) {
+                const InjEntry &e = inj[i];
+                size_t k = 0;
+                for (; k < cells.size(); k++)
+                    if (cells[k].gx == e.gx && cells[k].gz == e.gz && cells[k].comp == e.comp) break;
+                if (k == cells.size()) {
+                    InitCell q;
+                    std::memset(&q, 0, sizeof(q));
+                    q.gx = e.gx;
+                    q.gz = e.gz;
+                    q.comp = e.comp;
+                    cells.push_back(q);
+                    lists.emplace_back();
+                }
+                lists[k].push_back((int)i);
+            }
+            for (size_t k = 0; k < cells.size(); k++) {
+                cells[k].i0 = (int)P.iidx[mode].size();
+                P.iidx[mode].insert(P.iidx[mode].end(), lists[k].begin(), lists[k].end());
+                cells[k].i1 = (int)P.iidx[mode].size();
+                P.icells[mode].push_back(cells[k]);
+            }
+            P.ioff[mode][s + 1] = (int)P.icells[mode].size();
+        }
+    }
+    init_factors(M, P);
+}
+
+static void upload_init_cells(Plan &P, cudaStream_t st)
+{
+    for (int mode = 0; mode < 2; mode++) {
+        P.d_icells[mode].upload(P.icells[mode], st);
+        P.d_ioff[mode].upload(P.ioff[mode], st);
+        P.d_iidx[mode].upload(P.iidx[mode], st);
+    }
+}
+
+static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
 {
     ModelState &M = ctx->M;
     if (M.kind < 0) throw Error(FWI2D_ERR_STATE, "fwi2d_set_model must be called first");
@@ -637,50 +727,87 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
     }
     P->d_shots_f.upload(sf, ctx->st);
     P->d_shots_a.upload(sa, ctx->st);
-    // initial-state scatter buffers: at most one entry per injection sample
-    size_t cap = 0;
-    for (auto &S : P->shots) cap += std::max(S->inj_f.size(), S->inj_a.size());
-    P->init_cap = std::max<size_t>(cap, 1);
-    P->d_init.alloc(P->init_cap * sizeof(InitEntry));
-    P->d_init_off.alloc((nshots + 1) * sizeof(int));
+    build_init_cells(M, *P);
+    upload_init_cells(*P, ctx->st);
     P->d_grad_full.alloc((size_t)P->ncompg * M.nx * M.ldz * sizeof(float));
     CK(cudaStreamSynchronize(ctx->st));
     ctx->plan = std::move(P);
 }
 
-// Initial "prev" of the leapfrog (we_op.cpp:657-663): inject sample 0 with
-// add=false, then scale by dt^2/(2 rho) in double.
-static void compute_init(const ModelState &M, const Plan &P, bool adjoint, const float *const *trace_blocks,
-                         std::vector<InitEntry> &ent, std::vector<int> &off)
+// Time `steps` forward steps of the current plan (fields zeroed, no output),
+// in milliseconds per step.
+static float time_forward_steps(fwi2d_ctx *ctx, int steps)
 {
-    ent.clear();
-    off.assign(P.shots.size() + 1, 0);
-    for (size_t s = 0; s < P.shots.size(); s++) {
-        const ShotPlan &S = *P.shots[s];
-        const std::vector<InjEntry> &inj = adjoint ? S.inj_a : S.inj_f;
-        const float *tr = trace_blocks[s];   // [rows][nt]
-        // accumulate per cell in entry order (entries of one cell keep the reference's trace order)
-        std::vector<InitEntry> cells;
-        for (const InjEntry &e : inj) {
-            const float a = tr[(size_t)e.ia * S.nt];
-            const float c = e.mt ? (e.wa * a - e.wb * tr[(size_t)e.ib * S.nt]) : e.wa * a;
-            bool found = false;
-            for (InitEntry &q : cells)
-                if (q.gx == e.gx && q.gz == e.gz && q.comp == e.comp) {
-                    q.val += c;
-                    found = true;
-                    break;
-                }
-            if (!found) cells.push_back(InitEntry{e.gx, e.gz, e.comp, 0.f + c});
-        }
-        for (InitEntry &q : cells) {
-            const size_t mi = (size_t)(S.x0 + q.gx) * M.nz + q.gz;
-            const double rho = M.host[2 * (size_t)M.nx * M.nz + mi];
-            q.val = (float)((double)q.val * (0.5 * (double)P.par.dt * (double)P.par.dt / rho));
-            ent.push_back(q);
-        }
-        off[s + 1] = (int)ent.size();
+    Plan &P = *ctx->plan;
+    for (auto &S : P.shots) {
+        CK(cudaMemsetAsync(S->u0.p, 0, S->u0.n, ctx->st));
+        CK(cudaMemsetAsync(S->u1.p, 0, S->u1.n, ctx->st));
     }
+    const ModelDev md = ctx->M.dev();
+    const ShotDev *shots = P.d_shots_f.as<ShotDev>();
+    const int nsteps = std::min(steps, P.nt_max - 1);
+    for (int it = 0; it < std::min(3, nsteps); it++)
+        launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
+                            it, STEP_EXTRACT, P.dtg, ctx->st);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, ctx->st));
+    for (int it = 0; it < nsteps; it++)
+        launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
+                            it, STEP_EXTRACT, P.dtg, ctx->st);
+    CK(cudaEventRecord(b, ctx->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaGetLastError());
+    return ms / std::max(nsteps, 1);
+}
+
+// Tile-shape autotuner: for plans that leave the shape open (tile_shape < 0),
+// time a few forward steps of every shape that tiles the grids and keep the
+// fastest.  The choice is cached per (kind, nz, shot grid widths).
+static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
+{
+    REQ(par != nullptr && shots != nullptr && nshots > 0, "no shots");
+    fwi2d_params p = *par;
+    if (p.tile_shape < 0 && ctx->M.kind >= 0) {
+        static std::vector<std::pair<std::string, int>> cache;
+        std::string key = std::to_string(ctx->M.kind) + "/" + std::to_string(ctx->M.nz) + "/" + std::to_string(nshots);
+        long long cells = 0;
+        for (int i = 0; i < nshots; i++) {
+            key += "/" + std::to_string(shots[i].nx);
+            cells += (long long)shots[i].nx * ctx->M.nz * shots[i].nt;
+        }
+        int chosen = -1;
+        for (auto &kv : cache)
+            if (kv.first == key) chosen = kv.second;
+        if (chosen < 0 && cells >= 20000000LL) {
+            float best = 1e30f;
+            for (int s = 0; s < elastic_tile_count(); s++) {
+                fwi2d_params q = p;
+                q.tile_shape = s;
+                q.sub = 0;
+                try {
+                    set_shots_impl(ctx, &q, nshots, shots);
+                } catch (const Error &e) {
+                    if (e.code == FWI2D_ERR_ARG) continue;   // shape does not tile these grids
+                    throw;
+                }
+                const float ms = time_forward_steps(ctx, 30);
+                if (ms < best) {
+                    best = ms;
+                    chosen = s;
+                }
+            }
+            ctx->plan.reset();
+            if (chosen >= 0) cache.emplace_back(key, chosen);
+        }
+        p.tile_shape = chosen;
+    }
+    set_shots_impl(ctx, &p, nshots, shots);
 }
 
 static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
@@ -689,17 +816,22 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
     const bool adj = mode == 2;
     const bool store = mode == 1;
     cudaGraph_t g;
-    CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+    // graphs are captured on the context's own stream and may be launched on any stream
+    cudaStream_t cst = ctx->own;
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaStreamBeginCapture(cst, cudaStreamCaptureModeThreadLocal));
     long long n = 0;
     for (auto &S : P.shots) {
-        CK(cudaMemsetAsync(S->u0.p, 0, S->u0.n, ctx->st));
-        CK(cudaMemsetAsync(S->u1.p, 0, S->u1.n, ctx->st));
-        if (adj) CK(cudaMemsetAsync(S->grad.p, 0, S->grad.n, ctx->st));
-        if (store && S->amax.p) CK(cudaMemsetAsync(S->amax.p, 0, S->amax.n, ctx->st));
+        CK(cudaMemsetAsync(S->u0.p, 0, S->u0.n, cst));
+        CK(cudaMemsetAsync(S->u1.p, 0, S->u1.n, cst));
+        if (adj) CK(cudaMemsetAsync(S->grad.p, 0, S->grad.n, cst));
+        if (store && S->amax.p) CK(cudaMemsetAsync(S->amax.p, 0, S->amax.n, cst));
     }
     const ShotDev *shots = (adj ? P.d_shots_a : P.d_shots_f).as<ShotDev>();
     const int nshots = (int)P.shots.size();
-    launch_scatter_init(shots, nshots, P.d_init.as<InitEntry>(), P.d_init_off.as<int>(), ctx->st);
+    const int im = adj ? 1 : 0;
+    launch_init_state(shots, nshots, P.d_icells[im].as<InitCell>(), P.d_ioff[im].as<int>(), P.d_iidx[im].as<int>(),
+                      cst);
     n++;
     int flags = 0;
     if (adj) flags = STEP_GRAD;
@@ -713,15 +845,15 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
     const ModelDev md = M.dev();
     for (int it = 0; it < P.nt_max - 1; it++) {
         launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
-                            it, flags, P.dtg, ctx->st);
+                            it, flags, P.dtg, cst);
         n++;
     }
     if (!adj) {
-        launch_finalize(shots, nshots, P.C, 2, STEP_EXTRACT | (store ? STEP_STORE : 0), ctx->st);
+        launch_finalize(shots, nshots, P.C, 2, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
         n++;
     }
     CK(cudaGetLastError());
-    CK(cudaStreamEndCapture(ctx->st, &g));
+    CK(cudaStreamEndCapture(cst, &g));
     cudaGraphExec_t ge;
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
@@ -757,15 +889,8 @@ static void upload_traces(fwi2d_ctx *ctx, const float *traces, bool adjoint)
         CK(cudaGetLastError());
         blocks.push_back(p);
         p += n;
+        CK(cudaStreamSynchronize(ctx->st));   // the staging buffer is reused by the next shot
     }
-    std::vector<InitEntry> ent;
-    std::vector<int> off;
-    compute_init(ctx->M, P, adjoint, blocks.data(), ent, off);
-    REQ(ent.size() <= P.init_cap, "internal: initial-state table overflow");
-    if (!ent.empty())
-        CK(cudaMemcpyAsync(P.d_init.p, ent.data(), ent.size() * sizeof(InitEntry), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(P.d_init_off.p, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));   // host arrays above are temporaries
 }
 
 static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
@@ -779,7 +904,15 @@ static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
     if (store && !P.have_snapshots) throw Error(FWI2D_ERR_ARG, "snapshots requested with sub = 0");
     const int mode = adjoint ? 2 : (store ? 1 : 0);
     if (!P.graph[mode]) capture(ctx, P, mode);
+    const int e = adjoint ? 1 : 0;
+    if (!P.ev[e][0]) {
+        CK(cudaEventCreate(&P.ev[e][0]));
+        CK(cudaEventCreate(&P.ev[e][1]));
+    }
+    CK(cudaEventRecord(P.ev[e][0], ctx->st));
     CK(cudaGraphLaunch(P.graph[mode], ctx->st));
+    CK(cudaEventRecord(P.ev[e][1], ctx->st));
+    P.timed[e] = true;
     if (adjoint) {
         CK(cudaMemsetAsync(P.d_grad_full.p, 0, P.d_grad_full.n, ctx->st));
         for (auto &S : P.shots)
@@ -821,6 +954,176 @@ static void download_grad(fwi2d_ctx *ctx, float *grad)
     CK(cudaStreamSynchronize(ctx->st));
 }
 
+
+// ---------------------------------------------------------------------------
+// FWI gradient pieces on the device (optimization.hpp:590-951 and the
+// adjoint-source preparation of we_op.cpp:1108-1134)
+// ---------------------------------------------------------------------------
+
+// Per trace: synthetic data (Dt of the extracted displacement when
+// seismotype = 1, misc.cpp:71-84), residual r = syn - obs, the trace's misfit
+// sum(r^2) - (r_0^2 + r_{nt-1}^2)/2 (compensated), and the adjoint source
+//   q[t] = -r[nt-1-t]  (Ht^-1 of the caller's Ht r, reversed, scaled by -1),
+//   then Dt^T (misc.cpp:85-94) when seismotype = 1.
+__global__ void k_residual(const float *__restrict__ u, const float *__restrict__ obs, float *__restrict__ adj,
+                           float *__restrict__ syn_out, double *__restrict__ misfit, int nt, int rows, float dt,
+                           int seismotype)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    auto U = [&](int t) { return u[(long long)t * rows + r]; };
+    auto syn = [&](int t) -> float {
+        if (!seismotype) return U(t);
+        if (t == 0) return (U(1) - U(0)) / dt;
+        if (t == nt - 1) return (U(nt - 1) - U(nt - 2)) / dt;
+        return (U(t + 1) - U(t - 1)) / (2 * dt);
+    };
+    auto res = [&](int t) { return syn(t) - obs[(long long)t * rows + r]; };
+    // misfit with Neumaier summation
+    float sum = 0.f, comp = 0.f;
+    for (int t = 0; t < nt; t++) {
+        const float rv = res(t);
+        float term = rv * rv;
+        if (t == 0 || t == nt - 1) term = 0.5f * term;
+        const float y = sum + term;
+        if (fabsf(sum) >= fabsf(term)) comp += (sum - y) + term;
+        else comp += (term - y) + sum;
+        sum = y;
+        if (syn_out) syn_out[(long long)t * rows + r] = syn(t);
+    }
+    misfit[r] = (double)sum + (double)comp;
+    auto q = [&](int t) { return -res(nt - 1 - t); };
+    for (int t = 0; t < nt; t++) {
+        float a;
+        if (!seismotype) a = q(t);
+        else if (t == 0) a = (q(1) + q(0)) / dt;
+        else if (t == nt - 1) a = (-q(nt - 1) - q(nt - 2)) / dt;
+        else a = (q(t + 1) - q(t - 1)) / (2 * dt);
+        adj[(long long)t * rows + r] = a;
+    }
+}
+
+// H quadrature (spatial_operators.cpp:6-98) and the chain rule from
+// (lambda, mu, rho) to (vp, vs, rho) (we_op.cpp:1193-1228), in place on the
+// pitched model-grid gradient.
+__global__ void k_quadrature_chain(float *__restrict__ g, const float *__restrict__ lam, const float *__restrict__ mu,
+                                   const float *__restrict__ rho, int nx, int nz, int ldz, float dx, float dz,
+                                   float h0, float h1, float h2, float h3)
+{
+    const long long n = (long long)nx * ldz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(i / ldz), iz = (int)(i - (long long)ix * ldz);
+        if (iz >= nz) continue;
+        const float hc[4] = {h0, h1, h2, h3};
+        const float wz = iz < 4 ? hc[iz] : (iz >= nz - 4 ? hc[nz - 1 - iz] : 1.f);
+        const float wx = ix < 4 ? hc[ix] : (ix >= nx - 4 ? hc[nx - 1 - ix] : 1.f);
+        float g0 = g[i], g1 = g[n + i], g2 = g[2 * n + i];
+        // applyHz then applyHx on each component
+        if (iz < 4 || iz >= nz - 4) { g0 = g0 * wz * dz; g1 = g1 * wz * dz; g2 = g2 * wz * dz; }
+        else { g0 = g0 * dz; g1 = g1 * dz; g2 = g2 * dz; }
+        if (ix < 4 || ix >= nx - 4) { g0 = g0 * wx * dx; g1 = g1 * wx * dx; g2 = g2 * wx * dx; }
+        else { g0 = g0 * dx; g1 = g1 * dx; g2 = g2 * dx; }
+        const float l = lam[i], m = mu[i], r = rho[i];
+        const float n2 = (l / r) * g0 + (m / r) * g1 + g2;
+        const float n1 = (float)(2 * sqrt((double)(m * r)) * (double)(g1 - 2 * g0));
+        const float n0 = (float)(2 * sqrt((double)(r * (l + 2 * m))) * (double)g0);
+        g[i] = n0;
+        g[n + i] = n1;
+        g[2 * n + i] = n2;
+    }
+}
+
+static void update_model(fwi2d_ctx *ctx, const float *model)
+{
+    ModelState &M = ctx->M;
+    if (M.kind < 0) throw Error(FWI2D_ERR_STATE, "fwi2d_set_model must be called first");
+    REQ(model != nullptr, "null model");
+    set_device(ctx);
+    upload_model_values(ctx, model);
+    if (!ctx->plan) return;
+    Plan &P = *ctx->plan;
+    const fwi2d_params &p = P.par;
+    for (auto &S : P.shots) {
+        std::vector<float> den;
+        const float *lam = M.hp(0) + (size_t)S->x0 * M.nz, *mu = M.hp(1) + (size_t)S->x0 * M.nz,
+                    *rho = M.hp(2) + (size_t)S->x0 * M.nz;
+        const float *eps = M.kind == KIND_VTI ? M.hp(4) + (size_t)S->x0 * M.nz : nullptr;
+        elastic_scale_divisors(S->nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, p.bc_top == 2,
+                               p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
+        S->den.upload(den, ctx->st);
+    }
+    init_factors(M, P);
+    upload_init_cells(P, ctx->st);
+    CK(cudaStreamSynchronize(ctx->st));
+}
+
+// One FWI gradient on the device: forward with snapshots, residual against
+// the resident observed data, adjoint sources, adjoint with the imaging
+// condition, quadrature and chain rule.  Leaves the model-space gradient in
+// d_grad_full and the per-trace misfit terms in d_misfit.
+static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
+{
+    Plan &P = need_plan(ctx);
+    REQ(P.d_obs.p != nullptr, "no observed data (fwi2d_set_observed)");
+    run(ctx, false, true);
+    size_t rows_total = 0;
+    for (auto &S : P.shots) rows_total += S->nrcv_rows;
+    P.d_misfit.ensure(std::max<size_t>(rows_total, 1) * sizeof(double));
+    size_t obs_off = 0, row_off = 0;
+    for (auto &S : P.shots) {
+        k_residual<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
+            S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off, S->src_a.as<float>(), nullptr,
+            P.d_misfit.as<double>() + row_off, S->nt, S->nrcv_rows, P.par.dt, seismotype);
+        CK(cudaGetLastError());
+        obs_off += (size_t)S->nt * S->nrcv_rows;
+        row_off += S->nrcv_rows;
+    }
+    run(ctx, true, false);
+    if (chain && P.kind != KIND_ACOUSTIC) {
+        const ModelState &M = ctx->M;
+        const SbpTables &t = sbp_tables();
+        k_quadrature_chain<<<592, 256, 0, ctx->st>>>(P.d_grad_full.as<float>(), M.p0.as<float>(), M.p1.as<float>(),
+                                                     M.p2.as<float>(), M.nx, M.nz, M.ldz, M.dx, M.dz, t.hc[0], t.hc[1],
+                                                     t.hc[2], t.hc[3]);
+        CK(cudaGetLastError());
+    }
+}
+
+static void set_observed(fwi2d_ctx *ctx, const float *obs)
+{
+    Plan &P = need_plan(ctx);
+    REQ(obs != nullptr, "null observed data");
+    set_device(ctx);
+    size_t total = 0, maxn = 0;
+    for (auto &S : P.shots) {
+        total += (size_t)S->nt * S->nrcv_rows;
+        maxn = std::max(maxn, (size_t)S->nt * S->nrcv_rows);
+    }
+    P.d_obs.ensure(total * sizeof(float));
+    if (P.d_stage.n < maxn * sizeof(float)) P.d_stage.alloc(maxn * sizeof(float));
+    size_t off = 0;
+    for (auto &S : P.shots) {
+        const size_t n = (size_t)S->nt * S->nrcv_rows;
+        CK(cudaMemcpyAsync(P.d_stage.p, obs + off, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        launch_to_time_major(P.d_stage.as<float>(), P.d_obs.as<float>() + off, S->nrcv_rows, S->nt, ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->st));
+        off += n;
+    }
+}
+
+static double read_misfit(fwi2d_ctx *ctx)
+{
+    Plan &P = need_plan(ctx);
+    size_t rows_total = 0;
+    for (auto &S : P.shots) rows_total += S->nrcv_rows;
+    std::vector<double> m(rows_total);
+    CK(cudaMemcpyAsync(m.data(), P.d_misfit.p, rows_total * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    double f = 0.0;
+    for (double v : m) f += v;
+    return 0.5 * (double)P.par.dt * f;
+}
 
 // Host snapshots [nslot][ncomp][nx][nz] (fp32) -> the device store of shot 0.
 static void load_host_snapshots(fwi2d_ctx *ctx, const float *full)
@@ -929,7 +1232,8 @@ int fwi2d_ctx_create(int device, fwi2d_ctx **out)
     auto c = std::make_unique<fwi2d_ctx>();
     c->device = device;
     CK(cudaSetDevice(device));
-    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+    c->st = c->own;
     const SbpTables &t = sbp_tables();
     upload_sbp_tables(&t.b1[0][0], &t.b2[0][0][0], t.c2, t.c1, t.sc, t.hc);
     CK(cudaGetLastError());
@@ -945,7 +1249,7 @@ int fwi2d_ctx_destroy(fwi2d_ctx *ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->st);
     ctx->plan.reset();
-    cudaStreamDestroy(ctx->st);
+    cudaStreamDestroy(ctx->own);
     delete ctx;
     ABI_END
 }
@@ -1078,6 +1382,46 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     ABI_END
 }
 
+int fwi2d_set_stream(fwi2d_ctx *ctx, void *stream)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    set_device(ctx);
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->st = stream ? (cudaStream_t)stream : ctx->own;
+    ABI_END
+}
+
+int fwi2d_copy_gradient(fwi2d_ctx *ctx, float *dst_device)
+{
+    ABI_TRY
+    REQ(ctx && dst_device, "null argument");
+    Plan &P = need_plan(ctx);
+    const ModelState &M = ctx->M;
+    set_device(ctx);
+    k_unpitch<<<592, 256, 0, ctx->st>>>(P.d_grad_full.as<float>(), dst_device, (long long)P.ncompg * M.nx, M.nz, M.ldz);
+    CK(cudaGetLastError());
+    ABI_END
+}
+
+int fwi2d_last_timing(fwi2d_ctx *ctx, float *forward_ms, float *adjoint_ms)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    Plan &P = need_plan(ctx);
+    set_device(ctx);
+    float *out[2] = {forward_ms, adjoint_ms};
+    for (int e = 0; e < 2; e++) {
+        if (!out[e]) continue;
+        *out[e] = -1.f;
+        if (P.timed[e]) {
+            CK(cudaEventSynchronize(P.ev[e][1]));
+            CK(cudaEventElapsedTime(out[e], P.ev[e][0], P.ev[e][1]));
+        }
+    }
+    ABI_END
+}
+
 int fwi2d_tile_shape_count(void) { return elastic_tile_count(); }
 
 int fwi2d_tile_shape(int index, int *tz, int *tx)
@@ -1085,6 +1429,37 @@ int fwi2d_tile_shape(int index, int *tz, int *tx)
     ABI_TRY
     REQ(index >= 0 && index < elastic_tile_count() && tz && tx, "no such tile shape");
     elastic_tile_shape(index, tz, tx);
+    ABI_END
+}
+
+int fwi2d_update_model(fwi2d_ctx *ctx, const float *model)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    update_model(ctx, model);
+    ABI_END
+}
+
+int fwi2d_set_observed(fwi2d_ctx *ctx, const float *obs)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    set_observed(ctx, obs);
+    ABI_END
+}
+
+int fwi2d_fwi_gradient(fwi2d_ctx *ctx, const float *model, const float *src, const float *obs, int seismotype,
+                       float *grad, double *misfit)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    REQ(seismotype == 0 || seismotype == 1, "seismotype must be 0 or 1");
+    if (model) update_model(ctx, model);
+    if (src) upload_traces(ctx, src, false);
+    if (obs) set_observed(ctx, obs);
+    fwi_gradient(ctx, seismotype, true);
+    if (grad) download_grad(ctx, grad);
+    if (misfit) *misfit = read_misfit(ctx);
     ABI_END
 }
 

@@ -29,11 +29,12 @@ struct ExtEntry {
     float w[9];
 };
 
-// Initial-state scatter: u[comp][gx][gz] = val (precomputed on the host in the
-// reference's double arithmetic, we_op.cpp:657-663).
-struct InitEntry {
-    int gx, gz, comp;
-    float val;
+// Initial "prev" of the leapfrog (we_op.cpp:657-663): the cell accumulates its
+// injection entries idx[i0..i1) at time sample 0 in the reference's order,
+// then is scaled in double by `factor` (dt^2/(2 rho), or K dt^2/2 acoustic).
+struct InitCell {
+    int gx, gz, comp, i0, i1, pad;
+    double factor;
 };
 
 struct ShotDev {

@@ -66,353 +66,655 @@ __device__ __forceinline__ void tile_window(int k, int ntile, int n, int T, int 
 // ---------------------------------------------------------------------------
 // Elastic isotropic / VTI step.
 // ---------------------------------------------------------------------------
-template <bool VTI, int TZ, int TX, bool GRAD>
-__global__ void __launch_bounds__(TZ *TX)
+__device__ __forceinline__ float2 ld2(const float *base, int idx)
+{
+    return *reinterpret_cast<const float2 *>(base + idx);
+}
+__device__ __forceinline__ float pick(const float2 v, int c) { return c ? v.y : v.x; }
+// the five z-samples around cell c of a z-pair from the pairs (z-2,z-1) (z,z+1) (z+2,z+3)
+struct Z5 {
+    float m2, m1, c, p1, p2;
+};
+__device__ __forceinline__ Z5 zsel(const float2 lo, const float2 mid, const float2 hi, int c)
+{
+    Z5 r;
+    if (c == 0) {
+        r.m2 = lo.x; r.m1 = lo.y; r.c = mid.x; r.p1 = mid.y; r.p2 = hi.x;
+    } else {
+        r.m2 = lo.y; r.m1 = mid.x; r.c = mid.y; r.p1 = hi.x; r.p2 = hi.y;
+    }
+    return r;
+}
+
+// Two-sample snapshot loads for the lean path (even index).
+__device__ __forceinline__ float2 snap_load2(const void *base, long long idx, int prec, float inv)
+{
+    if (prec == SNAP_FP32) return *reinterpret_cast<const float2 *>((const float *)base + idx);
+    if (prec == SNAP_BF16) {
+        const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>((const __nv_bfloat16 *)base + idx));
+        return make_float2(v.x * inv, v.y * inv);
+    }
+    const float2 v = __half22float2(*reinterpret_cast<const __half2 *>((const __half *)base + idx));
+    return make_float2(v.x * inv, v.y * inv);
+}
+
+// ---------------------------------------------------------------------------
+// Elastic isotropic / VTI step.  Tiles are TZ = 32*RZ (z) by TX (x) cells on
+// 32*TX threads.  Tiles whose every evaluated point is clear of the SBP
+// boundary bands take the lean path (RZ == 2): each thread owns a z-pair of
+// one column, loads are vectorised and all offsets are compile-time.  Other
+// tiles take the general path, which carries the boundary closures, the SAT
+// terms and the absorbing scaling.  Both paths perform the same arithmetic.
+// ---------------------------------------------------------------------------
+template <bool VTI, int RZ, int TX, bool GRAD>
+__global__ void __launch_bounds__(32 * TX)
 elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C,
              int it, int flags, float dtg)
 {
+    constexpr int TZ = 32 * RZ;
     constexpr int UZ = TZ + 8, UX = TX + 8;
     constexpr int WZ = TZ + 4, WX = TX + 4;
-    constexpr int NT = TZ * TX;
-    __shared__ float U0[UX * UZ], U1[UX * UZ];
-    __shared__ float MU[WX * WZ], Q[WX * WZ];          // mu; lambda (iso) or (1+2eps)2mu (VTI)
-    __shared__ float T0[WX * WZ], T1[WX * WZ];         // iso: ux_x+uz_z ; VTI: tmp_x, tmp_z
-    __shared__ float BX[WX * WZ], CZ[WX * WZ];         // uz_x, ux_z
-    __shared__ float F0[GRAD ? WX * WZ : 1], F1[GRAD ? WX * WZ : 1];
-    __shared__ float red[NT / 32];
+    constexpr int NT = 32 * TX;
+    // dynamic shared memory: see elastic_smem_bytes()
+    extern __shared__ __align__(16) float smem[];
+    float *U0 = smem;
+    float *U1 = U0 + UX * UZ;
+    float *MU = U1 + UX * UZ;
+    float *Q = MU + WX * WZ;       // lambda (iso) or (1+2eps)2mu (VTI)
+    float *T0 = Q + WX * WZ;       // iso: ux_x+uz_z ; VTI: tmp_x
+    float *BX = T0 + WX * WZ;      // uz_x
+    float *CZ = BX + WX * WZ;      // ux_z
+    float *T1 = CZ + WX * WZ;      // VTI: tmp_z
+    float *F0 = T1 + (VTI ? WX * WZ : 0);
+    float *F1 = F0 + (GRAD ? WX * WZ : 0);
+    float *red = F1 + (GRAD ? WX * WZ : 0);
 
     const TileRef tr = tiles[blockIdx.x];
-    const ShotDev &S = shots[tr.shot];
-    const int nt = S.nt;
+    const ShotDev *__restrict__ Sp = shots + tr.shot;
+    const int nt = Sp->nt;
     if (it >= nt - 1) return;
-    const int nx = S.nx, nz = S.nz, ldz = S.ldz;
-    const long long nxz = (long long)nx * ldz;
+    const int nx = Sp->nx, nz = Sp->nz, ldz = Sp->ldz;
+    const int tiles_x = Sp->tiles_x, tiles_z = Sp->tiles_z;
+    const int nxz = nx * ldz;
     int wx0, ownx, wz0, ownz;
-    tile_window(tr.tx, S.tiles_x, nx, TX, wx0, ownx);
-    tile_window(tr.tz, S.tiles_z, nz, TZ, wz0, ownz);
+    tile_window(tr.tx, tiles_x, nx, TX, wx0, ownx);
+    tile_window(tr.tz, tiles_z, nz, TZ, wz0, ownz);
+    // every point this tile evaluates is clear of the SBP boundary bands
+    const bool interior = wx0 >= 6 && wx0 + TX + 6 <= nx && wz0 >= 6 && wz0 + TZ + 6 <= nz;
+    const bool lean = RZ == 2 && interior && (wz0 & 3) == 0;
 
-    const float *curr = S.u[(it + 1) & 1];
-    float *pn = S.u[it & 1];                 // prev in, next out
-    const long long mofs = (long long)S.x0 * M.ldz;
+    const float *__restrict__ curr = Sp->u[(it + 1) & 1];
+    float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
+    const int mld = M.ldz;
+    const long long mofs = (long long)Sp->x0 * mld;
+    const float *__restrict__ mp0 = M.p0 + mofs;
+    const float *__restrict__ mp1 = M.p1 + mofs;
+    const float *__restrict__ mp2 = M.p2 + mofs;
+    const float *__restrict__ qsrc = VTI ? M.fxx + mofs : mp0;
 
-    // ---- phase 1: curr with a 4-cell halo, coefficients with a 2-cell halo
-    for (int i = threadIdx.x; i < UX * UZ; i += NT) {
-        const int sx = i / UZ, sz = i - sx * UZ;
-        const int gx = wx0 - 4 + sx, gz = wz0 - 4 + sz;
-        float a = 0.f, b = 0.f;
-        if (gx >= 0 && gx < nx && gz >= 0 && gz < nz) {
-            const long long o = (long long)gx * ldz + gz;
-            a = curr[o];
-            b = curr[nxz + o];
-        }
-        U0[i] = a;
-        U1[i] = b;
-    }
     const int itf = GRAD ? (nt - 1 - (it + 1)) / C.sub : 0;
     const bool do_grad = GRAD && (flags & F_GRAD) && ((nt - 1 - (it + 1)) % C.sub == 0);
+    const int prec = C.snap_prec;
     float finv = 1.f;
-    if (GRAD && do_grad && C.snap_prec != SNAP_FP32) finv = 1.f / snap_scale(S.snap_amax, itf);
-    for (int i = threadIdx.x; i < WX * WZ; i += NT) {
-        const int sx = i / WZ, sz = i - sx * WZ;
-        const int gx = wx0 - 2 + sx, gz = wz0 - 2 + sz;
-        float m = 0.f, q = 0.f;
-        if (gx >= 0 && gx < nx && gz >= 0 && gz < nz) {
-            const long long o = mofs + (long long)gx * M.ldz + gz;
-            m = M.p1[o];
-            q = VTI ? M.fxx[o] : M.p0[o];
+    if (GRAD && do_grad && prec != SNAP_FP32) finv = 1.f / snap_scale(Sp->snap_amax, itf);
+    const long long slot_elems = Sp->snap_slot;
+    const void *snap = Sp->snap;
+
+    // ---- phase 1: curr with a 4-cell halo, coefficients (and snapshot) with a 2-cell halo
+    if (lean) {
+        constexpr int Q4 = UZ / 4;   // float4 per window row
+        for (int f = threadIdx.x; f < UX * Q4; f += NT) {
+            const int r = f / Q4, q = f - r * Q4;
+            const int o = (wx0 - 4 + r) * ldz + wz0 - 4 + 4 * q;
+            const float4 a = *reinterpret_cast<const float4 *>(curr + o);
+            const float4 b = *reinterpret_cast<const float4 *>(curr + nxz + o);
+            *reinterpret_cast<float4 *>(U0 + r * UZ + 4 * q) = a;
+            *reinterpret_cast<float4 *>(U1 + r * UZ + 4 * q) = b;
         }
-        MU[i] = m;
-        Q[i] = q;
-        if (GRAD) {
-            float f0 = 0.f, f1 = 0.f;
-            if (do_grad && gx >= 0 && gx < nx && gz >= 0 && gz < nz) {
-                const long long o = (long long)itf * S.snap_slot + (long long)gx * ldz + gz;
-                f0 = snap_load(S.snap, o, C.snap_prec, finv);
-                f1 = snap_load(S.snap, o + nxz, C.snap_prec, finv);
+        constexpr int Q2 = WZ / 2;
+        for (int f = threadIdx.x; f < WX * Q2; f += NT) {
+            const int r = f / Q2, q = f - r * Q2;
+            const int o = (wx0 - 2 + r) * mld + wz0 - 2 + 2 * q;
+            *reinterpret_cast<float2 *>(MU + r * WZ + 2 * q) = *reinterpret_cast<const float2 *>(mp1 + o);
+            *reinterpret_cast<float2 *>(Q + r * WZ + 2 * q) = *reinterpret_cast<const float2 *>(qsrc + o);
+            if (GRAD) {
+                float2 f0 = make_float2(0.f, 0.f), f1 = f0;
+                if (do_grad) {
+                    const long long so = (long long)itf * slot_elems + (wx0 - 2 + r) * ldz + wz0 - 2 + 2 * q;
+                    f0 = snap_load2(snap, so, prec, finv);
+                    f1 = snap_load2(snap, so + nxz, prec, finv);
+                }
+                *reinterpret_cast<float2 *>(F0 + r * WZ + 2 * q) = f0;
+                *reinterpret_cast<float2 *>(F1 + r * WZ + 2 * q) = f1;
             }
-            F0[i] = f0;
-            F1[i] = f1;
+        }
+    } else {
+        for (int i = threadIdx.x; i < UX * UZ; i += NT) {
+            const int sx = i / UZ, sz = i - sx * UZ;
+            const int gx = wx0 - 4 + sx, gz = wz0 - 4 + sz;
+            float a = 0.f, b = 0.f;
+            if (gx >= 0 && gx < nx && gz >= 0 && gz < nz) {
+                const int o = gx * ldz + gz;
+                a = curr[o];
+                b = curr[nxz + o];
+            }
+            U0[i] = a;
+            U1[i] = b;
+        }
+        for (int i = threadIdx.x; i < WX * WZ; i += NT) {
+            const int sx = i / WZ, sz = i - sx * WZ;
+            const int gx = wx0 - 2 + sx, gz = wz0 - 2 + sz;
+            float m = 0.f, q = 0.f;
+            const bool in = gx >= 0 && gx < nx && gz >= 0 && gz < nz;
+            if (in) {
+                const int o = gx * mld + gz;
+                m = mp1[o];
+                q = qsrc[o];
+            }
+            MU[i] = m;
+            Q[i] = q;
+            if (GRAD) {
+                float f0 = 0.f, f1 = 0.f;
+                if (do_grad && in) {
+                    const long long o = (long long)itf * slot_elems + gx * ldz + gz;
+                    f0 = snap_load(snap, o, prec, finv);
+                    f1 = snap_load(snap, o + nxz, prec, finv);
+                }
+                F0[i] = f0;
+                F1[i] = f1;
+            }
         }
     }
     __syncthreads();
 
     // ---- phase 2: first derivatives of curr on the tile plus a 2-cell halo
-    for (int i = threadIdx.x; i < WX * WZ; i += NT) {
-        const int sx = i / WZ, sz = i - sx * WZ;
-        const int gx = wx0 - 2 + sx, gz = wz0 - 2 + sz;
-        float t0 = 0.f, t1 = 0.f, bx = 0.f, cz = 0.f;
-        // a closure reads up to 5 samples from its boundary: evaluate only
-        // where the loaded window holds them (other points are never used)
-        const bool okx = (gx >= 4 && gx < nx - 4) || (gx < 4 ? wx0 <= 4 : wx0 + TX + 4 >= nx);
-        const bool okz = (gz >= 4 && gz < nz - 4) || (gz < 4 ? wz0 <= 4 : wz0 + TZ + 4 >= nz);
-        if (gx >= 0 && gx < nx && gz >= 0 && gz < nz && okx && okz) {
-            const int ui = (sx + 2) * UZ + (sz + 2);
-            const float ux_x = d1(U0 + ui, UZ, gx, nx, C.dx, C.sdx);
-            const float uz_z = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
-            bx = d1(U1 + ui, UZ, gx, nx, C.dx, C.sdx);
-            cz = d1(U0 + ui, 1, gz, nz, C.dz, C.sdz);
-            if (!VTI) {
-                t0 = ux_x + uz_z;
-            } else {
-                const long long o = mofs + (long long)gx * M.ldz + gz;
-                const float lb = M.lbis[o], c13 = M.c13[o], lam = M.p0[o];
-                t0 = lb * ux_x + c13 * uz_z;
-                t1 = lam * uz_z + c13 * ux_x;
+    if (lean) {
+        constexpr int Q2 = WZ / 2;
+        for (int f = threadIdx.x; f < WX * Q2; f += NT) {
+            const int sx = f / Q2, pz = 2 * (f - sx * Q2);
+            const int ui = (sx + 2) * UZ + pz + 2;
+            const float2 am2 = ld2(U0, ui - 2 * UZ), am1 = ld2(U0, ui - UZ), ap1 = ld2(U0, ui + UZ), ap2 = ld2(U0, ui + 2 * UZ);
+            const float2 bm2 = ld2(U1, ui - 2 * UZ), bm1 = ld2(U1, ui - UZ), bp1 = ld2(U1, ui + UZ), bp2 = ld2(U1, ui + 2 * UZ);
+            const float2 alo = ld2(U0, ui - 2), amid = ld2(U0, ui), ahi = ld2(U0, ui + 2);
+            const float2 blo = ld2(U1, ui - 2), bmid = ld2(U1, ui), bhi = ld2(U1, ui + 2);
+            float2 t0, t1, bx, cz;
+            float vlb[2], vc13[2], vlam[2];
+            if (VTI) {
+                const long long o = mofs + (long long)(wx0 - 2 + sx) * mld + wz0 - 2 + pz;
+                const float2 lb = *reinterpret_cast<const float2 *>(M.lbis + o);
+                const float2 cc = *reinterpret_cast<const float2 *>(M.c13 + o);
+                const float2 ll = *reinterpret_cast<const float2 *>(M.p0 + o);
+                vlb[0] = lb.x; vlb[1] = lb.y; vc13[0] = cc.x; vc13[1] = cc.y; vlam[0] = ll.x; vlam[1] = ll.y;
             }
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const Z5 az = zsel(alo, amid, ahi, c), bz = zsel(blo, bmid, bhi, c);
+                const float ux_x = d1s(pick(am2, c), pick(am1, c), pick(ap1, c), pick(ap2, c), C.sdx);
+                const float uz_z = d1s(bz.m2, bz.m1, bz.p1, bz.p2, C.sdz);
+                const float vbx = d1s(pick(bm2, c), pick(bm1, c), pick(bp1, c), pick(bp2, c), C.sdx);
+                const float vcz = d1s(az.m2, az.m1, az.p1, az.p2, C.sdz);
+                float vt0, vt1 = 0.f;
+                if (!VTI) vt0 = ux_x + uz_z;
+                else {
+                    vt0 = vlb[c] * ux_x + vc13[c] * uz_z;
+                    vt1 = vlam[c] * uz_z + vc13[c] * ux_x;
+                }
+                if (c == 0) { t0.x = vt0; t1.x = vt1; bx.x = vbx; cz.x = vcz; }
+                else { t0.y = vt0; t1.y = vt1; bx.y = vbx; cz.y = vcz; }
+            }
+            const int wo = sx * WZ + pz;
+            *reinterpret_cast<float2 *>(T0 + wo) = t0;
+            if (VTI) *reinterpret_cast<float2 *>(T1 + wo) = t1;
+            *reinterpret_cast<float2 *>(BX + wo) = bx;
+            *reinterpret_cast<float2 *>(CZ + wo) = cz;
         }
-        T0[i] = t0;
-        T1[i] = t1;
-        BX[i] = bx;
-        CZ[i] = cz;
+    } else {
+        for (int i = threadIdx.x; i < WX * WZ; i += NT) {
+            const int sx = i / WZ, sz = i - sx * WZ;
+            const int gx = wx0 - 2 + sx, gz = wz0 - 2 + sz;
+            const int ui = (sx + 2) * UZ + (sz + 2);
+            // a closure reads up to 5 samples from its boundary: evaluate only
+            // where the loaded window holds them (other points are never used)
+            const bool okx = (gx >= 4 && gx < nx - 4) || (gx < 4 ? wx0 <= 4 : wx0 + TX + 4 >= nx);
+            const bool okz = (gz >= 4 && gz < nz - 4) || (gz < 4 ? wz0 <= 4 : wz0 + TZ + 4 >= nz);
+            const bool ok = gx >= 0 && gx < nx && gz >= 0 && gz < nz && okx && okz;
+            float t0 = 0.f, t1 = 0.f, bx = 0.f, cz = 0.f;
+            if (ok) {
+                const float ux_x = d1(U0 + ui, UZ, gx, nx, C.dx, C.sdx);
+                const float uz_z = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
+                bx = d1(U1 + ui, UZ, gx, nx, C.dx, C.sdx);
+                cz = d1(U0 + ui, 1, gz, nz, C.dz, C.sdz);
+                if (!VTI) {
+                    t0 = ux_x + uz_z;
+                } else {
+                    const long long o = mofs + (long long)gx * mld + gz;
+                    const float lb = M.lbis[o], c13 = M.c13[o], lam = M.p0[o];
+                    t0 = lb * ux_x + c13 * uz_z;
+                    t1 = lam * uz_z + c13 * ux_x;
+                }
+            }
+            T0[i] = t0;
+            if (VTI) T1[i] = t1;
+            BX[i] = bx;
+            CZ[i] = cz;
+        }
     }
     __syncthreads();
 
-    // ---- phase 3: the cell of this thread
-    const int tz = threadIdx.x % TZ, tx = threadIdx.x / TZ;
-    const int gx = wx0 + tx, gz = wz0 + tz;
-    const bool owned = (gx < ownx) && (gz < ownz);
-    const int ui = (tx + 4) * UZ + (tz + 4);
-    const int wi = (tx + 2) * WZ + (tz + 2);
-    const long long cell = (long long)gx * ldz + gz;
-    const long long mcell = mofs + (long long)gx * M.ldz + gz;
-
-    // snapshot of curr (forward), before anything else as the reference does
-    if ((flags & F_STORE) && (it % C.sub == 0) && owned) {
-        const int slot = it / C.sub;
-        const float sc = C.snap_prec == SNAP_FP32 ? 1.f : snap_scale(S.snap_amax, slot);
-        const long long o = (long long)slot * S.snap_slot + cell;
-        snap_store(S.snap, o, C.snap_prec, U0[ui], sc);
-        snap_store(S.snap, o + nxz, C.snap_prec, U1[ui], sc);
-    }
+    // ---- phase 3
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile_id = tr.tz * tiles_x + tr.tx;
 
     // receivers (forward): one thread per receiver of this tile
     if (flags & F_EXTRACT) {
-        const int tile_id = tr.tz * S.tiles_x + tr.tx;
-        const int e0 = S.ext_off[tile_id], e1 = S.ext_off[tile_id + 1];
+        const int e0 = Sp->ext_off[tile_id], e1 = Sp->ext_off[tile_id + 1];
         for (int e = e0 + threadIdx.x; e < e1; e += NT) {
-            const ExtEntry E = S.ext[e];
+            const ExtEntry &E = Sp->ext[e];
             const float *U = E.comp == 0 ? U0 : U1;
+            const int base = (E.gx0 - wx0 + 4) * UZ + (E.gz0 - wz0 + 4);
             float o = 0.f;
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
-                for (int b = 0; b < 3; b++)
-                    o += E.w[a * 3 + b] * U[(E.gx0 + a - wx0 + 4) * UZ + (E.gz0 + b - wz0 + 4)];
-            S.rcv[(long long)it * S.nrcv + E.row] = o;
+                for (int b = 0; b < 3; b++) o += E.w[a * 3 + b] * U[base + a * UZ + b];
+            Sp->rcv[(long long)it * Sp->nrcv + E.row] = o;
         }
     }
+    const int e0 = Sp->inj_off[tile_id], e1 = Sp->inj_off[tile_id + 1];
+    const float *srcrow = Sp->src + (long long)it * Sp->nsrc;
+    const bool store = (flags & F_STORE) && (it % C.sub == 0);
+    float amax = 0.f;
 
-    float n0 = 0.f, n1 = 0.f;
-    if (owned) {
-        // interior operators, in the reference's order of accumulation
-        const float mu = MU[wi];
-        if (!VTI) {
-            d2acc(n0, U0 + ui, UZ, MU + wi, WZ, 2.f, gx, nx, C.inv_d2x, C.d2x);   // Dxx_var<2mu>(ux)
-            d2acc(n1, U1 + ui, 1, MU + wi, 1, 2.f, gz, nz, C.inv_d2z, C.d2z);     // Dzz_var<2mu>(uz)
-        } else {
-            d2acc(n0, U0 + ui, UZ, Q + wi, WZ, 1.f, gx, nx, C.inv_d2x, C.d2x);    // Dxx_var<(1+2eps)2mu>(ux)
-            d2acc(n1, U1 + ui, 1, MU + wi, 1, 2.f, gz, nz, C.inv_d2z, C.d2z);     // Dzz_var<2mu>(uz)
+    if (lean) {
+        const int gx = wx0 + warp;
+        const int gz0 = wz0 + 2 * lane;
+        const int ui = (warp + 4) * UZ + 2 * lane + 4;
+        const int wi = (warp + 2) * WZ + 2 * lane + 2;
+        const int cell0 = gx * ldz + gz0;
+        // x-direction samples
+        const float2 am2 = ld2(U0, ui - 2 * UZ), am1 = ld2(U0, ui - UZ), a00 = ld2(U0, ui), ap1 = ld2(U0, ui + UZ), ap2 = ld2(U0, ui + 2 * UZ);
+        const float2 bm2 = ld2(U1, ui - 2 * UZ), bm1 = ld2(U1, ui - UZ), b00 = ld2(U1, ui), bp1 = ld2(U1, ui + UZ), bp2 = ld2(U1, ui + 2 * UZ);
+        const float2 alo = ld2(U0, ui - 2), ahi = ld2(U0, ui + 2), blo = ld2(U1, ui - 2), bhi = ld2(U1, ui + 2);
+        const float2 mm2 = ld2(MU, wi - 2 * WZ), mm1 = ld2(MU, wi - WZ), m00 = ld2(MU, wi), mp1v = ld2(MU, wi + WZ), mp2v = ld2(MU, wi + 2 * WZ);
+        const float2 mlo = ld2(MU, wi - 2), mhi = ld2(MU, wi + 2);
+        const float2 qm2 = ld2(Q, wi - 2 * WZ), qm1 = ld2(Q, wi - WZ), qp1 = ld2(Q, wi + WZ), qp2 = ld2(Q, wi + 2 * WZ);
+        const float2 tm2 = ld2(T0, wi - 2 * WZ), tm1 = ld2(T0, wi - WZ), tp1 = ld2(T0, wi + WZ), tp2 = ld2(T0, wi + 2 * WZ);
+        const float *TZS = VTI ? T1 : T0;
+        const float2 tlo = ld2(TZS, wi - 2), tmid = ld2(TZS, wi), thi = ld2(TZS, wi + 2);
+        const float2 cm2 = ld2(CZ, wi - 2 * WZ), cm1 = ld2(CZ, wi - WZ), cp1 = ld2(CZ, wi + WZ), cp2 = ld2(CZ, wi + 2 * WZ);
+        const float2 xlo = ld2(BX, wi - 2), xmid = ld2(BX, wi), xhi = ld2(BX, wi + 2);
+        const float2 tzv2 = *reinterpret_cast<const float2 *>(Sp->tz + gz0);
+        const float txv = Sp->tx[gx];
+        float2 pv0 = *reinterpret_cast<const float2 *>(pn + cell0);
+        float2 pv1 = *reinterpret_cast<const float2 *>(pn + nxz + cell0);
+        const float2 rho2 = *reinterpret_cast<const float2 *>(mp2 + gx * mld + gz0);
+        if (store) {
+            const int slot = it / C.sub;
+            const float sc = prec == SNAP_FP32 ? 1.f : snap_scale(Sp->snap_amax, slot);
+            const long long o = (long long)slot * slot_elems + cell0;
+            snap_store(Sp->snap, o, prec, a00.x, sc);
+            snap_store(Sp->snap, o + 1, prec, a00.y, sc);
+            snap_store(Sp->snap, o + nxz, prec, b00.x, sc);
+            snap_store(Sp->snap, o + nxz + 1, prec, b00.y, sc);
         }
-        d2acc(n1, U1 + ui, UZ, MU + wi, WZ, 1.f, gx, nx, C.inv_d2x, C.d2x);       // Dxx_var<mu>(uz)
-        d2acc(n0, U0 + ui, 1, MU + wi, 1, 1.f, gz, nz, C.inv_d2z, C.d2z);         // Dzz_var<mu>(ux)
-        if (!VTI) {
-            n0 += md1(T0 + wi, Q + wi, WZ, gx, nx, C.adx);                        // mult_Dx(lambda, tmp)
-            n1 += md1(T0 + wi, Q + wi, 1, gz, nz, C.adz);                         // mult_Dz(lambda, tmp)
-        } else {
-            n0 += d1(T0 + wi, WZ, gx, nx, C.dx, C.sdx);                           // Dx(tmp_x)
-            n1 += d1(T1 + wi, 1, gz, nz, C.dz, C.sdz);                            // Dz(tmp_z)
-        }
-        n1 += md1(CZ + wi, MU + wi, WZ, gx, nx, C.adx);                           // mult_Dx(mu, ux_z)
-        n0 += md1(BX + wi, MU + wi, 1, gz, nz, C.adz);                            // mult_Dz(mu, uz_x)
-
-        // sources
-        {
-            const int tile_id = tr.tz * S.tiles_x + tr.tx;
-            const int e0 = S.inj_off[tile_id], e1 = S.inj_off[tile_id + 1];
-            const float *src = S.src + (long long)it * S.nsrc;
+        float2 out0, out1;
+        float vax0[2], vaz1[2];
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            const int gz = gz0 + c;
+            const Z5 az = zsel(alo, a00, ahi, c), bz = zsel(blo, b00, bhi, c), mz = zsel(mlo, m00, mhi, c);
+            const Brk bkx = brk5(pick(mm2, c), pick(mm1, c), pick(m00, c), pick(mp1v, c), pick(mp2v, c));
+            const Brk bkz = brk5(mz.m2, mz.m1, mz.c, mz.p1, mz.p2);
+            float n0, n1;
+            if (!VTI) n0 = d2s(0.f, twice(bkx), pick(am2, c), pick(am1, c), pick(a00, c), pick(ap1, c), pick(ap2, c), C.inv_d2x);
+            else {
+                const float2 q00 = ld2(Q, wi);
+                n0 = d2s(0.f, brk5(pick(qm2, c), pick(qm1, c), pick(q00, c), pick(qp1, c), pick(qp2, c)), pick(am2, c),
+                         pick(am1, c), pick(a00, c), pick(ap1, c), pick(ap2, c), C.inv_d2x);
+            }
+            n1 = d2s(0.f, twice(bkz), bz.m2, bz.m1, bz.c, bz.p1, bz.p2, C.inv_d2z);
+            n1 = d2s(n1, bkx, pick(bm2, c), pick(bm1, c), pick(b00, c), pick(bp1, c), pick(bp2, c), C.inv_d2x);
+            n0 = d2s(n0, bkz, az.m2, az.m1, az.c, az.p1, az.p2, C.inv_d2z);
+            const Z5 tz5 = zsel(tlo, tmid, thi, c);
+            if (!VTI) {
+                const float2 qlo = ld2(Q, wi - 2), qmid = ld2(Q, wi), qhi = ld2(Q, wi + 2);
+                const Z5 qz = zsel(qlo, qmid, qhi, c);
+                n0 += md1s(pick(tm2, c), pick(qm2, c), pick(tm1, c), pick(qm1, c), pick(tp1, c), pick(qp1, c),
+                           pick(tp2, c), pick(qp2, c), C.adx);
+                n1 += md1s(tz5.m2, qz.m2, tz5.m1, qz.m1, tz5.p1, qz.p1, tz5.p2, qz.p2, C.adz);
+            } else {
+                n0 += d1s(pick(tm2, c), pick(tm1, c), pick(tp1, c), pick(tp2, c), C.sdx);
+                n1 += d1s(tz5.m2, tz5.m1, tz5.p1, tz5.p2, C.sdz);
+            }
+            n1 += md1s(pick(cm2, c), pick(mm2, c), pick(cm1, c), pick(mm1, c), pick(cp1, c), pick(mp1v, c),
+                       pick(cp2, c), pick(mp2v, c), C.adx);
+            const Z5 xz = zsel(xlo, xmid, xhi, c);
+            n0 += md1s(xz.m2, mz.m2, xz.m1, mz.m1, xz.p1, mz.p1, xz.p2, mz.p2, C.adz);
+            // sources
             for (int e = e0; e < e1; e++) {
-                const InjEntry E = S.inj[e];
+                const InjEntry &E = Sp->inj[e];
                 if (E.gx == gx && E.gz == gz) {
-                    const float c = E.mt ? (E.wa * src[E.ia] - E.wb * src[E.ib]) : E.wa * src[E.ia];
-                    if (E.comp == 0) n0 += c;
-                    else n1 += c;
+                    const float v = E.mt ? (E.wa * srcrow[E.ia] - E.wb * srcrow[E.ib]) : E.wa * srcrow[E.ia];
+                    if (E.comp == 0) n0 += v;
+                    else n1 += v;
                 }
             }
-        }
-
-        // previous field, with the taper it received at the end of the last step
-        const float tzv = S.tz[gz], txv = S.tx[gx];
-        float p0 = pn[cell], p1 = pn[nxz + cell];
-        if (it > 0) {
-            p0 = p0 * tzv * txv;
-            p1 = p1 * tzv * txv;
-        }
-
-        // SAT closures (spatial_operators.hpp:160-822), in the reference's side order
-        const bool edge = gz == 0 || gz == nz - 1 || gx == 0 || gx == nx - 1;
-        if (edge) {
-            const float lam = VTI ? M.p0[mcell] : Q[wi];
-            const float rho = M.p2[mcell];
-            const float c13 = VTI ? M.c13[mcell] : lam;
-            const float fxx = VTI ? Q[wi] : 2 * mu;
-            const float lamx = VTI ? M.lbis[mcell] : lam;
-            const float eps = VTI ? M.eps[mcell] : 0.f;
-            const float imp_s = 0.5f * sqrtf(mu * rho);
-            const float imp_p = 0.5f * sqrtf((lam + 2 * mu) * rho);
-            const float imp_px = VTI ? 0.5f * sqrtf((1 + 2 * eps) * (lam + 2 * mu) * rho) : imp_p;
-            for (int side = 0; side < 4; side++) {
-                const int bc = C.bc[side];
-                if (bc != 1 && bc != 2) continue;
-                const bool ab = bc == 2;
-                if (side < 2) {
-                    if (gz != (side == 0 ? 0 : nz - 1)) continue;
-                    const int in = side == 0 ? 1 : -1;
-                    const float sg = side == 0 ? -1.f : 1.f;
-                    // next0: f1 = f2 = mu, in1 = uz (along x), in2 = ux (outward)
-                    {
-                        float t = (sg * mu) * tsum(U1 + ui, UZ, gx, nx) / C.dx + mu * nsum(U0 + ui, in) / C.dz;
-                        if (ab) t = t - imp_s * p0 / C.dt;
-                        n0 = n0 - C.sat_z * t;
-                    }
-                    // next1: f1 = lambda (c13), f2 = 2mu, in1 = ux, in2 = uz ; then -H^-1(lambda Dz uz)_0
-                    {
-                        float t = (sg * c13) * tsum(U0 + ui, UZ, gx, nx) / C.dx + (2 * mu) * nsum(U1 + ui, in) / C.dz;
-                        if (ab) t = t - imp_p * p1 / C.dt;
-                        n1 = n1 - C.sat_z * t;
-                        n1 = n1 - C.nsat_z * lam * ndsum(U1 + ui, in);
-                    }
-                } else {
-                    if (gx != (side == 2 ? 0 : nx - 1)) continue;
-                    const int in = side == 2 ? UZ : -UZ;
-                    const float sg = side == 2 ? -1.f : 1.f;
-                    // next0: f1 = lambda (c13), f2 = 2mu ((1+2eps)2mu), in1 = uz (along z), in2 = ux
-                    {
-                        float t = (sg * c13) * tsum(U1 + ui, 1, gz, nz) / C.dz + fxx * nsum(U0 + ui, in) / C.dx;
-                        if (ab) t = t - imp_px * p0 / C.dt;
-                        n0 = n0 - C.sat_x * t;
-                        n0 = n0 - C.nsat_x * lamx * ndsum(U0 + ui, in);
-                    }
-                    // next1: f1 = f2 = mu, in1 = ux, in2 = uz
-                    {
-                        float t = (sg * mu) * tsum(U0 + ui, 1, gz, nz) / C.dz + mu * nsum(U1 + ui, in) / C.dx;
-                        if (ab) t = t - imp_s * p1 / C.dt;
-                        n1 = n1 - C.sat_x * t;
-                    }
-                }
+            const float tzv = pick(tzv2, c);
+            float p0 = pick(pv0, c), p1 = pick(pv1, c);
+            if (it > 0) {
+                p0 = p0 * tzv * txv;
+                p1 = p1 * tzv * txv;
             }
+            const float rho = pick(rho2, c);
+            n0 = C.dt2 * n0 / rho + 2 * az.c - p0;
+            n1 = C.dt2 * n1 / rho + 2 * bz.c - p1;
+            n0 = n0 * tzv * txv;
+            n1 = n1 * tzv * txv;
+            if (c == 0) { out0.x = n0; out1.x = n1; } else { out0.y = n0; out1.y = n1; }
+            amax = fmaxf(amax, fmaxf(fabsf(n0), fabsf(n1)));
+            vax0[c] = d1s(pick(am2, c), pick(am1, c), pick(ap1, c), pick(ap2, c), C.sdx);
+            vaz1[c] = d1s(bz.m2, bz.m1, bz.p1, bz.p2, C.sdz);
         }
+        *reinterpret_cast<float2 *>(pn + cell0) = out0;
+        *reinterpret_cast<float2 *>(pn + nxz + cell0) = out1;
 
-        // leapfrog (we_op.cpp:825-830)
-        const float rho = M.p2[mcell];
-        n0 = C.dt2 * n0 / rho + 2 * U0[ui] - p0;
-        n1 = C.dt2 * n1 / rho + 2 * U1[ui] - p1;
-
-        // implicit absorbing scaling (esat_scale_boundaries)
-        if (edge) {
-            const int per = 2 * nx + 2 * nz;
-            int k = -1;
-            if (gz == 0) k = gx;
-            else if (gz == nz - 1) k = nx + gx;
-            else if (gx == 0) k = 2 * nx + gz;
-            else if (gx == nx - 1) k = 2 * nx + nz + gz;
-            n0 = n0 / S.den[k];
-            n1 = n1 / S.den[per + k];
-        }
-
-        // taper of next
-        n0 = n0 * tzv * txv;
-        n1 = n1 * tzv * txv;
-
-        pn[cell] = n0;
-        pn[nxz + cell] = n1;
-
-        // imaging condition for the next adjoint sample (we_op.cpp:505-562)
         if (GRAD && do_grad) {
-            const float ax0 = d1(U0 + ui, UZ, gx, nx, C.dx, C.sdx);
-            const float az1 = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
-            const float az0 = CZ[wi], ax1 = BX[wi];
-            const float t0 = d1(F0 + wi, WZ, gx, nx, C.dx, C.sdx);
-            const float t1 = d1(F1 + wi, 1, gz, nz, C.dz, C.sdz);
-            const float t2 = d1(F1 + wi, WZ, gx, nx, C.dx, C.sdx);
-            const float t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
+            const float2 f0m2 = ld2(F0, wi - 2 * WZ), f0m1 = ld2(F0, wi - WZ), f0p1 = ld2(F0, wi + WZ), f0p2 = ld2(F0, wi + 2 * WZ);
+            const float2 f1m2 = ld2(F1, wi - 2 * WZ), f1m1 = ld2(F1, wi - WZ), f1p1 = ld2(F1, wi + WZ), f1p2 = ld2(F1, wi + 2 * WZ);
+            const float2 f0lo = ld2(F0, wi - 2), f0c = ld2(F0, wi), f0hi = ld2(F0, wi + 2);
+            const float2 f1lo = ld2(F1, wi - 2), f1c = ld2(F1, wi), f1hi = ld2(F1, wi + 2);
             const int last = nt / C.sub;
-            const float f0 = F0[wi], f1 = F1[wi];
-            float fp0 = 0.f, fp1 = 0.f, fm0 = 0.f, fm1 = 0.f;
+            float2 fp0 = make_float2(0.f, 0.f), fp1 = fp0, fm0 = fp0, fm1 = fp0;
             if (itf + 1 <= last) {
-                const float inv = C.snap_prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(S.snap_amax, itf + 1);
-                const long long o = (long long)(itf + 1) * S.snap_slot + cell;
-                fp0 = snap_load(S.snap, o, C.snap_prec, inv);
-                fp1 = snap_load(S.snap, o + nxz, C.snap_prec, inv);
+                const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf + 1);
+                const long long o = (long long)(itf + 1) * slot_elems + cell0;
+                fp0 = snap_load2(snap, o, prec, inv);
+                fp1 = snap_load2(snap, o + nxz, prec, inv);
             }
             if (itf > 0) {
-                const float inv = C.snap_prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(S.snap_amax, itf - 1);
-                const long long o = (long long)(itf - 1) * S.snap_slot + cell;
-                fm0 = snap_load(S.snap, o, C.snap_prec, inv);
-                fm1 = snap_load(S.snap, o + nxz, C.snap_prec, inv);
+                const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
+                const long long o = (long long)(itf - 1) * slot_elems + cell0;
+                fm0 = snap_load2(snap, o, prec, inv);
+                fm1 = snap_load2(snap, o + nxz, prec, inv);
             }
-            float dl, dm;
-            if (!VTI) {
-                dl = 0.f;
-                dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
-            } else {
-                const float e2 = 1 + 2 * M.eps[mcell];
-                const float v2 = M.gv2[mcell], v3 = M.gv3[mcell];
-                dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
-                dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
+            float2 v2v = make_float2(0.f, 0.f), v3v = v2v, epsv = v2v;
+            if (VTI) {
+                const long long mo = mofs + (long long)gx * mld + gz0;
+                v2v = *reinterpret_cast<const float2 *>(M.gv2 + mo);
+                v3v = *reinterpret_cast<const float2 *>(M.gv3 + mo);
+                epsv = *reinterpret_cast<const float2 *>(M.eps + mo);
             }
-            float *g0 = S.grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
-            const float gw = S.gwt[itf];
+            float *g0 = Sp->grad + cell0, *g1 = g0 + nxz, *g2 = g1 + nxz;
+            float2 G0 = *reinterpret_cast<float2 *>(g0), G1 = *reinterpret_cast<float2 *>(g1), G2 = *reinterpret_cast<float2 *>(g2);
+            const float gw = Sp->gwt[itf];
             const double wdt = (double)gw * 1.0 / (double)dtg;
-            if (itf > 0 && itf < last) {
-                if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
-                else *g0 = *g0 + gw * dtg * dl;
-                *g1 = *g1 + gw * dtg * dm;
-                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
-            } else if (itf == 0) {
-                const double wh = (double)gw * 0.5 * (double)dtg;
-                if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
-                else *g0 = (float)((double)*g0 + wh * (double)dl);
-                *g1 = (float)((double)*g1 + wh * (double)dm);
-                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const float ax0 = vax0[c], az1 = vaz1[c];
+                const float az0 = pick(ld2(CZ, wi), c), ax1 = pick(xmid, c);
+                const Z5 f0z = zsel(f0lo, f0c, f0hi, c), f1z = zsel(f1lo, f1c, f1hi, c);
+                const float t0 = d1s(pick(f0m2, c), pick(f0m1, c), pick(f0p1, c), pick(f0p2, c), C.sdx);
+                const float t1 = d1s(f1z.m2, f1z.m1, f1z.p1, f1z.p2, C.sdz);
+                const float t2 = d1s(pick(f1m2, c), pick(f1m1, c), pick(f1p1, c), pick(f1p2, c), C.sdx);
+                const float t3 = d1s(f0z.m2, f0z.m1, f0z.p1, f0z.p2, C.sdz);
+                const float f0 = f0z.c, f1 = f1z.c;
+                const float a0 = pick(out0, c), a1 = pick(out1, c);
+                float dl, dm;
+                if (!VTI) {
+                    dl = 0.f;
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
+                } else {
+                    const float e2 = 1 + 2 * pick(epsv, c);
+                    const float v2 = pick(v2v, c), v3 = pick(v3v, c);
+                    dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
+                }
+                float g0v = pick(G0, c), g1v = pick(G1, c), g2v = pick(G2, c);
+                const float fp0c = pick(fp0, c), fp1c = pick(fp1, c), fm0c = pick(fm0, c), fm1c = pick(fm1, c);
+                if (itf > 0 && itf < last) {
+                    if (!VTI) g0v = g0v + gw * dtg * (ax0 + az1) * (t0 + t1);
+                    else g0v = g0v + gw * dtg * dl;
+                    g1v = g1v + gw * dtg * dm;
+                    g2v = (float)((double)g2v + wdt * (double)(a0 * (fp0c - 2 * f0 + fm0c) + a1 * (fp1c - 2 * f1 + fm1c)));
+                } else if (itf == 0) {
+                    const double wh = (double)gw * 0.5 * (double)dtg;
+                    if (!VTI) g0v = (float)((double)g0v + wh * (double)(ax0 + az1) * (double)(t0 + t1));
+                    else g0v = (float)((double)g0v + wh * (double)dl);
+                    g1v = (float)((double)g1v + wh * (double)dm);
+                    g2v = (float)((double)g2v + wdt * (double)(a0 * (fp0c - f0) + a1 * (fp1c - f1)));
+                } else {
+                    if (!VTI) g0v = g0v + gw * dtg * (ax0 + az1) * (t0 + t1);
+                    else g0v = g0v + gw * dtg * dl;
+                    g1v = g1v + gw * dtg * dm;
+                    g2v = (float)((double)g2v + wdt * (double)(a0 * (-f0 + fm0c) + a1 * (-f1 + fm1c)));
+                }
+                if (c == 0) { G0.x = g0v; G1.x = g1v; G2.x = g2v; } else { G0.y = g0v; G1.y = g1v; G2.y = g2v; }
+            }
+            *reinterpret_cast<float2 *>(g0) = G0;
+            *reinterpret_cast<float2 *>(g1) = G1;
+            *reinterpret_cast<float2 *>(g2) = G2;
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < RZ; h++) {
+            const int tz = lane + 32 * h, tx = warp;
+            const int gx = wx0 + tx, gz = wz0 + tz;
+            const bool owned = (gx < ownx) && (gz < ownz);
+            if (!owned) continue;
+            const int ui = (tx + 4) * UZ + (tz + 4);
+            const int wi = (tx + 2) * WZ + (tz + 2);
+            const int cell = gx * ldz + gz;
+            const int mcell = gx * mld + gz;
+            if (store) {
+                const int slot = it / C.sub;
+                const float sc = prec == SNAP_FP32 ? 1.f : snap_scale(Sp->snap_amax, slot);
+                const long long o = (long long)slot * slot_elems + cell;
+                snap_store(Sp->snap, o, prec, U0[ui], sc);
+                snap_store(Sp->snap, o + nxz, prec, U1[ui], sc);
+            }
+            const float mu = MU[wi];
+            float n0 = 0.f, n1 = 0.f;
+            if (!VTI) {
+                d2acc(n0, U0 + ui, UZ, MU + wi, WZ, 2.f, gx, nx, C.inv_d2x, C.d2x);
+                d2acc(n1, U1 + ui, 1, MU + wi, 1, 2.f, gz, nz, C.inv_d2z, C.d2z);
             } else {
-                if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
-                else *g0 = *g0 + gw * dtg * dl;
-                *g1 = *g1 + gw * dtg * dm;
-                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
+                d2acc(n0, U0 + ui, UZ, Q + wi, WZ, 1.f, gx, nx, C.inv_d2x, C.d2x);
+                d2acc(n1, U1 + ui, 1, MU + wi, 1, 2.f, gz, nz, C.inv_d2z, C.d2z);
+            }
+            d2acc(n1, U1 + ui, UZ, MU + wi, WZ, 1.f, gx, nx, C.inv_d2x, C.d2x);
+            d2acc(n0, U0 + ui, 1, MU + wi, 1, 1.f, gz, nz, C.inv_d2z, C.d2z);
+            if (!VTI) {
+                n0 += md1(T0 + wi, Q + wi, WZ, gx, nx, C.adx);
+                n1 += md1(T0 + wi, Q + wi, 1, gz, nz, C.adz);
+            } else {
+                n0 += d1(T0 + wi, WZ, gx, nx, C.dx, C.sdx);
+                n1 += d1(T1 + wi, 1, gz, nz, C.dz, C.sdz);
+            }
+            n1 += md1(CZ + wi, MU + wi, WZ, gx, nx, C.adx);
+            n0 += md1(BX + wi, MU + wi, 1, gz, nz, C.adz);
+
+            for (int e = e0; e < e1; e++) {
+                const InjEntry &E = Sp->inj[e];
+                if (E.gx == gx && E.gz == gz) {
+                    const float v = E.mt ? (E.wa * srcrow[E.ia] - E.wb * srcrow[E.ib]) : E.wa * srcrow[E.ia];
+                    if (E.comp == 0) n0 += v;
+                    else n1 += v;
+                }
+            }
+
+            const float tzv = Sp->tz[gz], txv = Sp->tx[gx];
+            float p0 = pn[cell], p1 = pn[nxz + cell];
+            if (it > 0) {
+                p0 = p0 * tzv * txv;
+                p1 = p1 * tzv * txv;
+            }
+            const float rho = mp2[mcell];
+
+            // SAT closures (spatial_operators.hpp:160-822), in the reference's side order
+            const bool edge = gz == 0 || gz == nz - 1 || gx == 0 || gx == nx - 1;
+            if (edge) {
+                const float lam = VTI ? mp0[mcell] : Q[wi];
+                const float c13 = VTI ? M.c13[mofs + mcell] : lam;
+                const float fxx = VTI ? Q[wi] : 2 * mu;
+                const float lamx = VTI ? M.lbis[mofs + mcell] : lam;
+                const float eps = VTI ? M.eps[mofs + mcell] : 0.f;
+                const float imp_s = 0.5f * sqrtf(mu * rho);
+                const float imp_p = 0.5f * sqrtf((lam + 2 * mu) * rho);
+                const float imp_px = VTI ? 0.5f * sqrtf((1 + 2 * eps) * (lam + 2 * mu) * rho) : imp_p;
+#pragma unroll
+                for (int side = 0; side < 4; side++) {
+                    const int bc = C.bc[side];
+                    if (bc != 1 && bc != 2) continue;
+                    const bool ab = bc == 2;
+                    if (side < 2) {
+                        if (gz != (side == 0 ? 0 : nz - 1)) continue;
+                        const int in = side == 0 ? 1 : -1;
+                        const float sg = side == 0 ? -1.f : 1.f;
+                        {
+                            float t = (sg * mu) * tsum(U1 + ui, UZ, gx, nx) / C.dx + mu * nsum(U0 + ui, in) / C.dz;
+                            if (ab) t = t - imp_s * p0 / C.dt;
+                            n0 = n0 - C.sat_z * t;
+                        }
+                        {
+                            float t = (sg * c13) * tsum(U0 + ui, UZ, gx, nx) / C.dx + (2 * mu) * nsum(U1 + ui, in) / C.dz;
+                            if (ab) t = t - imp_p * p1 / C.dt;
+                            n1 = n1 - C.sat_z * t;
+                            n1 = n1 - C.nsat_z * lam * ndsum(U1 + ui, in);
+                        }
+                    } else {
+                        if (gx != (side == 2 ? 0 : nx - 1)) continue;
+                        const int in = side == 2 ? UZ : -UZ;
+                        const float sg = side == 2 ? -1.f : 1.f;
+                        {
+                            float t = (sg * c13) * tsum(U1 + ui, 1, gz, nz) / C.dz + fxx * nsum(U0 + ui, in) / C.dx;
+                            if (ab) t = t - imp_px * p0 / C.dt;
+                            n0 = n0 - C.sat_x * t;
+                            n0 = n0 - C.nsat_x * lamx * ndsum(U0 + ui, in);
+                        }
+                        {
+                            float t = (sg * mu) * tsum(U0 + ui, 1, gz, nz) / C.dz + mu * nsum(U1 + ui, in) / C.dx;
+                            if (ab) t = t - imp_s * p1 / C.dt;
+                            n1 = n1 - C.sat_x * t;
+                        }
+                    }
+                }
+            }
+
+            n0 = C.dt2 * n0 / rho + 2 * U0[ui] - p0;
+            n1 = C.dt2 * n1 / rho + 2 * U1[ui] - p1;
+
+            if (edge) {
+                const int per = 2 * nx + 2 * nz;
+                int k;
+                if (gz == 0) k = gx;
+                else if (gz == nz - 1) k = nx + gx;
+                else if (gx == 0) k = 2 * nx + gz;
+                else k = 2 * nx + nz + gz;
+                n0 = n0 / Sp->den[k];
+                n1 = n1 / Sp->den[per + k];
+            }
+
+            n0 = n0 * tzv * txv;
+            n1 = n1 * tzv * txv;
+            pn[cell] = n0;
+            pn[nxz + cell] = n1;
+            amax = fmaxf(amax, fmaxf(fabsf(n0), fabsf(n1)));
+
+            if (GRAD && do_grad) {
+                const float ax0 = d1(U0 + ui, UZ, gx, nx, C.dx, C.sdx);
+                const float az1 = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
+                const float t0 = d1(F0 + wi, WZ, gx, nx, C.dx, C.sdx);
+                const float t1 = d1(F1 + wi, 1, gz, nz, C.dz, C.sdz);
+                const float t2 = d1(F1 + wi, WZ, gx, nx, C.dx, C.sdx);
+                const float t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
+                const float az0 = CZ[wi], ax1 = BX[wi];
+                const int last = nt / C.sub;
+                const float f0 = F0[wi], f1 = F1[wi];
+                float fp0 = 0.f, fp1 = 0.f, fm0 = 0.f, fm1 = 0.f;
+                if (itf + 1 <= last) {
+                    const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf + 1);
+                    const long long o = (long long)(itf + 1) * slot_elems + cell;
+                    fp0 = snap_load(snap, o, prec, inv);
+                    fp1 = snap_load(snap, o + nxz, prec, inv);
+                }
+                if (itf > 0) {
+                    const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
+                    const long long o = (long long)(itf - 1) * slot_elems + cell;
+                    fm0 = snap_load(snap, o, prec, inv);
+                    fm1 = snap_load(snap, o + nxz, prec, inv);
+                }
+                float dl, dm;
+                if (!VTI) {
+                    dl = 0.f;
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
+                } else {
+                    const long long mo = mofs + mcell;
+                    const float e2 = 1 + 2 * M.eps[mo];
+                    const float v2 = M.gv2[mo], v3 = M.gv3[mo];
+                    dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
+                }
+                float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
+                const float gw = Sp->gwt[itf];
+                const double wdt = (double)gw * 1.0 / (double)dtg;
+                if (itf > 0 && itf < last) {
+                    if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                    else *g0 = *g0 + gw * dtg * dl;
+                    *g1 = *g1 + gw * dtg * dm;
+                    *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
+                } else if (itf == 0) {
+                    const double wh = (double)gw * 0.5 * (double)dtg;
+                    if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
+                    else *g0 = (float)((double)*g0 + wh * (double)dl);
+                    *g1 = (float)((double)*g1 + wh * (double)dm);
+                    *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
+                } else {
+                    if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                    else *g0 = *g0 + gw * dtg * dl;
+                    *g1 = *g1 + gw * dtg * dm;
+                    *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
+                }
             }
         }
     }
 
     // max |next| for the scale of the next 16-bit snapshot
     if ((flags & F_AMAX) && ((it + 1) % C.sub == 0)) {
-        float m = owned ? fmaxf(fabsf(n0), fabsf(n1)) : 0.f;
+        float m = amax;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        if (lane == 0) red[warp] = m;
         __syncthreads();
         if (threadIdx.x < 32) {
             m = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.f;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (threadIdx.x == 0 && m > 0.f) atomicMax(S.snap_amax + (it + 1) / C.sub, __float_as_uint(m));
+            if (threadIdx.x == 0 && m > 0.f) atomicMax(Sp->snap_amax + (it + 1) / C.sub, __float_as_uint(m));
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Initial state: zero both buffers' touched cells is done by memset; this
-// scatters the precomputed first "prev" samples (we_op.cpp:657-663).
+// Initial state (we_op.cpp:657-663): inject sample 0 into a zeroed field and
+// scale by dt^2/(2 rho) in double.  One thread per touched cell, entries in
+// the reference's order.
 // ---------------------------------------------------------------------------
-__global__ void scatter_init(const ShotDev *__restrict__ shots, int nshots, const InitEntry *__restrict__ ent,
-                             const int *__restrict__ off)
+__global__ void init_state(const ShotDev *__restrict__ shots, int nshots, const InitCell *__restrict__ cells,
+                           const int *__restrict__ off, const int *__restrict__ idx)
 {
     const int s = blockIdx.x;
     if (s >= nshots) return;
     const ShotDev &S = shots[s];
     const long long nxz = (long long)S.nx * S.ldz;
-    for (int e = off[s] + threadIdx.x; e < off[s + 1]; e += blockDim.x) {
-        const InitEntry E = ent[e];
-        S.u[0][E.comp * nxz + (long long)E.gx * S.ldz + E.gz] = E.val;
+    const float *src0 = S.src;   // time sample 0 of the time-major traces
+    for (int c = off[s] + threadIdx.x; c < off[s + 1]; c += blockDim.x) {
+        const InitCell q = cells[c];
+        float acc = 0.f;
+        for (int k = q.i0; k < q.i1; k++) {
+            const InjEntry &E = S.inj[idx[k]];
+            acc += E.mt ? (E.wa * src0[E.ia] - E.wb * src0[E.ib]) : E.wa * src0[E.ia];
+        }
+        S.u[0][q.comp * nxz + (long long)q.gx * S.ldz + q.gz] = (float)((double)acc * q.factor);
     }
 }
 
@@ -479,21 +781,39 @@ void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const 
     cudaMemcpyToSymbol(kHC, hc, sizeof(float) * 4);
 }
 
-template <bool VTI, int TZ, int TX>
+template <bool VTI, int RZ, int TX, bool GRAD>
+static constexpr size_t elastic_smem_bytes()
+{
+    constexpr int TZ = 32 * RZ, UZ = TZ + 8, UX = TX + 8, WZ = TZ + 4, WX = TX + 4;
+    return sizeof(float) * (2 * UX * UZ + (5 + (VTI ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX);
+}
+
+template <bool VTI, int RZ, int TX, bool GRAD>
+static void launch_elastic_g(const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                             const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    constexpr size_t bytes = elastic_smem_bytes<VTI, RZ, TX, GRAD>();
+    static bool configured = false;   // per process; a kernel attribute applies to every device
+    if (!configured) {
+        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        configured = true;
+    }
+    elastic_step<VTI, RZ, TX, GRAD><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags, dtg);
+}
+
+template <bool VTI, int RZ, int TX>
 static void launch_elastic_t(const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M, const StepConst &C,
                              int it, int flags, float dtg, cudaStream_t st)
 {
-    if (flags & F_GRAD)
-        elastic_step<VTI, TZ, TX, true><<<ntiles, TZ * TX, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
-    else
-        elastic_step<VTI, TZ, TX, false><<<ntiles, TZ * TX, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+    if (flags & F_GRAD) launch_elastic_g<VTI, RZ, TX, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+    else launch_elastic_g<VTI, RZ, TX, false>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
 }
 
-// tile shapes offered to the autotuner: (TZ, TX)
-int elastic_tile_count() { return 3; }
+// tile shapes offered to the autotuner: (TZ, TX); TZ = 64 tiles take the lean interior path
+int elastic_tile_count() { return 4; }
 void elastic_tile_shape(int i, int *tz, int *tx)
 {
-    static const int s[3][2] = {{32, 16}, {32, 8}, {64, 8}};
+    static const int s[4][2] = {{64, 16}, {64, 8}, {32, 16}, {32, 8}};
     *tz = s[i][0];
     *tx = s[i][1];
 }
@@ -502,18 +822,21 @@ void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRe
                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
     switch (shape) {
-    case 0: vti ? launch_elastic_t<true, 32, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                : launch_elastic_t<false, 32, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
-    case 1: vti ? launch_elastic_t<true, 32, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                : launch_elastic_t<false, 32, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
-    default: vti ? launch_elastic_t<true, 64, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                 : launch_elastic_t<false, 64, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
+    case 0: vti ? launch_elastic_t<true, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
+                : launch_elastic_t<false, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
+    case 1: vti ? launch_elastic_t<true, 2, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
+                : launch_elastic_t<false, 2, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
+    case 2: vti ? launch_elastic_t<true, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
+                : launch_elastic_t<false, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
+    default: vti ? launch_elastic_t<true, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
+                 : launch_elastic_t<false, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
     }
 }
 
-void launch_scatter_init(const ShotDev *shots, int nshots, const InitEntry *ent, const int *off, cudaStream_t st)
+void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
+                       cudaStream_t st)
 {
-    scatter_init<<<nshots, 128, 0, st>>>(shots, nshots, ent, off);
+    init_state<<<nshots, 128, 0, st>>>(shots, nshots, cells, off, idx);
 }
 
 void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st)

@@ -13,7 +13,8 @@ int elastic_tile_count();
 void elastic_tile_shape(int i, int *tz, int *tx);
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
-void launch_scatter_init(const ShotDev *shots, int nshots, const InitEntry *ent, const int *off, cudaStream_t st);
+void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
+                       cudaStream_t st);
 void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st);
 
 // acoustic.cu

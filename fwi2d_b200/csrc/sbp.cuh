@@ -137,3 +137,91 @@ __device__ __forceinline__ float ndsum(const float *p, int in)
 }
 
 }  // namespace fwi2d
+
+namespace fwi2d {
+
+// ---------------------------------------------------------------------------
+// Interior forms (no boundary band within reach), same arithmetic as above.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float d1i(const float *p, int st, float scale)
+{
+    return scale * (kC1[0] * (p[st] - p[-st]) + kC1[1] * (p[2 * st] - p[-2 * st]));
+}
+
+__device__ __forceinline__ float md1i(const float *p, const float *q, int st, float ad)
+{
+    return ad * (kC1[0] * (p[st] * q[st] - p[-st] * q[-st]) + kC1[1] * (p[2 * st] * q[2 * st] - p[-2 * st] * q[-2 * st]));
+}
+
+// The five coefficient brackets of the interior Dxx_var/Dzz_var stencil for
+// the samples u0, u-1, u+1, u-2, u+2.  They depend on the coefficient only,
+// so one set serves every field differentiated with the same coefficient;
+// scaling the coefficient by 2 (expr4b = 2 mu) scales each bracket by exactly 2.
+struct Brk {
+    float b0, bm1, bp1, bm2, bp2;
+};
+
+__device__ __forceinline__ Brk brackets(const float *pf, int sf)
+{
+    const float fm2 = pf[-2 * sf], fm1 = pf[-sf], f0 = pf[0], fp1 = pf[sf], fp2 = pf[2 * sf];
+    Brk b;
+    b.b0 = kC2[0] * f0 + kC2[1] * (fm1 + fp1) + kC2[2] * (fm2 + fp2);
+    b.bm1 = kC2[3] * fm2 + kC2[4] * fm1 + kC2[5] * f0 + kC2[6] * fp1;
+    b.bp1 = kC2[3] * fp2 + kC2[4] * fp1 + kC2[5] * f0 + kC2[6] * fm1;
+    b.bm2 = kC2[7] * fm2 + kC2[8] * fm1 + kC2[9] * f0;
+    b.bp2 = kC2[7] * fp2 + kC2[8] * fp1 + kC2[9] * f0;
+    return b;
+}
+
+__device__ __forceinline__ Brk twice(const Brk &a)
+{
+    Brk b;
+    b.b0 = 2.f * a.b0;
+    b.bm1 = 2.f * a.bm1;
+    b.bp1 = 2.f * a.bp1;
+    b.bm2 = 2.f * a.bm2;
+    b.bp2 = 2.f * a.bp2;
+    return b;
+}
+
+// acc + (1/d^2) * (b0 u0 + b-1 u-1 + b+1 u+1 + b-2 u-2 + b+2 u+2)
+__device__ __forceinline__ float d2i(float acc, const Brk &b, const float *pu, int su, float invd2)
+{
+    return acc + invd2 * (b.b0 * pu[0] + b.bm1 * pu[-su] + b.bp1 * pu[su] + b.bm2 * pu[-2 * su] + b.bp2 * pu[2 * su]);
+}
+
+}  // namespace fwi2d
+
+namespace fwi2d {
+
+// Scalar-argument interior forms for register-resident samples (the lean
+// path of the step kernels); arithmetic identical to d1i / md1i / d2i.
+__device__ __forceinline__ float d1s(float vm2, float vm1, float vp1, float vp2, float scale)
+{
+    return scale * (kC1[0] * (vp1 - vm1) + kC1[1] * (vp2 - vm2));
+}
+
+__device__ __forceinline__ float md1s(float pm2, float qm2, float pm1, float qm1, float pp1, float qp1, float pp2,
+                                      float qp2, float ad)
+{
+    return ad * (kC1[0] * (pp1 * qp1 - pm1 * qm1) + kC1[1] * (pp2 * qp2 - pm2 * qm2));
+}
+
+__device__ __forceinline__ Brk brk5(float fm2, float fm1, float f0, float fp1, float fp2)
+{
+    Brk b;
+    b.b0 = kC2[0] * f0 + kC2[1] * (fm1 + fp1) + kC2[2] * (fm2 + fp2);
+    b.bm1 = kC2[3] * fm2 + kC2[4] * fm1 + kC2[5] * f0 + kC2[6] * fp1;
+    b.bp1 = kC2[3] * fp2 + kC2[4] * fp1 + kC2[5] * f0 + kC2[6] * fm1;
+    b.bm2 = kC2[7] * fm2 + kC2[8] * fm1 + kC2[9] * f0;
+    b.bp2 = kC2[7] * fp2 + kC2[8] * fp1 + kC2[9] * f0;
+    return b;
+}
+
+__device__ __forceinline__ float d2s(float acc, const Brk &b, float um2, float um1, float u0, float up1, float up2,
+                                     float invd2)
+{
+    return acc + invd2 * (b.b0 * u0 + b.bm1 * um1 + b.bp1 * up1 + b.bm2 * um2 + b.bp2 * up2);
+}
+
+}  // namespace fwi2d

@@ -153,6 +153,26 @@ class Propagator:
         C.check(self.L.fwi2d_snapshot(self.h, shot, slot, C.ptr(out)))
         return out
 
+    def update_model(self, model):
+        m = np.ascontiguousarray(model, np.float32)
+        C.check(self.L.fwi2d_update_model(self.h, C.ptr(m)))
+
+    def set_observed(self, obs_blocks):
+        buf = self._concat(obs_blocks, self.rcv_rows)
+        C.check(self.L.fwi2d_set_observed(self.h, C.ptr(buf)))
+
+    def fwi_gradient(self, model=None, src_blocks=None, obs_blocks=None, seismotype=1, download=True):
+        """One device FWI gradient: returns ((vp, vs, rho) gradient, misfit)
+        or (None, None) with download=False."""
+        m = None if model is None else np.ascontiguousarray(model, np.float32)
+        src = None if src_blocks is None else self._concat(src_blocks, self.src_rows)
+        obs = None if obs_blocks is None else self._concat(obs_blocks, self.rcv_rows)
+        g = np.zeros((3, self.nx, self.nz), np.float32) if download else None
+        f = ctypes.c_double(0.0)
+        C.check(self.L.fwi2d_fwi_gradient(self.h, C.ptr(m), C.ptr(src), C.ptr(obs), int(seismotype), C.ptr(g),
+                                          ctypes.byref(f) if download else None))
+        return (g, f.value) if download else (None, None)
+
     # -- device-resident API ----------------------------------------------
     def upload(self, blocks, adjoint):
         rows = self.rcv_rows if adjoint else self.src_rows
@@ -164,6 +184,19 @@ class Propagator:
 
     def sync(self):
         C.check(self.L.fwi2d_sync(self.h))
+
+    def set_stream(self, stream_handle):
+        """Order the context's work on a caller stream (an integer cudaStream_t,
+        e.g. torch.cuda.current_stream().cuda_stream); 0/None: own stream."""
+        C.check(self.L.fwi2d_set_stream(self.h, ctypes.c_void_p(stream_handle) if stream_handle else None))
+
+    def copy_gradient(self, dst_ptr):
+        C.check(self.L.fwi2d_copy_gradient(self.h, ctypes.c_void_p(dst_ptr)))
+
+    def last_timing(self):
+        f, a = ctypes.c_float(), ctypes.c_float()
+        C.check(self.L.fwi2d_last_timing(self.h, ctypes.byref(f), ctypes.byref(a)))
+        return f.value, a.value
 
     def plan_info(self):
         lf, la, sh, sb = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int(), ctypes.c_longlong()

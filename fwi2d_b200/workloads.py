@@ -1,0 +1,127 @@
+"""Seeded synthetic stand-ins for the benchmark configurations.
+
+No dataset ships with the reference; these generate the shapes, sizes and
+value distributions the configurations describe, in the reference's units
+(km, s, km/s, g/cm^3):
+
+* elastic_single  -- 401 x 801 grid at 5 m, vp = 2 + 0.75 z km/s with a
+  +-5 % smoothed random perturbation (sigma 50 m), vs = vp/1.73,
+  rho = 0.31 (1000 vp)^0.25; Ricker 10 Hz delayed 0.1 s, dt 0.4 ms, 5001
+  samples; one vertical force at (2.0, 0.01) km; 400 two-component receivers
+  at z = 10 m every 10 m; free surface on top, absorbing elsewhere with
+  60-cell tapers.  Starting model for the gradient: the true model smoothed
+  with sigma 250 m.
+* vti_batch       -- the same grid, VTI with eps in [0.05, 0.20] and delta in
+  [0, 0.10] as smooth seeded fields; 64 shots 60 m apart, each with a 1.0-3.5
+  km receiver aperture on its own cropped grid and a 1.2-2.0 s record.
+"""
+import math
+
+import numpy as np
+
+from . import _capi as C
+
+
+def ricker(nt, dt, f0, t0):
+    t = np.arange(nt, dtype=np.float64) * dt - t0
+    a = (math.pi * f0 * t) ** 2
+    return ((1 - 2 * a) * np.exp(-a)).astype(np.float32)
+
+
+def _smooth(rng_field, sigma):
+    from scipy.ndimage import gaussian_filter
+    return gaussian_filter(rng_field, sigma, mode="nearest")
+
+
+def elastic_model(nx=801, nz=401, d=0.005, seed=0):
+    """Raw (vp, vs, rho) of the true model."""
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz) * d
+    p = _smooth(rng.uniform(-1, 1, (nx, nz)), 10)
+    p *= 0.05 / np.abs(p).max()
+    vp = (2.0 + 0.75 * z)[None, :] * (1 + p)
+    vs = vp / 1.73
+    rho = 0.31 * (1000 * vp) ** 0.25
+    return np.stack([vp, vs, rho]).astype(np.float32)
+
+
+def smoothed(model, sigma_cells):
+    return np.stack([_smooth(m.astype(np.float64), sigma_cells) for m in model]).astype(np.float32)
+
+
+def vti_model(nx=801, nz=401, d=0.005, seed=2):
+    """Raw (vp, vs, rho, delta, eps)."""
+    base = elastic_model(nx, nz, d, seed=0)
+    rng = np.random.default_rng(seed)
+
+    def field(lo, hi):
+        f = _smooth(rng.uniform(-1, 1, (nx, nz)), 20)
+        f = (f - f.min()) / max(f.max() - f.min(), 1e-12)
+        return lo + (hi - lo) * f
+
+    eps = field(0.05, 0.20)
+    dl = field(0.0, 0.10)
+    return np.concatenate([base, dl[None], eps[None]]).astype(np.float32)
+
+
+def convert(kind, raw):
+    """nl_we_op_*::convert_model (we_op.cpp:476-494, 1441-1462, 1863-1881) in float32."""
+    m = raw.astype(np.float32).copy()
+    if kind == C.ACOUSTIC:
+        m[0] = m[1] * m[0] * m[0]
+        m[1] = np.float32(1.0) / m[1]
+        return m
+    vp, vs, rho = m[0].copy(), m[1].copy(), m[2].copy()
+    lam = rho * (vp * vp - np.float32(2) * vs * vs)
+    mu = rho * vs * vs
+    m[0], m[1] = lam, mu
+    if kind == C.VTI:
+        dl = m[3]
+        m[3] = (np.sqrt((np.float32(2) * (lam + np.float32(2) * mu) * (lam + mu) * dl + (lam + mu) * (lam + mu)).astype(np.float64))
+                - mu).astype(np.float32)
+    return m
+
+
+def elastic_single(nt=5001):
+    """Elastic single-shot gradient workload; returns a dict."""
+    nx, nz, d, dt = 801, 401, 0.005, 4e-4
+    true = elastic_model(nx, nz, d)
+    start = smoothed(true, 50)
+    w = ricker(nt, dt, 10.0, 0.1)
+    ang = np.float32(1.5708)
+    src = np.stack([w * np.float32(np.cos(ang)), w * np.float32(np.sin(ang))])[:, None, :].astype(np.float32)
+    rx = (0.005 + 0.01 * np.arange(400)).astype(np.float32)
+    rz = np.full(400, 0.01, np.float32)
+    params = dict(nt=nt, sub=1, dt=dt, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2, taper_top=0, taper_bottom=60,
+                  taper_left=60, taper_right=60, taper_strength=0.05)
+    return dict(kind=C.ELASTIC, nx=nx, nz=nz, d=d, dt=dt, nt=nt, true=true, start=start, src=src,
+                shots=[dict(x0=0, nx=nx, sx=[2.0], sz=[0.01], rx=rx, rz=rz, nt=nt)], params=params, seismotype=1)
+
+
+def vti_batch(nshots=64, nt_max=5001, seed=2):
+    """Batched VTI workload: 64 shots on cropped grids with uneven apertures
+    and record lengths."""
+    nx, nz, d, dt = 801, 401, 0.005, 4e-4
+    true = vti_model(nx, nz, d, seed=seed)
+    start = np.concatenate([smoothed(true[:3], 50), true[3:]])
+    rng = np.random.default_rng(seed)
+    w = ricker(nt_max, dt, 10.0, 0.1)
+    shots = []
+    margin = 60
+    for k in range(nshots):
+        sx = 0.03 + 0.06 * k
+        aperture = rng.uniform(1.0, 3.5)
+        rec = rng.uniform(1.2, 2.0)
+        nts = min(nt_max, int(round(rec / dt)) + 1)
+        lo = max(0.0, sx - aperture / 2)
+        hi = min((nx - 1) * d, sx + aperture / 2)
+        rx = np.arange(lo + 0.005, hi, 0.01, dtype=np.float32)
+        x0 = max(0, int(math.floor(min(lo, sx) / d)) - margin)
+        x1 = min(nx, int(math.ceil(max(hi, sx) / d)) + margin + 1)
+        shots.append(dict(x0=x0, nx=x1 - x0, sx=[sx], sz=[0.01], rx=rx, rz=np.full(len(rx), 0.01, np.float32), nt=nts))
+    ang = np.float32(1.5708)
+    src = np.stack([w * np.float32(np.cos(ang)), w * np.float32(np.sin(ang))])[:, None, :].astype(np.float32)
+    params = dict(nt=nt_max, sub=1, dt=dt, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2, taper_top=0,
+                  taper_bottom=60, taper_left=60, taper_right=60, taper_strength=0.05)
+    return dict(kind=C.VTI, nx=nx, nz=nz, d=d, dt=dt, nt=nt_max, true=true, start=start, src=src, shots=shots,
+                params=params, seismotype=1)

@@ -125,6 +125,25 @@ int fwi2d_upload_traces(fwi2d_ctx *ctx, const float *traces, int adjoint);
 int fwi2d_run(fwi2d_ctx *ctx, int adjoint, int store_snapshots);
 int fwi2d_sync(fwi2d_ctx *ctx);
 
+/* New values for the current model geometry (converted, host [npar][nx][nz]);
+ * the batch plan, its tables and graphs stay valid. */
+int fwi2d_update_model(fwi2d_ctx *ctx, const float *model);
+
+/* Observed data of every shot, concatenated per-shot blocks [ncomp][nr][nt],
+ * kept on the device for fwi2d_fwi_gradient. */
+int fwi2d_set_observed(fwi2d_ctx *ctx, const float *obs);
+
+/* One FWI gradient evaluation on the device (nlls_fwi_eco::compute_res_and_grad,
+ * optimization.hpp:590-951, with the data-side options off): forward with
+ * snapshots, residual against the observed data (seismotype 1: particle
+ * velocity, the time derivative of the extracted displacement), L2 misfit
+ * 1/2 dt (|r|^2 - (r_0^2 + r_end^2)/2), adjoint sources, adjoint propagation
+ * with the imaging condition, H quadrature and the chain rule to (vp, vs, rho).
+ * model / src / obs may be NULL to reuse what is resident; grad (host
+ * [3][nx][nz]) and misfit may be NULL to leave the results on the device. */
+int fwi2d_fwi_gradient(fwi2d_ctx *ctx, const float *model, const float *src, const float *obs, int seismotype,
+                       float *grad, double *misfit);
+
 /* Read back one stored snapshot [ncomp][nx][nz] of one shot (dequantised). */
 int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out);
 
@@ -132,6 +151,18 @@ int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out);
  * the tile shape in use, snapshot bytes held. */
 int fwi2d_plan_info(fwi2d_ctx *ctx, long long *launches_fwd, long long *launches_adj, int *tile_shape,
                     long long *snapshot_bytes);
+
+/* Order all later work of the context on a caller's CUDA stream (a
+ * cudaStream_t; NULL returns to the context's own stream). */
+int fwi2d_set_stream(fwi2d_ctx *ctx, void *stream);
+
+/* Copy the model-grid gradient of the last adjoint into caller device memory
+ * [3 or 2][nx][nz], ordered on the context stream. */
+int fwi2d_copy_gradient(fwi2d_ctx *ctx, float *dst_device);
+
+/* Device time (CUDA events on the context stream) of the last forward and
+ * adjoint time loops, in milliseconds (-1 if none ran). */
+int fwi2d_last_timing(fwi2d_ctx *ctx, float *forward_ms, float *adjoint_ms);
 
 /* Tile shapes offered to the autotuner. */
 int fwi2d_tile_shape_count(void);
