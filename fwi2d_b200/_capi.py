@@ -18,7 +18,7 @@ SYMBOLS = [
     "fwi2d_last_error", "fwi2d_version", "fwi2d_injector_weights", "fwi2d_ctx_create", "fwi2d_ctx_destroy",
     "fwi2d_set_model", "fwi2d_set_shots", "fwi2d_forward", "fwi2d_adjoint", "fwi2d_upload_traces", "fwi2d_run",
     "fwi2d_sync", "fwi2d_snapshot", "fwi2d_plan_info", "fwi2d_tile_shape_count", "fwi2d_tile_shape",
-    "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing", "fwi2d_set_stream", "fwi2d_copy_gradient",
+    "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing", "fwi2d_set_stream", "fwi2d_copy_gradient", "fwi2d_propagate_noalloc", "fwi2d_noalloc_last_error",
 ]
 
 

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfwi2d_b200.so")
-SOURCES = ["kernels.cu", "acoustic.cu", "engine.cu", "host_tables.cpp"]
+SOURCES = ["kernels.cu", "acoustic.cu", "engine.cu", "noalloc.cu", "host_tables.cpp"]
 HEADERS = ["engine.h", "launch.h", "sbp.cuh", "host_tables.h", "d2_closure.inc", "../../include/fwi2d_b200.h"]
 
 NVCC_FLAGS = [

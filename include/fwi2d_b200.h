@@ -181,6 +181,29 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
                     float *full_wfld, float *grad, const fwi2d_params *par, int ns, int nr,
                     int nx, int nz, float dx, float dz);
 
+/* Allocation-free forward propagation.  No counterpart in the reference: it
+ * serves callers that cannot allocate device memory (code running under CUDA
+ * graph capture, plug-ins whose host framework owns the device allocator,
+ * allocation-free real-time loops).  Same meaning and results as
+ * fwi2d_propagate with adj = 0 and no snapshots, for the elastic isotropic
+ * propagator with point-force sources: host inputs, receivers accumulated into
+ * allrcv.  All device-side buffers live in one static array of
+ * FWI2D_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; problems that do not fit it (or exceed the FWI2D_NOALLOC_MAX_* table
+ * limits) are rejected with FWI2D_ERR_ARG.  The array keeps the last call's
+ * contents (each call clears what must start at zero); calls serialise on the
+ * host, and calls that overlap on the GPU race on the array.  The first call
+ * on a device looks up the array's device address with that device current:
+ * make it before any stream capture.  Errors: fwi2d_noalloc_last_error(). */
+#define FWI2D_NOALLOC_SCRATCH_BYTES (64u << 20)
+#define FWI2D_NOALLOC_MAX_AXIS 16384
+#define FWI2D_NOALLOC_MAX_SOURCES 16
+#define FWI2D_NOALLOC_MAX_RECEIVERS 8192
+int fwi2d_propagate_noalloc(const float *model, const float *allsrc, float *allrcv, const fwi2d_injector *inj,
+                            const fwi2d_injector *ext, const fwi2d_params *par, int ns, int nr, int nx, int nz,
+                            float dx, float dz);
+const char *fwi2d_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
