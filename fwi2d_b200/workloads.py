@@ -113,8 +113,9 @@ def vti_batch(nshots=64, nt_max=5001, seed=2):
         aperture = rng.uniform(1.0, 3.5)
         rec = rng.uniform(1.2, 2.0)
         nts = min(nt_max, int(round(rec / dt)) + 1)
-        lo = max(0.0, sx - aperture / 2)
-        hi = min((nx - 1) * d, sx + aperture / 2)
+        # the aperture slides inside the 4 km line near its ends rather than being clipped
+        lo = min(max(0.0, sx - aperture / 2), (nx - 1) * d - aperture)
+        hi = lo + aperture
         rx = np.arange(lo + 0.005, hi, 0.01, dtype=np.float32)
         x0 = max(0, int(math.floor(min(lo, sx) / d)) - margin)
         x1 = min(nx, int(math.ceil(max(hi, sx) / d)) + margin + 1)

@@ -185,6 +185,13 @@ class Reference(_Lib):
         self._weights(itype, n, _ptr(lx), _ptr(lz), nx, nz, dx, dz, ox, oz, _ptr(xind), _ptr(zind), _ptr(xw), _ptr(zw))
         return xind, zind, xw, zw
 
+    def convert_model(self, kind, m, forward=True):
+        m = self.arr(m).copy()
+        f = self.lib.ref_convert_model
+        f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        f(kind, _ptr(m), m.shape[-1] * m.shape[-2], 1 if forward else 0)
+        return m
+
     def propagate(self, kind, adj, model, src, rcv, par, nx, nz, dx, dz, ox, oz, inj_locs, ext_locs,
                   inj_type=0, full=None, grad=None, water_inj_locs=None, water_ext_locs=None):
         def loc(l):

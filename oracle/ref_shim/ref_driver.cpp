@@ -59,6 +59,16 @@ extern "C" {
 
 int ref_real_size(void) { return (int)sizeof(data_t); }
 
+// nl_we_op_*::convert_model, in place on [npar][n].
+int ref_convert_model(int kind, data_t *m, int n, int forward)
+{
+    if (kind == 0 || kind == 3) { nl_we_op_e op; op.convert_model(m, n, forward != 0); }
+    else if (kind == 1) { nl_we_op_vti op; op.convert_model(m, n, forward != 0); }
+    else if (kind == 2) { nl_we_op_a op; op.convert_model(m, n, forward != 0); }
+    else return -1;
+    return 0;
+}
+
 // injector tables built by the reference's delta_m3 / ddelta_m3.
 int ref_injector_weights(int type, int ntr, const data_t *lx, const data_t *lz, int nx, int nz,
                          double dx, double dz, double ox, double oz, int *xind, int *zind, data_t *xw, data_t *zw)

@@ -1,0 +1,101 @@
+"""Generate tests/golden/*.npz from the reference itself.
+
+Runs the reference's own propagation code (src/cpp/we_op.cpp et al., compiled
+from the reference tree by oracle/build_ref.sh into oracle/_ref/) on small
+seeded cases and stores inputs and outputs.  The tests check the oracle's C
+restatement and the library's host tables against these files; they never
+need the reference tree.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+from tests import cases as K  # noqa: E402
+
+
+CASES = [
+    # name, kind, mt, bc, nx, nz, nt
+    ("elastic_fs_abs", O.KIND_ELASTIC, 0, (1, 2, 2, 2), 60, 44, 140),
+    ("elastic_all_abs", O.KIND_ELASTIC, 0, (2, 2, 2, 2), 52, 48, 120),
+    ("elastic_all_free", O.KIND_ELASTIC, 0, (1, 1, 1, 1), 48, 40, 120),
+    ("elastic_mt", O.KIND_ELASTIC, 1, (1, 2, 2, 2), 56, 44, 120),
+    ("vti_fs_abs", O.KIND_VTI, 0, (1, 2, 2, 2), 60, 44, 140),
+    ("acoustic_dirichlet_abs", O.KIND_ACOUSTIC, 0, (1, 2, 2, 2), 60, 44, 140),
+    ("acoustic_neumann", O.KIND_ACOUSTIC, 0, (3, 3, 2, 2), 52, 40, 120),
+]
+
+
+def elastic_like(name, kind, mt, bc, nx, nz, nt, prec):
+    d = 0.01
+    lib = O.Reference(prec)
+    raw = K.model_case(kind, nx, nz, d, seed=11)
+    ref_mc = lib.convert_model(kind, raw.astype(lib.dtype))
+    sl, rl = K.geometry(nx, nz, d, nr=14)
+    ncs = 1 if kind == O.KIND_ACOUSTIC else (3 if mt else 2)
+    src = K.sources(ncs, nt, 1e-3).astype(lib.dtype)
+    par = O.make_par(**K.par_dict(nt=nt, dt=1e-3, bc=bc, taper=(0, 6, 6, 6), mt=mt), ns=1, nr=14)
+    rcv, full = K.oracle_forward(lib, kind, ref_mc, src, par, nx, nz, d, sl, rl, mt=mt)
+    adj = np.ascontiguousarray(rcv[:, :, ::-1])
+    g = K.oracle_adjoint(lib, kind, ref_mc, adj, par, nx, nz, d, sl, rl, full, mt=mt)
+    itype = 1 if mt else 0
+    sw = lib.injector_weights(itype, sl[0], sl[1], nx, nz, d, d, 0.0, 0.0)
+    rw = lib.injector_weights(0, rl[0], rl[1], nx, nz, d, d, 0.0, 0.0)
+    idx = np.linspace(0, nt - 1, 5).astype(int)
+    return dict(kind=kind, mt=mt, bc=np.array(bc), nx=nx, nz=nz, nt=nt, d=d, raw=raw, model=ref_mc, src=src,
+                src_x=sl[0], src_z=sl[1], rcv_x=rl[0], rcv_z=rl[1], rcv=rcv, snap_idx=idx, snaps=full[idx], grad=g,
+                src_xind=sw[0], src_zind=sw[1], src_xw=sw[2], src_zw=sw[3],
+                rcv_xind=rw[0], rcv_zind=rw[1], rcv_xw=rw[2], rcv_zw=rw[3])
+
+
+def ae_case(prec):
+    lib = O.Reference(prec)
+    nx, nz, d, nt = 56, 40, 0.01, 120
+    oz = 0.12
+    nza = int(np.floor(oz / d + 1e-6)) + 1
+    raw = K.model_case(O.KIND_ELASTIC, nx, nz, d, seed=12)
+    raw[0] += 0.5
+    raw[1] = raw[0] / 1.8
+    mc = lib.convert_model(O.KIND_ELASTIC, raw.astype(lib.dtype))
+    par = O.make_par(**K.par_dict(nt=nt, dt=1e-3, bc=(1, 2, 2, 2), taper=(0, 6, 6, 6)), ns=1, nr=14, nza=nza,
+                     acoustic_source=1)
+    src = K.sources(1, nt, 1e-3, f0=20.0, t0=0.05).astype(lib.dtype)
+    rx = np.linspace(0.05, 0.5, 14).astype(np.float32)
+    rz_w = np.full(14, 0.06, np.float32)
+    rz_e = np.full(14, oz, np.float32)
+    wsrc = (np.array([0.3], np.float32), np.array([0.05], np.float32))
+    rcv = np.zeros((3, 14, nt), lib.dtype)
+    full = np.zeros((nt + 1, 2, nx, nz), lib.dtype)
+    lib.propagate(O.KIND_AE, 0, mc, src, rcv, par, nx, nz, d, d, 0.0, oz, None, (rx, rz_e), full=full,
+                  water_inj_locs=wsrc, water_ext_locs=(rx, rz_w))
+    adj = np.ascontiguousarray(rcv[:, :, ::-1])
+    g = np.zeros((3, nx, nz), lib.dtype)
+    srcb = np.zeros((1, 1, nt), lib.dtype)
+    lib.propagate(O.KIND_AE, 1, mc, adj, srcb, par, nx, nz, d, d, 0.0, oz, (rx, rz_e), None, full=full, grad=g,
+                  water_inj_locs=wsrc, water_ext_locs=(rx, rz_w))
+    idx = np.linspace(0, nt - 1, 5).astype(int)
+    return dict(kind=O.KIND_AE, nx=nx, nz=nz, nt=nt, d=d, oz=oz, nza=nza, raw=raw, model=mc, src=src, rcv_x=rx,
+                rcv_zw=rz_w, rcv_ze=rz_e, wsrc_x=wsrc[0], wsrc_z=wsrc[1], rcv=rcv, snap_idx=idx, snaps=full[idx],
+                grad=g)
+
+
+def main():
+    if not O.have_reference(32):
+        sys.exit("oracle/_ref is not built (oracle/build_ref.sh needs the reference tree)")
+    for prec in (32, 64):
+        for name, kind, mt, bc, nx, nz, nt in CASES:
+            out = elastic_like(name, kind, mt, bc, nx, nz, nt, prec)
+            np.savez_compressed(os.path.join(HERE, "%s_f%d.npz" % (name, prec)), **out)
+        np.savez_compressed(os.path.join(HERE, "acoustic_elastic_f%d.npz" % prec), **ae_case(prec))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

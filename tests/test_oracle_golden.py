@@ -1,0 +1,74 @@
+"""The oracle's C restatement against outputs of the reference itself.
+
+tests/golden/*.npz were produced by tests/golden/make_golden.py from the
+reference sources compiled in oracle/_ref (FP32 and FP64 builds).  The
+restatement must reproduce every sample: model conversion, injector tables,
+traces, snapshots and gradients.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from tests import cases as K
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FILES = sorted(glob.glob(os.path.join(GOLD, "*.npz")))
+
+
+def test_golden_fixtures_present():
+    assert len(FILES) >= 16
+
+
+@pytest.mark.parametrize("path", FILES, ids=[os.path.basename(f) for f in FILES])
+def test_port_matches_reference(path):
+    g = dict(np.load(path))
+    prec = 64 if path.endswith("_f64.npz") else 32
+    P = O.Port(prec)
+    kind = int(g["kind"])
+    nx, nz, nt, d = int(g["nx"]), int(g["nz"]), int(g["nt"]), float(g["d"])
+    conv_kind = O.KIND_ELASTIC if kind == O.KIND_AE else kind
+    mc = P.convert_model(conv_kind, g["raw"])
+    assert np.array_equal(mc, g["model"]), "convert_model"
+    if kind == O.KIND_AE:
+        nza, oz = int(g["nza"]), float(g["oz"])
+        par = O.make_par(**K.par_dict(nt=nt, dt=1e-3, bc=(1, 2, 2, 2), taper=(0, 6, 6, 6)), ns=1,
+                         nr=len(g["rcv_x"]), nza=nza, acoustic_source=1)
+        wsrc = (g["wsrc_x"], g["wsrc_z"])
+        rcv = np.zeros_like(g["rcv"])
+        full = np.zeros((nt + 1, 2, nx, nz), P.dtype)
+        P.propagate(kind, 0, mc, g["src"], rcv, par, nx, nz, d, d, 0.0, oz, None, (g["rcv_x"], g["rcv_ze"]),
+                    full=full, water_inj_locs=wsrc, water_ext_locs=(g["rcv_x"], g["rcv_zw"]))
+        adj = np.ascontiguousarray(rcv[:, :, ::-1])
+        grad = np.zeros_like(g["grad"])
+        P.propagate(kind, 1, mc, adj, np.zeros((1, 1, nt), P.dtype), par, nx, nz, d, d, 0.0, oz,
+                    (g["rcv_x"], g["rcv_ze"]), None, full=full, grad=grad, water_inj_locs=wsrc,
+                    water_ext_locs=(g["rcv_x"], g["rcv_zw"]))
+    else:
+        mt = int(g["mt"])
+        bc = tuple(int(b) for b in g["bc"])
+        par = O.make_par(**K.par_dict(nt=nt, dt=1e-3, bc=bc, taper=(0, 6, 6, 6), mt=mt), ns=1, nr=len(g["rcv_x"]))
+        sl, rl = (g["src_x"], g["src_z"]), (g["rcv_x"], g["rcv_z"])
+        w = P.injector_weights(1 if mt else 0, sl[0], sl[1], nx, nz, d, d, 0.0, 0.0)
+        for a, b in zip(w, (g["src_xind"], g["src_zind"], g["src_xw"], g["src_zw"])):
+            assert np.array_equal(a, b), "source injector tables"
+        w = P.injector_weights(0, rl[0], rl[1], nx, nz, d, d, 0.0, 0.0)
+        for a, b in zip(w, (g["rcv_xind"], g["rcv_zind"], g["rcv_xw"], g["rcv_zw"])):
+            assert np.array_equal(a, b), "receiver injector tables"
+        rcv, full = K.oracle_forward(P, kind, mc, g["src"], par, nx, nz, d, sl, rl, mt=mt)
+        adj = np.ascontiguousarray(rcv[:, :, ::-1])
+        grad = K.oracle_adjoint(P, kind, mc, adj, par, nx, nz, d, sl, rl, full, mt=mt)
+    assert np.array_equal(rcv, g["rcv"]), "traces differ (max %g)" % np.abs(rcv - g["rcv"]).max()
+    assert np.array_equal(full[g["snap_idx"]], g["snaps"]), "snapshots"
+    assert np.array_equal(grad, g["grad"][:grad.shape[0]]), "gradient"
+
+
+def test_fp32_vs_fp64_distance_is_small():
+    """The FP32 build stays within the FP32 rounding budget of the FP64 oracle
+    on these short runs (a sanity bound, not a parity criterion)."""
+    a = dict(np.load(os.path.join(GOLD, "elastic_fs_abs_f32.npz")))
+    b = dict(np.load(os.path.join(GOLD, "elastic_fs_abs_f64.npz")))
+    assert K.rel_l2(a["rcv"], b["rcv"]) < 1e-4
+    assert K.rel_l2(a["grad"], b["grad"]) < 1e-3
