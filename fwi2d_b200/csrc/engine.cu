@@ -202,29 +202,34 @@ static int npar_of(int kind)
 // plan
 // ---------------------------------------------------------------------------
 struct ShotPlan {
-    int x0 = 0, nx = 0, nt = 0, tiles_x = 0, tiles_z = 0;
+    int x0 = 0, nx = 0, nt = 0;
     int ncomp = 2;                 // field components
     int ncomp_src = 2, ntr_src = 0, nr = 0;
     int nsrc_rows = 0, nrcv_rows = 0;
     int nslot = 0;
     std::vector<InjEntry> inj_f, inj_a;
-    std::vector<int> inj_f_off, inj_a_off;
+    std::vector<int> inj_f_off, inj_a_off, inj_f_roff, inj_a_roff;
     std::vector<ExtEntry> ext_f;
-    std::vector<int> ext_f_off, ext_none_off;
+    std::vector<int> ext_f_off, ext_none_off, ext_f_roff, ext_none_roff;
     DevBuf u0, u1, src_f, rcv_f, src_a;
     DevBuf d_inj_f, d_inj_f_off, d_inj_a, d_inj_a_off, d_ext_f, d_ext_f_off, d_ext_none_off;
+    DevBuf d_inj_f_roff, d_inj_a_roff, d_ext_f_roff, d_ext_none_roff;
     DevBuf den, tz, tx, snap, amax, grad, gwt;
 };
 
 struct Plan {
     fwi2d_params par;
     int kind = 0;
-    int shape = 0, TZ = 32, TX = 16;
+    int shape = 0;                 // index into the shape list (tile shapes, then marching shapes)
+    int tshape = 0, TZ = 32, TX = 16;   // tile shape of the tile kernel's units
+    bool march = false;            // interior rows on the marching kernel
+    int nth = 0, lx = 0;           // marching: threads (z window) per unit, rows per unit
     int nt_max = 0;
     int ncompg = 3;
     std::vector<std::unique_ptr<ShotPlan>> shots;
     std::vector<TileRef> tiles;
-    DevBuf d_tiles, d_shots_f, d_shots_a;
+    std::vector<MarchRef> marches;
+    DevBuf d_tiles, d_march, d_shots_f, d_shots_a;
     // initial-state cells per mode (0 forward, 1 adjoint)
     std::vector<InitCell> icells[2];
     std::vector<int> ioff[2], iidx[2];
@@ -355,11 +360,177 @@ static void check_injector(const fwi2d_injector &J, int nx, int nz, const char *
         }
 }
 
+// ---- work decomposition ---------------------------------------------------------
+// A plan runs either the tile kernel over the whole of every shot grid, or the
+// marching kernel over the rows clear of the x boundary bands (6 <= x < nx-6)
+// with the tile kernel (tiles of kBandTile) on the two bands.
+struct MarchShape {
+    int nth, lx;
+};
+static const MarchShape kMarchShapes[] = {{224, 64}, {256, 64}, {192, 64}, {128, 64},
+                                          {224, 32}, {256, 32}, {192, 32}, {128, 32}};
+static const int kNumMarch = sizeof(kMarchShapes) / sizeof(kMarchShapes[0]);
+static const int kBandTile = 3;    // (TZ, TX) = (32, 8): band windows of 8 columns own 6
+static const int kBand = 6;
+
+static int shape_count() { return elastic_tile_count() + kNumMarch; }
+
+// Work units of one shot.  Units are numbered per shot: tiles first, then
+// marching units (segment-major, then z window).
+struct ShotUnits {
+    bool march = false;
+    int nx = 0, nz = 0;
+    int TX = 0, TZ = 0, tiles_x = 0, tiles_z = 0;
+    int lx = 0, nseg = 0, nwin = 0;
+    std::vector<int> zo;           // marching: owned z starts of the windows, plus nz
+    std::vector<TileRef> tiles;
+    std::vector<MarchRef> marches;
+    int nunits() const { return (int)(tiles.size() + marches.size()); }
+    int unit_of(int x, int z) const
+    {
+        if (!march) return owner_tile(z, nz, TZ) * tiles_x + owner_tile(x, nx, TX);
+        if (x < kBand) return owner_tile(z, nz, TZ);
+        if (x >= nx - kBand) return tiles_z + owner_tile(z, nz, TZ);
+        const int seg = (x - kBand) / lx;
+        const int k = (int)(std::upper_bound(zo.begin(), zo.end(), z) - zo.begin()) - 1;
+        return 2 * tiles_z + seg * nwin + k;
+    }
+    bool is_march(int u) const { return u >= (int)tiles.size(); }
+    const MarchRef &mref(int u) const { return marches[u - tiles.size()]; }
+};
+
+static bool axis_fits(int T, int n) { return n == T || n >= T + 8; }
+
+// z windows of the marching kernel for nth threads: window k owns
+// [zo[k], zo[k+1]) and covers [za, za + nth), two cells beyond its owned range
+// on each side; the last window owns at least 8 cells and its ring reaches
+// 8 cells above the bottom, so each SBP boundary band lies in one window.
+static void march_windows(int nz, int nth, std::vector<int> &zo, std::vector<int> &za)
+{
+    const int w = nth - 4;
+    const int K = (nz + w - 1) / w;
+    zo.assign(K + 1, 0);
+    for (int k = 0; k < K; k++) zo[k] = k * w;
+    zo[K] = nz;
+    if (K > 1 && nz - zo[K - 1] < 8) zo[K - 1] = nz - 8;
+    za.assign(K, 0);
+    for (int k = 0; k < K; k++) za[k] = zo[k] - 2;
+    if (K > 1) za[K - 1] = std::min(zo[K - 1] - 2, nz + 2 - nth);
+}
+
+// Whether a shape can run a shot grid of nx x nz.
+static bool shape_fits(int shape, int nx, int nz)
+{
+    if (shape < 0 || shape >= shape_count()) return false;
+    int tz, tx;
+    if (shape < elastic_tile_count()) {
+        elastic_tile_shape(shape, &tz, &tx);
+        return axis_fits(tz, nz) && axis_fits(tx, nx);
+    }
+    elastic_tile_shape(kBandTile, &tz, &tx);
+    return axis_fits(tz, nz) && nx >= 2 * tx && nx > 2 * kBand && nz >= 16 &&
+           march_threads_ok(kMarchShapes[shape - elastic_tile_count()].nth);
+}
+
+static ShotUnits make_units(int shape, int shot, int nx, int nz)
+{
+    ShotUnits U;
+    U.nx = nx;
+    U.nz = nz;
+    const bool march = shape >= elastic_tile_count();
+    U.march = march;
+    elastic_tile_shape(march ? kBandTile : shape, &U.TZ, &U.TX);
+    U.tiles_z = (nz + U.TZ - 1) / U.TZ;
+    if (!march) {
+        U.tiles_x = (nx + U.TX - 1) / U.TX;
+        for (int tzi = 0; tzi < U.tiles_z; tzi++)
+            for (int txi = 0; txi < U.tiles_x; txi++) {
+                TileRef r;
+                r.shot = shot;
+                r.unit = (int)U.tiles.size();
+                tile_window_host(txi, U.tiles_x, nx, U.TX, r.wx0, r.ox0, r.ox1);
+                tile_window_host(tzi, U.tiles_z, nz, U.TZ, r.wz0, r.oz0, r.oz1);
+                U.tiles.push_back(r);
+            }
+        return U;
+    }
+    for (int side = 0; side < 2; side++)
+        for (int tzi = 0; tzi < U.tiles_z; tzi++) {
+            TileRef r;
+            r.shot = shot;
+            r.unit = (int)U.tiles.size();
+            r.wx0 = side == 0 ? 0 : nx - U.TX;
+            r.ox0 = side == 0 ? 0 : nx - kBand;
+            r.ox1 = side == 0 ? kBand : nx;
+            tile_window_host(tzi, U.tiles_z, nz, U.TZ, r.wz0, r.oz0, r.oz1);
+            U.tiles.push_back(r);
+        }
+    const MarchShape ms = kMarchShapes[shape - elastic_tile_count()];
+    std::vector<int> za;
+    march_windows(nz, ms.nth, U.zo, za);
+    U.nwin = (int)za.size();
+    U.lx = ms.lx;
+    const int rows = nx - 2 * kBand;
+    U.nseg = (rows + U.lx - 1) / U.lx;
+    int roff = 0;
+    for (int sg = 0; sg < U.nseg; sg++)
+        for (int k = 0; k < U.nwin; k++) {
+            MarchRef m;
+            m.shot = shot;
+            m.unit = (int)(U.tiles.size() + U.marches.size());
+            m.xb = kBand + sg * U.lx;
+            m.xe = std::min(m.xb + U.lx, nx - kBand);
+            m.za = za[k];
+            m.oz0 = U.zo[k];
+            m.oz1 = U.zo[k + 1];
+            m.roff = roff;
+            roff += m.xe - m.xb + 1;
+            U.marches.push_back(m);
+        }
+    return U;
+}
+
+// Group entries by unit (stable: the reference's order survives within a
+// cell); within a marching unit order them by row (then z for injection).
+// off: [units+1] offsets; roff: per marching unit and row, the first entry of
+// the row (absolute), plus the end.
+template <class E>
+static void group_entries(const ShotUnits &U, const std::vector<E> &ent, const std::vector<int> &unit,
+                          const std::vector<int> &row, const std::vector<int> &zkey, std::vector<E> &out,
+                          std::vector<int> &off, std::vector<int> &roff)
+{
+    const int nu = U.nunits();
+    std::vector<size_t> idx(ent.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+        if (unit[a] != unit[b]) return unit[a] < unit[b];
+        if (!U.is_march(unit[a])) return false;
+        if (row[a] != row[b]) return row[a] < row[b];
+        return zkey[a] < zkey[b];
+    });
+    out.clear();
+    off.assign(nu + 1, 0);
+    for (size_t i : idx) {
+        out.push_back(ent[i]);
+        off[unit[i] + 1]++;
+    }
+    for (int t = 0; t < nu; t++) off[t + 1] += off[t];
+    int nro = 0;
+    for (const MarchRef &m : U.marches) nro += m.xe - m.xb + 1;
+    roff.assign(std::max(nro, 1), 0);
+    for (const MarchRef &m : U.marches) {
+        int e = off[m.unit];
+        for (int r = m.xb; r <= m.xe; r++) {
+            while (e < off[m.unit + 1] && row[idx[e]] < r) e++;
+            roff[m.roff + r - m.xb] = e;
+        }
+    }
+}
+
 // Injection entries of one injector into a field, in the reference's order
-// (trace, x, z), then stably grouped by owning tile.  rows(c, itr, which)
-// gives the trace row of component c.
-static void build_inj(const fwi2d_injector &J, int ncomp, const int *rowbase_a, const int *rowbase_b, int nx, int nz,
-                      int TX, int TZ, int tiles_x, int ntiles, std::vector<InjEntry> &out, std::vector<int> &off)
+// (component, trace, x, z), grouped by owning unit.
+static void build_inj(const fwi2d_injector &J, int ncomp, const int *rowbase_a, const int *rowbase_b,
+                      const ShotUnits &U, std::vector<InjEntry> &out, std::vector<int> &off, std::vector<int> &roff)
 {
     std::vector<InjEntry> ent;
     const int w = J.type == FWI2D_INJ_DELTA ? 3 : 6;
@@ -388,26 +559,21 @@ static void build_inj(const fwi2d_injector &J, int ncomp, const int *rowbase_a, 
                     ent.push_back(e);
                 }
         }
-    std::vector<int> tile_of(ent.size());
-    for (size_t i = 0; i < ent.size(); i++)
-        tile_of[i] = owner_tile(ent[i].gz, nz, TZ) * tiles_x + owner_tile(ent[i].gx, nx, TX);
-    std::vector<size_t> idx(ent.size());
-    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return tile_of[a] < tile_of[b]; });
-    out.clear();
-    off.assign(ntiles + 1, 0);
-    for (size_t i : idx) {
-        out.push_back(ent[i]);
-        off[tile_of[i] + 1]++;
+    std::vector<int> unit(ent.size()), row(ent.size()), zk(ent.size());
+    for (size_t i = 0; i < ent.size(); i++) {
+        unit[i] = U.unit_of(ent[i].gx, ent[i].gz);
+        row[i] = ent[i].gx;
+        zk[i] = ent[i].gz;
     }
-    for (int t = 0; t < ntiles; t++) off[t + 1] += off[t];
+    group_entries(U, ent, unit, row, zk, out, off, roff);
 }
 
-static void build_ext(const fwi2d_injector &J, int ncomp, int nx, int nz, int TX, int TZ, int tiles_x, int ntiles,
-                      std::vector<ExtEntry> &out, std::vector<int> &off)
+// Receiver entries, owned by the unit of the pivot cell (the middle of the 3x3).
+static void build_ext(const fwi2d_injector &J, int ncomp, const ShotUnits &U, std::vector<ExtEntry> &out,
+                      std::vector<int> &off, std::vector<int> &roff)
 {
     std::vector<ExtEntry> ent;
-    std::vector<int> tile_of;
+    std::vector<int> unit, row, zk;
     for (int c = 0; c < ncomp; c++)
         for (int t = 0; t < J.ntr; t++) {
             ExtEntry e;
@@ -419,18 +585,11 @@ static void build_ext(const fwi2d_injector &J, int ncomp, int nx, int nz, int TX
             for (int a = 0; a < 3; a++)
                 for (int b = 0; b < 3; b++) e.w[a * 3 + b] = xe[a] * ze[b];
             ent.push_back(e);
-            tile_of.push_back(owner_tile(J.zind[t * 3 + 1], nz, TZ) * tiles_x + owner_tile(J.xind[t * 3 + 1], nx, TX));
+            unit.push_back(U.unit_of(J.xind[t * 3 + 1], J.zind[t * 3 + 1]));
+            row.push_back(J.xind[t * 3 + 1]);
+            zk.push_back(J.zind[t * 3 + 1]);
         }
-    std::vector<size_t> idx(ent.size());
-    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return tile_of[a] < tile_of[b]; });
-    out.clear();
-    off.assign(ntiles + 1, 0);
-    for (size_t i : idx) {
-        out.push_back(ent[i]);
-        off[tile_of[i] + 1]++;
-    }
-    for (int t = 0; t < ntiles; t++) off[t + 1] += off[t];
+    group_entries(U, ent, unit, row, zk, out, off, roff);
 }
 
 static StepConst make_const(const fwi2d_params &p, float dx, float dz)
@@ -473,8 +632,6 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
     d.ldz = M.ldz;
     d.x0 = s.x0;
     d.nt = s.nt;
-    d.tiles_x = s.tiles_x;
-    d.tiles_z = s.tiles_z;
     d.u[0] = s.u0.as<float>();
     d.u[1] = s.u1.as<float>();
     if (!adjoint) {
@@ -484,8 +641,11 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
         d.nrcv = s.nrcv_rows;
         d.inj = s.d_inj_f.as<InjEntry>();
         d.inj_off = s.d_inj_f_off.as<int>();
+        d.inj_roff = s.d_inj_f_roff.as<int>();
         d.ext = s.d_ext_f.as<ExtEntry>();
         d.ext_off = s.d_ext_f_off.as<int>();
+        d.ext_roff = s.d_ext_f_roff.as<int>();
+        d.n_ext = (int)s.ext_f.size();
     } else {
         d.src = s.src_a.as<float>();
         d.nsrc = s.nrcv_rows;
@@ -493,8 +653,11 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
         d.nrcv = 0;
         d.inj = s.d_inj_a.as<InjEntry>();
         d.inj_off = s.d_inj_a_off.as<int>();
+        d.inj_roff = s.d_inj_a_roff.as<int>();
         d.ext = nullptr;
         d.ext_off = s.d_ext_none_off.as<int>();
+        d.ext_roff = s.d_ext_none_roff.as<int>();
+        d.n_ext = 0;
     }
     d.den = s.den.as<float>();
     d.tz = s.tz.as<float>();
@@ -600,29 +763,35 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     P->C = make_const(p, M.dx, M.dz);
     P->dtg = (float)(P->C.sub) * p.dt;
 
-    // tile shape: the requested one, else the first that tiles every shot
-    // grid.  An axis of n samples takes tiles of T when n == T or n >= T + 8,
-    // so that each SBP boundary band lies in a window that reaches its boundary.
-    auto fits = [&](int T, int n) { return n == T || n >= T + 8; };
+    // shape: the requested one, else the marching kernel where it has enough
+    // units to fill the GPU, else the first tile shape that fits every shot
     auto shape_ok = [&](int i) {
-        int tz, tx;
-        elastic_tile_shape(i, &tz, &tx);
-        if (!fits(tz, M.nz)) return false;
         for (int s = 0; s < nshots; s++)
-            if (!fits(tx, shots[s].nx)) return false;
+            if (!shape_fits(i, shots[s].nx, M.nz)) return false;
         return true;
     };
-    const int nshapes = elastic_tile_count();
     int shape = p.tile_shape;
-    if (shape < 0 || shape >= nshapes) {
+    if (shape < 0 || shape >= shape_count()) {
         shape = -1;
-        for (int i = 0; i < nshapes && shape < 0; i++)
+        const int m0 = elastic_tile_count();
+        if (shape_ok(m0)) {
+            long long units = 0;
+            for (int s = 0; s < nshots; s++) units += (long long)make_units(m0, s, shots[s].nx, M.nz).marches.size();
+            if (units >= 148) shape = m0;
+        }
+        for (int i = 0; i < elastic_tile_count() && shape < 0; i++)
             if (shape_ok(i)) shape = i;
         REQ(shape >= 0, "no tile shape fits the grid (an axis needs n == T or n >= T + 8)");
     }
     REQ(shape_ok(shape), "the requested tile shape does not fit a shot grid");
     P->shape = shape;
-    elastic_tile_shape(shape, &P->TZ, &P->TX);
+    P->march = shape >= elastic_tile_count();
+    P->tshape = P->march ? kBandTile : shape;
+    elastic_tile_shape(P->tshape, &P->TZ, &P->TX);
+    if (P->march) {
+        P->nth = kMarchShapes[shape - elastic_tile_count()].nth;
+        P->lx = kMarchShapes[shape - elastic_tile_count()].lx;
+    }
 
     const bool vti = M.kind == KIND_VTI;
     long long total_bytes = 0;
@@ -641,9 +810,8 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->nx = sh.nx;
         S->nt = sh.nt;
         S->ncomp = 2;
-        S->tiles_x = (sh.nx + P->TX - 1) / P->TX;
-        S->tiles_z = (M.nz + P->TZ - 1) / P->TZ;
-        const int ntiles = S->tiles_x * S->tiles_z;
+        const ShotUnits U = make_units(shape, s, sh.nx, M.nz);
+        const int nunits = U.nunits();
         S->ntr_src = sh.src.ntr;
         S->ncomp_src = p.mt ? 3 : 2;
         S->nr = sh.rcv.ntr;
@@ -661,11 +829,12 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             ra[1] = 2 * S->ntr_src;     // next1: inx = mxz, inz = mzz
             rb[1] = S->ntr_src;
         }
-        build_inj(sh.src, 2, ra, rb, sh.nx, M.nz, P->TX, P->TZ, S->tiles_x, ntiles, S->inj_f, S->inj_f_off);
+        build_inj(sh.src, 2, ra, rb, U, S->inj_f, S->inj_f_off, S->inj_f_roff);
         int qa[2] = {0, S->nr}, qb[2] = {0, 0};
-        build_inj(sh.rcv, 2, qa, qb, sh.nx, M.nz, P->TX, P->TZ, S->tiles_x, ntiles, S->inj_a, S->inj_a_off);
-        build_ext(sh.rcv, 2, sh.nx, M.nz, P->TX, P->TZ, S->tiles_x, ntiles, S->ext_f, S->ext_f_off);
-        S->ext_none_off.assign(ntiles + 1, 0);
+        build_inj(sh.rcv, 2, qa, qb, U, S->inj_a, S->inj_a_off, S->inj_a_roff);
+        build_ext(sh.rcv, 2, U, S->ext_f, S->ext_f_off, S->ext_f_roff);
+        S->ext_none_off.assign(nunits + 1, 0);
+        S->ext_none_roff.assign(S->ext_f_roff.size(), 0);
 
         // boundary divisors and taper on this shot's window of the model
         std::vector<float> den, tz, tx;
@@ -700,6 +869,10 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->d_ext_f.upload(S->ext_f, ctx->st);
         S->d_ext_f_off.upload(S->ext_f_off, ctx->st);
         S->d_ext_none_off.upload(S->ext_none_off, ctx->st);
+        S->d_inj_f_roff.upload(S->inj_f_roff, ctx->st);
+        S->d_inj_a_roff.upload(S->inj_a_roff, ctx->st);
+        S->d_ext_f_roff.upload(S->ext_f_roff, ctx->st);
+        S->d_ext_none_roff.upload(S->ext_none_roff, ctx->st);
         S->den.upload(den, ctx->st);
         S->tz.upload(tz, ctx->st);
         S->tx.upload(tx, ctx->st);
@@ -714,12 +887,13 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             total_bytes += bytes;
         }
         P->nt_max = std::max(P->nt_max, sh.nt);
-        for (int tzi = 0; tzi < S->tiles_z; tzi++)
-            for (int txi = 0; txi < S->tiles_x; txi++) P->tiles.push_back(TileRef{s, txi, tzi, 0});
+        P->tiles.insert(P->tiles.end(), U.tiles.begin(), U.tiles.end());
+        P->marches.insert(P->marches.end(), U.marches.begin(), U.marches.end());
         P->shots.push_back(std::move(S));
     }
     P->have_snapshots = p.sub > 0;
     P->d_tiles.upload(P->tiles, ctx->st);
+    P->d_march.upload(P->marches, ctx->st);
     std::vector<ShotDev> sf(nshots), sa(nshots);
     for (int s = 0; s < nshots; s++) {
         shot_dev(*P, *P->shots[s], M, false, sf[s]);
@@ -734,6 +908,24 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     ctx->plan = std::move(P);
 }
 
+// One time step of every shot: the tile kernel on its units, then the
+// marching kernel on the interior rows.  Returns the number of launches.
+static int launch_step(const Plan &P, const ShotDev *shots, const ModelDev &md, int it, int flags, cudaStream_t st)
+{
+    int n = 0;
+    if (!P.tiles.empty()) {
+        launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md,
+                            P.C, it, flags, P.dtg, st);
+        n++;
+    }
+    if (!P.marches.empty()) {
+        launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>(), (int)P.marches.size(), P.nth, md,
+                             P.C, it, flags, P.dtg, st);
+        n++;
+    }
+    return n;
+}
+
 // Time `steps` forward steps of the current plan (fields zeroed, no output),
 // in milliseconds per step.
 static float time_forward_steps(fwi2d_ctx *ctx, int steps)
@@ -746,16 +938,12 @@ static float time_forward_steps(fwi2d_ctx *ctx, int steps)
     const ModelDev md = ctx->M.dev();
     const ShotDev *shots = P.d_shots_f.as<ShotDev>();
     const int nsteps = std::min(steps, P.nt_max - 1);
-    for (int it = 0; it < std::min(3, nsteps); it++)
-        launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
-                            it, STEP_EXTRACT, P.dtg, ctx->st);
+    for (int it = 0; it < std::min(3, nsteps); it++) launch_step(P, shots, md, it, STEP_EXTRACT, ctx->st);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     CK(cudaEventRecord(a, ctx->st));
-    for (int it = 0; it < nsteps; it++)
-        launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
-                            it, STEP_EXTRACT, P.dtg, ctx->st);
+    for (int it = 0; it < nsteps; it++) launch_step(P, shots, md, it, STEP_EXTRACT, ctx->st);
     CK(cudaEventRecord(b, ctx->st));
     CK(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -786,7 +974,7 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
             if (kv.first == key) chosen = kv.second;
         if (chosen < 0 && cells >= 20000000LL) {
             float best = 1e30f;
-            for (int s = 0; s < elastic_tile_count(); s++) {
+            for (int s = 0; s < shape_count(); s++) {
                 fwi2d_params q = p;
                 q.tile_shape = s;
                 q.sub = 0;
@@ -843,11 +1031,7 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
         }
     }
     const ModelDev md = M.dev();
-    for (int it = 0; it < P.nt_max - 1; it++) {
-        launch_elastic_step(P.shape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
-                            it, flags, P.dtg, cst);
-        n++;
-    }
+    for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(P, shots, md, it, flags, cst);
     if (!adj) {
         launch_finalize(shots, nshots, P.C, 2, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
         n++;
@@ -1375,8 +1559,9 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     REQ(ctx, "null context");
     Plan &P = need_plan(ctx);
     const long long steps = P.nt_max - 1;
-    if (lf) *lf = steps + 2;
-    if (la) *la = steps + 1 + (long long)P.shots.size();
+    const long long per = (P.tiles.empty() ? 0 : 1) + (P.marches.empty() ? 0 : 1);
+    if (lf) *lf = steps * per + 2;
+    if (la) *la = steps * per + 1 + (long long)P.shots.size();
     if (shape) *shape = P.shape;
     if (snap_bytes) *snap_bytes = P.snap_bytes;
     ABI_END
@@ -1422,13 +1607,17 @@ int fwi2d_last_timing(fwi2d_ctx *ctx, float *forward_ms, float *adjoint_ms)
     ABI_END
 }
 
-int fwi2d_tile_shape_count(void) { return elastic_tile_count(); }
+int fwi2d_tile_shape_count(void) { return shape_count(); }
 
 int fwi2d_tile_shape(int index, int *tz, int *tx)
 {
     ABI_TRY
-    REQ(index >= 0 && index < elastic_tile_count() && tz && tx, "no such tile shape");
-    elastic_tile_shape(index, tz, tx);
+    REQ(index >= 0 && index < shape_count() && tz && tx, "no such tile shape");
+    if (index < elastic_tile_count()) elastic_tile_shape(index, tz, tx);
+    else {
+        *tz = kMarchShapes[index - elastic_tile_count()].nth;
+        *tx = kMarchShapes[index - elastic_tile_count()].lx;
+    }
     ABI_END
 }
 

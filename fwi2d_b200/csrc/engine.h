@@ -41,16 +41,18 @@ struct ShotDev {
     int nx, nz, ldz;      // shot grid (nz == model nz)
     int x0;               // first model column of this shot's grid
     int nt;               // time samples of this shot
-    int tiles_x, tiles_z;
     float *u[2];          // two field buffers, each [ncomp][nx][ldz]
     const float *src;     // time-major injection traces [nt][nsrc]
     int nsrc;
     float *rcv;           // time-major extraction output [nt][nrcv]
     int nrcv;
-    const InjEntry *inj;  // sorted by (tile, cell, trace)
-    const int *inj_off;   // [tiles+1]
-    const ExtEntry *ext;
-    const int *ext_off;   // [tiles+1]
+    const InjEntry *inj;  // grouped by work unit; march units sorted by (x, z), reference order per cell
+    const int *inj_off;   // [units+1]
+    const int *inj_roff;  // per march unit and row: first entry of the row (absolute index)
+    const ExtEntry *ext;  // grouped by the unit owning the pivot; march units sorted by pivot row
+    const int *ext_off;   // [units+1]
+    const int *ext_roff;
+    int n_ext;
     const float *den;     // absorbing-boundary divisors: [ncomp][2*nx + 2*nz] (top, bottom, left, right)
     const float *tz;      // taper factor along z [nz]
     const float *tx;      // taper factor along x [nx]
@@ -93,9 +95,34 @@ struct StepConst {
     int kahan;                   // compensated gradient accumulation
 };
 
-// Per-launch tile table entry.
+// Work unit of the tile kernel: a TX x TZ window of one shot grid starting
+// at (wx0, wz0) that writes the cells of [ox0, ox1) x [oz0, oz1).
 struct TileRef {
-    int shot, tx, tz, pad;
+    int shot, unit;
+    int wx0, ox0, ox1;
+    int wz0, oz0, oz1;
 };
+
+// Work unit of the x-marching kernel: rows [xb, xe) (all clear of the x
+// boundary bands) of a z window of 2*blockDim.x cells starting at za (even,
+// -2 for the first window) that writes the cells of [oz0, oz1).  roff is the
+// first of this unit's (xe - xb + 1) per-row entry offsets.
+struct MarchRef {
+    int shot, unit;
+    int xb, xe;
+    int za, oz0, oz1;
+    int roff;
+};
+
+// Tile k of an axis of n samples with tiles of T (n == T or n >= T + 8):
+// the window [min(kT, n-T), +T) owns the cells up to the next window, the
+// last window is flush with the far boundary.
+inline void tile_window_host(int k, int ntile, int n, int T, int &w0, int &o0, int &o1)
+{
+    auto w = [&](int i) { return i * T < n - T ? i * T : n - T; };
+    w0 = w(k);
+    o0 = k == 0 ? 0 : w(k);
+    o1 = k == ntile - 1 ? n : w(k + 1);
+}
 
 }  // namespace fwi2d

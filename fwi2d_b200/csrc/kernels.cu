@@ -26,6 +26,7 @@
 #include <cstdio>
 #include "engine.h"
 #include "sbp.cuh"
+#include "launch.h"
 
 namespace fwi2d {
 
@@ -57,11 +58,6 @@ __device__ __forceinline__ float snap_load(const void *base, long long idx, int 
     return __half2float(((const __half *)base)[idx]) * inv;
 }
 
-__device__ __forceinline__ void tile_window(int k, int ntile, int n, int T, int &w0, int &own_hi)
-{
-    w0 = min(k * T, n - T);
-    own_hi = (k == ntile - 1) ? n : min((k + 1) * T, n - T);
-}
 
 // ---------------------------------------------------------------------------
 // Elastic isotropic / VTI step.
@@ -134,14 +130,13 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     const int nt = Sp->nt;
     if (it >= nt - 1) return;
     const int nx = Sp->nx, nz = Sp->nz, ldz = Sp->ldz;
-    const int tiles_x = Sp->tiles_x, tiles_z = Sp->tiles_z;
     const int nxz = nx * ldz;
-    int wx0, ownx, wz0, ownz;
-    tile_window(tr.tx, tiles_x, nx, TX, wx0, ownx);
-    tile_window(tr.tz, tiles_z, nz, TZ, wz0, ownz);
+    const int wx0 = tr.wx0, wz0 = tr.wz0;
     // every point this tile evaluates is clear of the SBP boundary bands
     const bool interior = wx0 >= 6 && wx0 + TX + 6 <= nx && wz0 >= 6 && wz0 + TZ + 6 <= nz;
-    const bool lean = RZ == 2 && interior && (wz0 & 3) == 0;
+    // the lean path writes every cell of its window: only for tiles that own all of it
+    const bool full = tr.ox0 == wx0 && tr.ox1 == wx0 + TX && tr.oz0 == wz0 && tr.oz1 == wz0 + TZ;
+    const bool lean = RZ == 2 && interior && full && (wz0 & 3) == 0;
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
@@ -303,7 +298,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
 
     // ---- phase 3
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tile_id = tr.tz * tiles_x + tr.tx;
+    const int tile_id = tr.unit;
 
     // receivers (forward): one thread per receiver of this tile
     if (flags & F_EXTRACT) {
@@ -499,7 +494,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
         for (int h = 0; h < RZ; h++) {
             const int tz = lane + 32 * h, tx = warp;
             const int gx = wx0 + tx, gz = wz0 + tz;
-            const bool owned = (gx < ownx) && (gz < ownz);
+            const bool owned = gx >= tr.ox0 && gx < tr.ox1 && gz >= tr.oz0 && gz < tr.oz1;
             if (!owned) continue;
             const int ui = (tx + 4) * UZ + (tz + 4);
             const int wi = (tx + 2) * WZ + (tz + 2);
@@ -694,6 +689,10 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     }
 }
 
+}  // namespace fwi2d
+#include "march.cuh"
+namespace fwi2d {
+
 // ---------------------------------------------------------------------------
 // Initial state (we_op.cpp:657-663): inject sample 0 into a zeroed field and
 // scale by dt^2/(2 rho) in double.  One thread per touched cell, entries in
@@ -731,8 +730,7 @@ __global__ void finalize_shots(const ShotDev *__restrict__ shots, int nshots, St
     const float *curr = S.u[(it + 1) & 1];
     const long long nxz = (long long)S.nx * S.ldz;
     if (flags & F_EXTRACT) {
-        const int tiles = S.tiles_x * S.tiles_z;
-        const int e1 = S.ext_off[tiles];
+        const int e1 = S.n_ext;
         for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < e1; e += gridDim.x * blockDim.x) {
             const ExtEntry E = S.ext[e];
             const float *U = curr + E.comp * nxz;
@@ -830,6 +828,47 @@ void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRe
                 : launch_elastic_t<false, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
     default: vti ? launch_elastic_t<true, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
                  : launch_elastic_t<false, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
+    }
+}
+
+template <bool VTI, bool GRAD, int NTH>
+static void launch_march_n(const ShotDev *shots, const MarchRef *units, int nunits, const ModelDev &M,
+                           const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    constexpr size_t bytes = sizeof(float) * MarchLayout<VTI, GRAD, NTH>::FLOATS;
+    static bool configured = false;   // per process; a kernel attribute applies to every device
+    if (!configured) {
+        cudaFuncSetAttribute(elastic_march<VTI, GRAD, NTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        configured = true;
+    }
+    elastic_march<VTI, GRAD, NTH><<<nunits, NTH, bytes, st>>>(shots, units, M, C, it, flags, dtg);
+}
+
+template <bool VTI, bool GRAD>
+static void launch_march_g(const ShotDev *shots, const MarchRef *units, int nunits, int nth, const ModelDev &M,
+                           const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    switch (nth) {
+    case 128: launch_march_n<VTI, GRAD, 128>(shots, units, nunits, M, C, it, flags, dtg, st); break;
+    case 192: launch_march_n<VTI, GRAD, 192>(shots, units, nunits, M, C, it, flags, dtg, st); break;
+    case 224: launch_march_n<VTI, GRAD, 224>(shots, units, nunits, M, C, it, flags, dtg, st); break;
+    default: launch_march_n<VTI, GRAD, 256>(shots, units, nunits, M, C, it, flags, dtg, st); break;
+    }
+}
+
+bool march_threads_ok(int nth) { return nth == 128 || nth == 192 || nth == 224 || nth == 256; }
+
+void launch_elastic_march(bool vti, const ShotDev *shots, const MarchRef *units, int nunits, int nth,
+                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    if (nunits <= 0) return;
+    const bool grad = (flags & F_GRAD) != 0;
+    if (vti) {
+        if (grad) launch_march_g<true, true>(shots, units, nunits, nth, M, C, it, flags, dtg, st);
+        else launch_march_g<true, false>(shots, units, nunits, nth, M, C, it, flags, dtg, st);
+    } else {
+        if (grad) launch_march_g<false, true>(shots, units, nunits, nth, M, C, it, flags, dtg, st);
+        else launch_march_g<false, false>(shots, units, nunits, nth, M, C, it, flags, dtg, st);
     }
 }
 

@@ -13,6 +13,11 @@ int elastic_tile_count();
 void elastic_tile_shape(int i, int *tz, int *tx);
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+// x-marching kernel for the rows clear of the x boundary bands; nth threads
+// per unit, one z cell each (march_threads_ok lists the compiled widths)
+bool march_threads_ok(int nth);
+void launch_elastic_march(bool vti, const ShotDev *shots, const MarchRef *units, int nunits, int nth,
+                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
                        cudaStream_t st);
 void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st);

@@ -396,7 +396,13 @@ extern "C" int fwi2d_propagate_noalloc(const float *model, const float *allsrc, 
                    p.bc_right == 2);
     tapers(nx, nz, p);
     for (int tzi = 0, k = 0; tzi < tiles_z; tzi++)
-        for (int txi = 0; txi < tiles_x; txi++) h_tiles[k++] = TileRef{0, txi, tzi, 0};
+        for (int txi = 0; txi < tiles_x; txi++, k++) {
+            TileRef &r = h_tiles[k];
+            r.shot = 0;
+            r.unit = k;
+            tile_window_host(txi, tiles_x, nx, TX, r.wx0, r.ox0, r.ox1);
+            tile_window_host(tzi, tiles_z, nz, TZ, r.wz0, r.oz0, r.oz1);
+        }
     const float one = 1.f;
 
     ShotDev sd;
@@ -406,8 +412,7 @@ extern "C" int fwi2d_propagate_noalloc(const float *model, const float *allsrc, 
     sd.ldz = ldz;
     sd.x0 = 0;
     sd.nt = nt;
-    sd.tiles_x = tiles_x;
-    sd.tiles_z = tiles_z;
+    sd.n_ext = next;
     sd.u[0] = (float *)(S + o_u0);
     sd.u[1] = (float *)(S + o_u1);
     sd.src = (const float *)(S + o_src);
