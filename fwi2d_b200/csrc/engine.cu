@@ -210,10 +210,11 @@ struct ShotPlan {
     std::vector<InjEntry> inj_f, inj_a;
     std::vector<int> inj_f_off, inj_a_off, inj_f_roff, inj_a_roff;
     std::vector<ExtEntry> ext_f;
-    std::vector<int> ext_f_off, ext_none_off, ext_f_roff, ext_none_roff;
+    std::vector<int> ext_f_off, ext_none_off, ext_f_roff;
+    std::vector<MarchRow> mrow_f, mrow_a;
     DevBuf u0, u1, src_f, rcv_f, src_a;
     DevBuf d_inj_f, d_inj_f_off, d_inj_a, d_inj_a_off, d_ext_f, d_ext_f_off, d_ext_none_off;
-    DevBuf d_inj_f_roff, d_inj_a_roff, d_ext_f_roff, d_ext_none_roff;
+    DevBuf d_mrow_f, d_mrow_a;
     DevBuf den, tz, tx, snap, amax, grad, gwt;
 };
 
@@ -229,7 +230,8 @@ struct Plan {
     std::vector<std::unique_ptr<ShotPlan>> shots;
     std::vector<TileRef> tiles;
     std::vector<MarchRef> marches;
-    DevBuf d_tiles, d_march, d_shots_f, d_shots_a;
+    std::vector<BandRef> bands;
+    DevBuf d_tiles, d_march, d_bands, d_shots_f, d_shots_a;
     // initial-state cells per mode (0 forward, 1 adjoint)
     std::vector<InitCell> icells[2];
     std::vector<int> ioff[2], iidx[2];
@@ -262,6 +264,8 @@ struct fwi2d_ctx {
     int device = 0;
     cudaStream_t st = nullptr;      // stream all work is ordered on
     cudaStream_t own = nullptr;     // the context's own stream
+    cudaStream_t side = nullptr;    // boundary-band kernels run here, overlapping the core kernel
+    cudaEvent_t fork = nullptr, join = nullptr;
     fwi2d::ModelState M;
     std::unique_ptr<fwi2d::Plan> plan;
 };
@@ -362,8 +366,9 @@ static void check_injector(const fwi2d_injector &J, int nx, int nz, const char *
 
 // ---- work decomposition ---------------------------------------------------------
 // A plan runs either the tile kernel over the whole of every shot grid, or the
-// marching kernel over the rows clear of the x boundary bands (6 <= x < nx-6)
-// with the tile kernel (tiles of kBandTile) on the two bands.
+// marching kernel over the cells clear of the four boundary bands
+// (6 <= x < nx-6, 6 <= z < nz-6), the tile kernel (full-height tiles of
+// kBandTile) on the x bands and the band kernel on the top and bottom bands.
 struct MarchShape {
     int nth, lx;
 };
@@ -382,40 +387,53 @@ struct ShotUnits {
     int nx = 0, nz = 0;
     int TX = 0, TZ = 0, tiles_x = 0, tiles_z = 0;
     int lx = 0, nseg = 0, nwin = 0;
-    std::vector<int> zo;           // marching: owned z starts of the windows, plus nz
-    std::vector<TileRef> tiles;
+    std::vector<int> zo;           // marching: owned z starts of the core windows, plus nz - 6
+    std::vector<TileRef> tiles;    // marching plans: the x-band tiles
+    std::vector<BandRef> bands;    // top / bottom band units (two per run of rows)
     std::vector<MarchRef> marches;
-    int nunits() const { return (int)(tiles.size() + marches.size()); }
+    int nunits() const { return (int)(tiles.size() + bands.size() + marches.size()); }
     int unit_of(int x, int z) const
     {
         if (!march) return owner_tile(z, nz, TZ) * tiles_x + owner_tile(x, nx, TX);
         if (x < kBand) return owner_tile(z, nz, TZ);
         if (x >= nx - kBand) return tiles_z + owner_tile(z, nz, TZ);
+        const int nt = (int)tiles.size();
+        if (z < kBand || z >= nz - kBand) return nt + 2 * ((x - kBand) / zband_rows()) + (z < kBand ? 0 : 1);
         const int seg = (x - kBand) / lx;
         const int k = (int)(std::upper_bound(zo.begin(), zo.end(), z) - zo.begin()) - 1;
-        return 2 * tiles_z + seg * nwin + k;
+        return nt + (int)bands.size() + seg * nwin + k;
     }
-    bool is_march(int u) const { return u >= (int)tiles.size(); }
-    const MarchRef &mref(int u) const { return marches[u - tiles.size()]; }
+    // units whose entries are sorted by row and indexed by per-row records
+    bool row_sorted(int u) const { return u >= (int)tiles.size(); }
+    struct RowUnit {
+        int unit, xb, xe, roff;
+    };
+    std::vector<RowUnit> row_units() const
+    {
+        std::vector<RowUnit> r;
+        for (const BandRef &b : bands) r.push_back({b.unit, b.xb, b.xe, b.roff});
+        for (const MarchRef &m : marches) r.push_back({m.unit, m.xb, m.xe, m.roff});
+        return r;
+    }
 };
 
 static bool axis_fits(int T, int n) { return n == T || n >= T + 8; }
 
-// z windows of the marching kernel for nth threads: window k owns
-// [zo[k], zo[k+1]) and covers [za, za + nth), two cells beyond its owned range
-// on each side; the last window owns at least 8 cells and its ring reaches
-// 8 cells above the bottom, so each SBP boundary band lies in one window.
+// Core z windows of the marching kernel for nth threads: window k owns
+// [zo[k], zo[k+1]) within [6, nz-6) and covers [za, za + nth), two cells
+// beyond its owned range on each side (the last one flush with nz-4, or
+// starting at 4 when one window covers the whole core), so every cell it
+// evaluates lies in [4, nz-4) where the stencils take their interior form.
 static void march_windows(int nz, int nth, std::vector<int> &zo, std::vector<int> &za)
 {
-    const int w = nth - 4;
-    const int K = (nz + w - 1) / w;
+    const int w = nth - 4, lo = kBand, hi = nz - kBand;
+    const int K = (hi - lo + w - 1) / w;
     zo.assign(K + 1, 0);
-    for (int k = 0; k < K; k++) zo[k] = k * w;
-    zo[K] = nz;
-    if (K > 1 && nz - zo[K - 1] < 8) zo[K - 1] = nz - 8;
+    for (int k = 0; k < K; k++) zo[k] = lo + k * w;
+    zo[K] = hi;
     za.assign(K, 0);
     for (int k = 0; k < K; k++) za[k] = zo[k] - 2;
-    if (K > 1) za[K - 1] = std::min(zo[K - 1] - 2, nz + 2 - nth);
+    if (K > 1) za[K - 1] = std::max(lo - 2, std::min(zo[K - 1] - 2, hi + 2 - nth));
 }
 
 // Whether a shape can run a shot grid of nx x nz.
@@ -428,7 +446,7 @@ static bool shape_fits(int shape, int nx, int nz)
         return axis_fits(tz, nz) && axis_fits(tx, nx);
     }
     elastic_tile_shape(kBandTile, &tz, &tx);
-    return axis_fits(tz, nz) && nx >= 2 * tx && nx > 2 * kBand && nz >= 16 &&
+    return axis_fits(tz, nz) && nx >= 2 * tx && nx > 2 * kBand && nz >= 40 &&
            march_threads_ok(kMarchShapes[shape - elastic_tile_count()].nth);
 }
 
@@ -465,6 +483,19 @@ static ShotUnits make_units(int shape, int shot, int nx, int nz)
             tile_window_host(tzi, U.tiles_z, nz, U.TZ, r.wz0, r.oz0, r.oz1);
             U.tiles.push_back(r);
         }
+    int roff = 0;
+    for (int a = kBand; a < nx - kBand; a += zband_rows())
+        for (int side = 0; side < 2; side++) {
+            BandRef b;
+            b.shot = shot;
+            b.unit = (int)(U.tiles.size() + U.bands.size());
+            b.xb = a;
+            b.xe = std::min(a + zband_rows(), nx - kBand);
+            b.side = side;
+            b.roff = roff;
+            roff += b.xe - b.xb + 1;
+            U.bands.push_back(b);
+        }
     const MarchShape ms = kMarchShapes[shape - elastic_tile_count()];
     std::vector<int> za;
     march_windows(nz, ms.nth, U.zo, za);
@@ -472,12 +503,11 @@ static ShotUnits make_units(int shape, int shot, int nx, int nz)
     U.lx = ms.lx;
     const int rows = nx - 2 * kBand;
     U.nseg = (rows + U.lx - 1) / U.lx;
-    int roff = 0;
     for (int sg = 0; sg < U.nseg; sg++)
         for (int k = 0; k < U.nwin; k++) {
             MarchRef m;
             m.shot = shot;
-            m.unit = (int)(U.tiles.size() + U.marches.size());
+            m.unit = (int)(U.tiles.size() + U.bands.size() + U.marches.size());
             m.xb = kBand + sg * U.lx;
             m.xe = std::min(m.xb + U.lx, nx - kBand);
             m.za = za[k];
@@ -504,7 +534,7 @@ static void group_entries(const ShotUnits &U, const std::vector<E> &ent, const s
     for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
     std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
         if (unit[a] != unit[b]) return unit[a] < unit[b];
-        if (!U.is_march(unit[a])) return false;
+        if (!U.row_sorted(unit[a])) return false;
         if (row[a] != row[b]) return row[a] < row[b];
         return zkey[a] < zkey[b];
     });
@@ -515,10 +545,11 @@ static void group_entries(const ShotUnits &U, const std::vector<E> &ent, const s
         off[unit[i] + 1]++;
     }
     for (int t = 0; t < nu; t++) off[t + 1] += off[t];
+    const std::vector<ShotUnits::RowUnit> rus = U.row_units();
     int nro = 0;
-    for (const MarchRef &m : U.marches) nro += m.xe - m.xb + 1;
+    for (const auto &m : rus) nro += m.xe - m.xb + 1;
     roff.assign(std::max(nro, 1), 0);
-    for (const MarchRef &m : U.marches) {
+    for (const auto &m : rus) {
         int e = off[m.unit];
         for (int r = m.xb; r <= m.xe; r++) {
             while (e < off[m.unit + 1] && row[idx[e]] < r) e++;
@@ -592,6 +623,32 @@ static void build_ext(const fwi2d_injector &J, int ncomp, const ShotUnits &U, st
     group_entries(U, ent, unit, row, zk, out, off, roff);
 }
 
+// Row records of the marching units from the per-row entry offsets.
+static void build_march_rows(const ShotUnits &U, const std::vector<InjEntry> &inj, const std::vector<int> &iroff,
+                             const std::vector<int> *eroff, const std::vector<float> &tx, std::vector<MarchRow> &out)
+{
+    out.clear();
+    for (const auto &m : U.row_units())
+        for (int r = m.xb; r <= m.xe; r++) {   // one spare record per unit keeps the roff layout
+            MarchRow R;
+            std::memset(&R, 0, sizeof(R));
+            const int k = m.roff + r - m.xb;
+            if (r == m.xe) {
+                out.push_back(R);
+                continue;
+            }
+            R.e0 = iroff[k];
+            R.e1 = iroff[k + 1];
+            R.zlo = R.e1 > R.e0 ? inj[R.e0].gz : 0;
+            R.zhi = R.e1 > R.e0 ? inj[R.e1 - 1].gz : -1;
+            R.r0 = eroff ? (*eroff)[k] : 0;
+            R.r1 = eroff ? (*eroff)[k + 1] : 0;
+            R.tx = tx[r];
+            out.push_back(R);
+        }
+    if (out.empty()) out.resize(1);
+}
+
 static StepConst make_const(const fwi2d_params &p, float dx, float dz)
 {
     StepConst C;
@@ -641,11 +698,10 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
         d.nrcv = s.nrcv_rows;
         d.inj = s.d_inj_f.as<InjEntry>();
         d.inj_off = s.d_inj_f_off.as<int>();
-        d.inj_roff = s.d_inj_f_roff.as<int>();
         d.ext = s.d_ext_f.as<ExtEntry>();
         d.ext_off = s.d_ext_f_off.as<int>();
-        d.ext_roff = s.d_ext_f_roff.as<int>();
         d.n_ext = (int)s.ext_f.size();
+        d.mrow = s.d_mrow_f.as<MarchRow>();
     } else {
         d.src = s.src_a.as<float>();
         d.nsrc = s.nrcv_rows;
@@ -653,11 +709,10 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
         d.nrcv = 0;
         d.inj = s.d_inj_a.as<InjEntry>();
         d.inj_off = s.d_inj_a_off.as<int>();
-        d.inj_roff = s.d_inj_a_roff.as<int>();
         d.ext = nullptr;
         d.ext_off = s.d_ext_none_off.as<int>();
-        d.ext_roff = s.d_ext_none_roff.as<int>();
         d.n_ext = 0;
+        d.mrow = s.d_mrow_a.as<MarchRow>();
     }
     d.den = s.den.as<float>();
     d.tz = s.tz.as<float>();
@@ -834,7 +889,6 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         build_inj(sh.rcv, 2, qa, qb, U, S->inj_a, S->inj_a_off, S->inj_a_roff);
         build_ext(sh.rcv, 2, U, S->ext_f, S->ext_f_off, S->ext_f_roff);
         S->ext_none_off.assign(nunits + 1, 0);
-        S->ext_none_roff.assign(S->ext_f_roff.size(), 0);
 
         // boundary divisors and taper on this shot's window of the model
         std::vector<float> den, tz, tx;
@@ -869,10 +923,10 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->d_ext_f.upload(S->ext_f, ctx->st);
         S->d_ext_f_off.upload(S->ext_f_off, ctx->st);
         S->d_ext_none_off.upload(S->ext_none_off, ctx->st);
-        S->d_inj_f_roff.upload(S->inj_f_roff, ctx->st);
-        S->d_inj_a_roff.upload(S->inj_a_roff, ctx->st);
-        S->d_ext_f_roff.upload(S->ext_f_roff, ctx->st);
-        S->d_ext_none_roff.upload(S->ext_none_roff, ctx->st);
+        build_march_rows(U, S->inj_f, S->inj_f_roff, &S->ext_f_roff, tx, S->mrow_f);
+        build_march_rows(U, S->inj_a, S->inj_a_roff, nullptr, tx, S->mrow_a);
+        S->d_mrow_f.upload(S->mrow_f, ctx->st);
+        S->d_mrow_a.upload(S->mrow_a, ctx->st);
         S->den.upload(den, ctx->st);
         S->tz.upload(tz, ctx->st);
         S->tx.upload(tx, ctx->st);
@@ -889,11 +943,13 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         P->nt_max = std::max(P->nt_max, sh.nt);
         P->tiles.insert(P->tiles.end(), U.tiles.begin(), U.tiles.end());
         P->marches.insert(P->marches.end(), U.marches.begin(), U.marches.end());
+        P->bands.insert(P->bands.end(), U.bands.begin(), U.bands.end());
         P->shots.push_back(std::move(S));
     }
     P->have_snapshots = p.sub > 0;
     P->d_tiles.upload(P->tiles, ctx->st);
     P->d_march.upload(P->marches, ctx->st);
+    P->d_bands.upload(P->bands, ctx->st);
     std::vector<ShotDev> sf(nshots), sa(nshots);
     for (int s = 0; s < nshots; s++) {
         shot_dev(*P, *P->shots[s], M, false, sf[s]);
@@ -908,21 +964,32 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     ctx->plan = std::move(P);
 }
 
-// One time step of every shot: the tile kernel on its units, then the
-// marching kernel on the interior rows.  Returns the number of launches.
-static int launch_step(const Plan &P, const ShotDev *shots, const ModelDev &md, int it, int flags, cudaStream_t st)
+// One time step of every shot.  Tile-only plans: one launch.  Marching
+// plans: the marching kernel on `st` while the tile kernel computes the
+// boundary bands on the context's side stream; the two branches write
+// disjoint cells and join before the next step.  Returns the number of
+// launches.
+static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, const ModelDev &md, int it, int flags,
+                       cudaStream_t st)
 {
     int n = 0;
-    if (!P.tiles.empty()) {
+    if (P.marches.empty()) {
         launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md,
                             P.C, it, flags, P.dtg, st);
-        n++;
+        return 1;
     }
-    if (!P.marches.empty()) {
-        launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>(), (int)P.marches.size(), P.nth, md,
-                             P.C, it, flags, P.dtg, st);
-        n++;
-    }
+    CK(cudaEventRecord(ctx->fork, st));
+    CK(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+    launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
+                        it, flags, P.dtg, ctx->side);
+    launch_elastic_zband(P.kind == KIND_VTI, P.d_bands.as<BandRef>(), (int)P.bands.size(), shots, md, P.C, it, flags,
+                         P.dtg, ctx->side);
+    n += 2;
+    CK(cudaEventRecord(ctx->join, ctx->side));
+    launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>(), (int)P.marches.size(), P.nth, md, P.C,
+                         it, flags, P.dtg, st);
+    n++;
+    CK(cudaStreamWaitEvent(st, ctx->join, 0));
     return n;
 }
 
@@ -938,12 +1005,12 @@ static float time_forward_steps(fwi2d_ctx *ctx, int steps)
     const ModelDev md = ctx->M.dev();
     const ShotDev *shots = P.d_shots_f.as<ShotDev>();
     const int nsteps = std::min(steps, P.nt_max - 1);
-    for (int it = 0; it < std::min(3, nsteps); it++) launch_step(P, shots, md, it, STEP_EXTRACT, ctx->st);
+    for (int it = 0; it < std::min(3, nsteps); it++) launch_step(ctx, P, shots, md, it, STEP_EXTRACT, ctx->st);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     CK(cudaEventRecord(a, ctx->st));
-    for (int it = 0; it < nsteps; it++) launch_step(P, shots, md, it, STEP_EXTRACT, ctx->st);
+    for (int it = 0; it < nsteps; it++) launch_step(ctx, P, shots, md, it, STEP_EXTRACT, ctx->st);
     CK(cudaEventRecord(b, ctx->st));
     CK(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -1031,7 +1098,7 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
         }
     }
     const ModelDev md = M.dev();
-    for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(P, shots, md, it, flags, cst);
+    for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(ctx, P, shots, md, it, flags, cst);
     if (!adj) {
         launch_finalize(shots, nshots, P.C, 2, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
         n++;
@@ -1417,6 +1484,9 @@ int fwi2d_ctx_create(int device, fwi2d_ctx **out)
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
     c->st = c->own;
     const SbpTables &t = sbp_tables();
     upload_sbp_tables(&t.b1[0][0], &t.b2[0][0][0], t.c2, t.c1, t.sc, t.hc);
@@ -1434,6 +1504,9 @@ int fwi2d_ctx_destroy(fwi2d_ctx *ctx)
     cudaStreamSynchronize(ctx->st);
     ctx->plan.reset();
     cudaStreamDestroy(ctx->own);
+    cudaStreamDestroy(ctx->side);
+    cudaEventDestroy(ctx->fork);
+    cudaEventDestroy(ctx->join);
     delete ctx;
     ABI_END
 }
@@ -1559,7 +1632,7 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     REQ(ctx, "null context");
     Plan &P = need_plan(ctx);
     const long long steps = P.nt_max - 1;
-    const long long per = (P.tiles.empty() ? 0 : 1) + (P.marches.empty() ? 0 : 1);
+    const long long per = P.marches.empty() ? 1 : 3;
     if (lf) *lf = steps * per + 2;
     if (la) *la = steps * per + 1 + (long long)P.shots.size();
     if (shape) *shape = P.shape;

@@ -37,6 +37,15 @@ struct InitCell {
     double factor;
 };
 
+// One row of a marching unit: its source entries [e0, e1) (sorted by z,
+// spanning [zlo, zhi]), its receivers [r0, r1) and its taper factor.  32 bytes,
+// fetched by one bulk copy per row.
+struct MarchRow {
+    int e0, e1, zlo, zhi, r0, r1;
+    float tx;
+    int pad;
+};
+
 struct ShotDev {
     int nx, nz, ldz;      // shot grid (nz == model nz)
     int x0;               // first model column of this shot's grid
@@ -48,11 +57,10 @@ struct ShotDev {
     int nrcv;
     const InjEntry *inj;  // grouped by work unit; march units sorted by (x, z), reference order per cell
     const int *inj_off;   // [units+1]
-    const int *inj_roff;  // per march unit and row: first entry of the row (absolute index)
     const ExtEntry *ext;  // grouped by the unit owning the pivot; march units sorted by pivot row
     const int *ext_off;   // [units+1]
-    const int *ext_roff;
     int n_ext;
+    const struct MarchRow *mrow;   // per march unit and row (MarchRef::roff + row - xb)
     const float *den;     // absorbing-boundary divisors: [ncomp][2*nx + 2*nz] (top, bottom, left, right)
     const float *tz;      // taper factor along z [nz]
     const float *tx;      // taper factor along x [nx]
@@ -106,12 +114,20 @@ struct TileRef {
 // Work unit of the x-marching kernel: rows [xb, xe) (all clear of the x
 // boundary bands) of a z window of 2*blockDim.x cells starting at za (even,
 // -2 for the first window) that writes the cells of [oz0, oz1).  roff is the
-// first of this unit's (xe - xb + 1) per-row entry offsets.
+// first of this unit's (xe - xb + 1) per-row offsets and row records.
 struct MarchRef {
     int shot, unit;
     int xb, xe;
     int za, oz0, oz1;
     int roff;
+};
+
+// Work unit of the top / bottom band kernel: rows [xb, xe) of one shot's
+// top (side 0: z < 6) or bottom (side 1: z >= nz-6) band; roff as MarchRef.
+struct BandRef {
+    int shot, unit;
+    int xb, xe;
+    int side, roff;
 };
 
 // Tile k of an axis of n samples with tiles of T (n == T or n >= T + 8):

@@ -691,6 +691,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
 
 }  // namespace fwi2d
 #include "march.cuh"
+#include "zband.cuh"
 namespace fwi2d {
 
 // ---------------------------------------------------------------------------
@@ -871,6 +872,22 @@ void launch_elastic_march(bool vti, const ShotDev *shots, const MarchRef *units,
         else launch_march_g<false, false>(shots, units, nunits, nth, M, C, it, flags, dtg, st);
     }
 }
+
+void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const ShotDev *shots, const ModelDev &M,
+                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    if (nunits <= 0) return;
+    const bool grad = (flags & F_GRAD) != 0;
+    if (vti) {
+        if (grad) elastic_zband<true, true><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        else elastic_zband<true, false><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+    } else {
+        if (grad) elastic_zband<false, true><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        else elastic_zband<false, false><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+    }
+}
+
+int zband_rows() { return kZbRows; }
 
 void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
                        cudaStream_t st)

@@ -13,11 +13,15 @@ int elastic_tile_count();
 void elastic_tile_shape(int i, int *tz, int *tx);
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
-// x-marching kernel for the rows clear of the x boundary bands; nth threads
-// per unit, one z cell each (march_threads_ok lists the compiled widths)
+// x-marching kernel for the cells clear of all four boundary bands; nth
+// threads per unit (one z cell each), a width march_threads_ok accepts
 bool march_threads_ok(int nth);
 void launch_elastic_march(bool vti, const ShotDev *shots, const MarchRef *units, int nunits, int nth,
                           const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+// top / bottom band kernel (rows clear of the x bands), zband_rows() rows per unit
+int zband_rows();
+void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const ShotDev *shots, const ModelDev &M,
+                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
                        cudaStream_t st);
 void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st);

@@ -1,79 +1,146 @@
 // x-marching elastic / VTI step kernel for the rows of a shot grid that lie
 // clear of the left and right SBP boundary bands (6 <= x < nx-6).
 //
-// One CTA owns a strip of z (a window of W = NTH cells, one per thread) and
-// marches along x over a run of rows [xb, xe).  Rows are contiguous in memory
-// (z fastest), so every row of every field is read from HBM once per step with
-// coalesced loads.  Along x the stencil samples
-// live in per-thread register queues; along z they come from shared-memory
-// ring buffers holding the last few rows.  Everything a step reads from
-// shared memory was written at an earlier row, so one barrier per row
-// suffices.  The arithmetic per cell is the same single-precision sequence
-// as the tile kernel's (src/cpp/we_op.cpp:667-871 elastic, :1640-1840 VTI);
-// z-boundary cells use the closure forms of sbp.cuh on the ring rows.
+// One CTA owns a strip of z (a window of NTH cells, one per thread) and
+// marches along x over a run of rows [xb, xe).  Units own cells of
+// 6 <= z < nz-6 only, where every stencil takes its interior form, so the
+// kernel carries no closure code and its warps stay in step; the boundary
+// frame (x or z within 6 cells of an edge) is computed by the tile kernel.  Rows are contiguous in memory
+// (z fastest).  Every row a step needs is fetched one step ahead by 1-D bulk
+// copies (cp.async.bulk, no multicast) into shared-memory rings, completion
+// tracked by a two-stage mbarrier pipeline, so HBM latency overlaps a whole
+// row of arithmetic and no register staging is needed.  Along x the stencil
+// samples live in per-thread register queues filled from the rings; along z
+// they are read from the rings directly.  Everything a step reads from shared
+// memory was written at an earlier step, so one barrier per row suffices.
+// The arithmetic per cell is the same single-precision sequence as the tile
+// kernel's (src/cpp/we_op.cpp:667-871 elastic, :1640-1840 VTI); z-boundary
+// cells use the closure forms of sbp.cuh on the ring rows.
 //
-// Row schedule of step j (output row j):
-//   loads       curr row j+5, coefficient and snapshot rows j+3, prev / rho
-//               of row j+1 (held in registers until the end of the step, or
-//               the next step, so that their latency overlaps the arithmetic);
-//   derivatives ux_x, uz_z, ux_z and T0 / T1 of row j+2, uz_x of row j+1
-//               (from rows loaded at earlier steps);
+// Step j (output row j), after the barrier:
+//   issue       bulk copies of curr row j+6, coefficient and snapshot rows
+//               j+4, and the own-cell rows of row j+1 (prev, rho, gradient,
+//               neighbouring snapshots) plus its row record;
+//   derivatives ux_x, uz_z, ux_z and T0 / T1 of row j+2, uz_x of row j+1;
 //   output      row j: SBP terms, sources, SAT (z edges), leapfrog, taper,
 //               receivers, snapshot store or imaging condition;
-//   queues      the rows loaded at this step enter the queues and rings.
-// The first output row is preceded by 9 steps that only fill the queues.
+//   queues      curr row j+5 and coefficient / snapshot rows j+3 (copied at
+//               step j-1) enter the register queues.
+// The first output row is preceded by 10 steps that only fill the pipeline.
+// The step body is unrolled over the 8 ring phases, so that register-queue
+// and ring slots are compile-time constants and nothing moves between steps.
 //
-// Shared-memory rings (RW = NTH + 4 floats per row, cell z at index z - za + 2):
-//   ux, uz         8 rows (curr, with a 2-cell z halo on each side); register
-//                  queues of 8 rows (j-2 .. j+5)
-//   mu             4 rows
-//   q              4 rows: lambda (isotropic) or T1 (VTI)
-//   t              4 rows: T0 = ux_x + uz_z (isotropic only)
-//   bx             4 rows: uz_x
-//   f0, f1         4 rows: forward snapshot (imaging condition only)
+// Shared memory, rows of RB = NTH + 24 floats; cell z of a row buffer sits
+// at index z - s0 with s0 = (za - 2) rounded down to a multiple of 8, so that
+// every copy starts and ends on a 16-byte boundary (and 16-bit snapshot rows
+// on 16-byte boundaries too):
+//   ux, uz, mu, q, f0, f1   8-row rings (q: lambda, or (1+2eps)(lambda+2mu) for VTI)
+//   t, bx                   4-row rings of T0 (VTI: T1) and uz_x
+//   vl, vc, va              4-row rings of the VTI coefficients lbis, c13, lambda
+//   own[2][..]              per step: prev, rho, gradient, snapshot rows of row j+1
 #pragma once
 
 namespace fwi2d {
 
+// Set (to the row where it happened + 1) when a bounded wait of the marching
+// kernel gives up; read and cleared by the host after each run.
+__device__ int g_march_timeout;
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// 1-D bulk copy global -> shared of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_row(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for a phase of an mbarrier; false when the limit was reached.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+    for (int k = 0; k < (1 << 20); k++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+template <bool VTI, bool GRAD, int NTH>
+struct MarchLayout {
+    static constexpr int RB = NTH + 24;
+    static constexpr int UX = 0, UZ = UX + 8 * RB, MU = UZ + 8 * RB, Q = MU + 8 * RB;
+    static constexpr int F0 = Q + 8 * RB, F1 = F0 + (GRAD ? 8 : 0) * RB;
+    static constexpr int T = F1 + (GRAD ? 8 : 0) * RB, BX = T + 4 * RB;
+    static constexpr int VL = BX + 4 * RB, VC = VL + (VTI ? 4 : 0) * RB, VA = VC + (VTI ? 4 : 0) * RB;
+    // own-cell rows of one step: prev ux, prev uz, rho, g0, g1, g2, fp0, fp1, fm0, fm1, eps, v2, v3
+    static constexpr int NOWN = 3 + (GRAD ? 7 : 0) + (VTI && GRAD ? 3 : 0);
+    static constexpr int OWN = VA + (VTI ? 4 : 0) * RB;
+    static constexpr int ROWREC = OWN + 2 * NOWN * RB;    // 2 x 8 ints
+    static constexpr int RED = ROWREC + 16;
+    static constexpr int MBAR = RED + 32;                 // 2 x u64, 8-byte aligned (MBAR even)
+    static constexpr int FLOATS = MBAR + 4;
+    static_assert(RB % 8 == 0, "row buffers must keep 32-byte alignment");
+    static_assert(MBAR % 2 == 0, "mbarrier alignment");
+};
+
+enum OwnRow { O_PV0 = 0, O_PV1, O_RHO, O_G0, O_G1, O_G2, O_FP0, O_FP1, O_FM0, O_FM1, O_EPS, O_V2, O_V3 };
 
 // Per-thread state that stays fixed during one launch.
 struct MarchCtx {
     float *u;                 // curr base (component stride nxz); prev/next at u + pn_off
     long long pn_off;
-    long long mofs;           // model offset of the shot's first column + this thread's z
+    long long mofs;           // model offset of the shot's first column
     int ldz, mld, nx, nz, nxz;
-    int xb, xe, z, li;
-    bool zin, zb4, zb6, own;
-    bool hlo, hhi;            // thread loads the low / high 2-cell z halo of curr
-    int hz;                   // first halo cell (hlo: za-2, hhi: za+NTH)
+    int xb, xe, z, li, s0, s0c, s1c;
+    bool zin, own;
     float tzv;
-    bool extract, store, do_grad;
+    bool extract, store, do_grad, has_fp, has_fm;
     int it, itf, last, prec, slot;
     float sc, finv, finvp, finvm, dtg, gw;
     double wdt, wh;
     int roff, zw0, zw1;
     float amax;
+    const float *srcrow;      // this time sample's injection row
+    void *snap;
+    long long slot_elems;
+    float *grad;
+    unsigned ph[2];           // mbarrier phase parity per stage
 };
 
 template <bool GRAD>
 struct MarchQ {
     float ux[8], uz[8], mu[8], q[8], t0[8], cz[8];
     float ax[8], az[8], bx[8], f0[8], f1[8];
-    float pv0[2], pv1[2], rh[2];
-    float vlb[2], vc13[2], vlam[2];   // VTI coefficients of the next derivative row
 };
 
-template <bool VTI, bool GRAD, int NTH>
-struct MarchLayout {
-    static constexpr int RW = NTH + 4;
-    static constexpr int UX = 0, UZ = 8 * RW, MU = 16 * RW, Q = 20 * RW, T = 24 * RW;
-    static constexpr int BX = T + (VTI ? 0 : 4 * RW);
-    static constexpr int F0 = BX + 4 * RW, F1 = F0 + (GRAD ? 4 * RW : 0);
-    static constexpr int RED = F1 + (GRAD ? 4 * RW : 0);
-    static constexpr int FLOATS = RED + 32;
-};
-
-__device__ __forceinline__ float ldz_pred(const float *p, bool ok) { return ok ? *p : 0.f; }
+// sample of a snapshot row buffer (fp32, or 16-bit scaled by inv)
+__device__ __forceinline__ float srow(const float *buf, int idx, int prec, float inv)
+{
+    if (prec == SNAP_FP32) return buf[idx];
+    if (prec == SNAP_BF16) return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(buf)[idx]) * inv;
+    return __half2float(reinterpret_cast<const __half *>(buf)[idx]) * inv;
+}
 
 __device__ __forceinline__ void add_sources(const InjEntry *__restrict__ inj, const float *__restrict__ srcrow, int e0,
                                             int e1, int gz, float &n0, float &n1)
@@ -88,125 +155,171 @@ __device__ __forceinline__ void add_sources(const InjEntry *__restrict__ inj, co
     }
 }
 
-template <bool VTI, bool GRAD, int NTH, int P>
-__device__ __forceinline__ void march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *sm, const ShotDev *__restrict__ Sp,
-                                           const ModelDev &M, const StepConst &C, int j)
+// Bulk copies issued at step j (by thread 0) for consumption at step j+1.
+template <bool VTI, bool GRAD, int NTH>
+__device__ __forceinline__ void march_issue(const MarchCtx &X, float *sm, const ShotDev &S, const ModelDev &M, int j,
+                                            int P)
 {
     using L = MarchLayout<VTI, GRAD, NTH>;
-    constexpr int RW = L::RW;
-    constexpr int S0 = P & 7, SM1 = (P + 7) & 7, SM2 = (P + 6) & 7, SP1 = (P + 1) & 7, SP2 = (P + 2) & 7,
-                  SP3 = (P + 3) & 7, SP4 = (P + 4) & 7, SP5 = (P + 5) & 7;
-    constexpr int R0 = P & 3, RP1 = (P + 1) & 3, RP2 = (P + 2) & 3, RP3 = (P + 3) & 3;
-    const int li = X.li;
-    const float *cur = X.u;
-
-    __syncthreads();
-
-    // ---- loads: curr row j+5 (+ z halo), coefficient and snapshot rows j+3, prev/rho of row j+1
-    const long long c4 = (long long)(j + 5) * X.ldz;
-    const float nux = ldz_pred(cur + c4 + X.z, X.zin);
-    const float nuz = ldz_pred(cur + X.nxz + c4 + X.z, X.zin);
-    float h0a = 0.f, h0b = 0.f, h1a = 0.f, h1b = 0.f;
-    if (X.hlo || X.hhi) {
-        const bool ia = X.hz >= 0 && X.hz < X.nz, ib = X.hz + 1 >= 0 && X.hz + 1 < X.nz;
-        h0a = ldz_pred(cur + c4 + X.hz, ia);
-        h0b = ldz_pred(cur + c4 + X.hz + 1, ib);
-        h1a = ldz_pred(cur + X.nxz + c4 + X.hz, ia);
-        h1b = ldz_pred(cur + X.nxz + c4 + X.hz + 1, ib);
-    }
-    const long long m2 = X.mofs + (long long)(j + 3) * X.mld;
-    const float nmu = ldz_pred(M.p1 + m2, X.zin);
-    const float nq = ldz_pred((VTI ? M.fxx : M.p0) + m2, X.zin);
-    float nlb = 0.f, nc13 = 0.f, nlam = 0.f;
-    if (VTI) {
-        nlb = ldz_pred(M.lbis + m2, X.zin);
-        nc13 = ldz_pred(M.c13 + m2, X.zin);
-        nlam = ldz_pred(M.p0 + m2, X.zin);
-    }
-    float nf0 = 0.f, nf1 = 0.f;
-    if (GRAD && X.do_grad && X.zin) {
-        const long long so = (long long)X.itf * Sp->snap_slot + (long long)(j + 3) * X.ldz + X.z;
-        nf0 = snap_load(Sp->snap, so, X.prec, X.finv);
-        nf1 = snap_load(Sp->snap, so + X.nxz, X.prec, X.finv);
-    }
-    if (j + 1 >= X.xb && j + 1 < X.xe) {
-        const float *pn = X.u + X.pn_off;
-        const long long o1 = (long long)(j + 1) * X.ldz + X.z;
-        Q.pv0[(P + 1) & 1] = ldz_pred(pn + o1, X.zin);
-        Q.pv1[(P + 1) & 1] = ldz_pred(pn + X.nxz + o1, X.zin);
-        Q.rh[(P + 1) & 1] = ldz_pred(M.p2 + X.mofs + (long long)(j + 1) * X.mld, X.zin);
-    }
-
-    // ---- derivatives of row j+2 (its curr ring row was written three steps ago)
-    {
-        const float *ux2 = sm + L::UX + SP2 * RW + li, *uz2 = sm + L::UZ + SP2 * RW + li;
-        const float uxx = d1s(Q.ux[S0], Q.ux[SP1], Q.ux[SP3], Q.ux[SP4], C.sdx);
-        float uzz, czz;
-        if (!X.zb4) {
-            uzz = d1s(uz2[-2], uz2[-1], uz2[1], uz2[2], C.sdz);
-            czz = d1s(ux2[-2], ux2[-1], ux2[1], ux2[2], C.sdz);
-        } else if (X.zin) {
-            uzz = d1(uz2, 1, X.z, X.nz, C.dz, C.sdz);
-            czz = d1(ux2, 1, X.z, X.nz, C.dz, C.sdz);
-        } else {
-            uzz = czz = 0.f;
+    constexpr int RB = L::RB;
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + L::MBAR) + ((P + 1) & 1);
+    const int n = X.s1c - X.s0c, dofs = X.s0c - X.s0;
+    const unsigned nf = 4u * n, nh = (X.prec == SNAP_FP32 ? 4u : 2u) * n;
+    const bool own_next = j + 1 >= X.xb;
+    unsigned bytes = 2 * nf + (VTI ? 5 : 2) * nf;
+    if (GRAD && X.do_grad) bytes += 2 * nh;
+    if (own_next) {
+        bytes += 3 * nf + 32;
+        if (GRAD && X.do_grad) {
+            bytes += 3 * nf + (X.has_fp ? 2 * nh : 0) + (X.has_fm ? 2 * nh : 0);
+            if (VTI) bytes += 3 * nf;
         }
+    }
+    mbar_expect_tx(bar, bytes);
+    // curr row j+6
+    const long long c6 = (long long)(j + 6) * X.ldz + X.s0c;
+    bulk_row(sm + L::UX + ((P + 6) & 7) * RB + dofs, X.u + c6, nf, bar);
+    bulk_row(sm + L::UZ + ((P + 6) & 7) * RB + dofs, X.u + X.nxz + c6, nf, bar);
+    // coefficient rows j+4
+    const long long m4 = X.mofs + (long long)(j + 4) * X.mld + X.s0c;
+    bulk_row(sm + L::MU + ((P + 4) & 7) * RB + dofs, M.p1 + m4, nf, bar);
+    bulk_row(sm + L::Q + ((P + 4) & 7) * RB + dofs, (VTI ? M.fxx : M.p0) + m4, nf, bar);
+    if (VTI) {
+        bulk_row(sm + L::VL + ((P + 4) & 3) * RB + dofs, M.lbis + m4, nf, bar);
+        bulk_row(sm + L::VC + ((P + 4) & 3) * RB + dofs, M.c13 + m4, nf, bar);
+        bulk_row(sm + L::VA + ((P + 4) & 3) * RB + dofs, M.p0 + m4, nf, bar);
+    }
+    const int esz = X.prec == SNAP_FP32 ? 4 : 2;
+    const char *snap = (const char *)S.snap;
+    if (GRAD && X.do_grad) {
+        const long long so = (long long)X.itf * S.snap_slot + (long long)(j + 4) * X.ldz + X.s0c;
+        bulk_row((char *)(sm + L::F0 + ((P + 4) & 7) * RB) + dofs * esz, snap + so * esz, nh, bar);
+        bulk_row((char *)(sm + L::F1 + ((P + 4) & 7) * RB) + dofs * esz, snap + (so + X.nxz) * esz, nh, bar);
+    }
+    if (own_next) {
+        float *own = sm + L::OWN + ((P + 1) & 1) * L::NOWN * RB;
+        const long long o1 = (long long)(j + 1) * X.ldz + X.s0c;
+        const float *pn = X.u + X.pn_off;
+        bulk_row(own + O_PV0 * RB + dofs, pn + o1, nf, bar);
+        bulk_row(own + O_PV1 * RB + dofs, pn + X.nxz + o1, nf, bar);
+        const long long m1 = X.mofs + (long long)(j + 1) * X.mld + X.s0c;
+        bulk_row(own + O_RHO * RB + dofs, M.p2 + m1, nf, bar);
+        bulk_row(sm + L::ROWREC + ((P + 1) & 1) * 8, S.mrow + X.roff + (j + 1 - X.xb), 32, bar);
+        if (GRAD && X.do_grad) {
+            bulk_row(own + O_G0 * RB + dofs, S.grad + o1, nf, bar);
+            bulk_row(own + O_G1 * RB + dofs, S.grad + X.nxz + o1, nf, bar);
+            bulk_row(own + O_G2 * RB + dofs, S.grad + 2 * (long long)X.nxz + o1, nf, bar);
+            if (X.has_fp) {
+                const long long o = (long long)(X.itf + 1) * S.snap_slot + o1;
+                bulk_row((char *)(own + O_FP0 * RB) + dofs * esz, snap + o * esz, nh, bar);
+                bulk_row((char *)(own + O_FP1 * RB) + dofs * esz, snap + (o + X.nxz) * esz, nh, bar);
+            }
+            if (X.has_fm) {
+                const long long o = (long long)(X.itf - 1) * S.snap_slot + o1;
+                bulk_row((char *)(own + O_FM0 * RB) + dofs * esz, snap + o * esz, nh, bar);
+                bulk_row((char *)(own + O_FM1 * RB) + dofs * esz, snap + (o + X.nxz) * esz, nh, bar);
+            }
+            if (VTI) {
+                bulk_row(own + O_EPS * RB + dofs, M.eps + m1, nf, bar);
+                bulk_row(own + O_V2 * RB + dofs, M.gv2 + m1, nf, bar);
+                bulk_row(own + O_V3 * RB + dofs, M.gv3 + m1, nf, bar);
+            }
+        }
+    }
+}
+
+// Returns false when the CTA must stop (a bounded wait gave up).
+// Register queues of 8 rows: row j+d sits at index (PH + d) & 7.
+
+template <bool VTI, bool GRAD, int NTH, int PH>
+__device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *sm, const ShotDev &S,
+                                           const ModelDev &M, const StepConst &C, int j, int j0)
+{
+    using L = MarchLayout<VTI, GRAD, NTH>;
+    constexpr int RB = L::RB;
+    constexpr int P = PH;
+    constexpr int QM2 = (PH + 6) & 7, QM1 = (PH + 7) & 7, Q00 = PH, QP1 = (PH + 1) & 7, QP2 = (PH + 2) & 7,
+                  QP3 = (PH + 3) & 7, QP4 = (PH + 4) & 7;
+    // register-queue slots of the rows arriving at the end of this step
+    constexpr int QN5 = (PH + 5) & 7, QN3 = (PH + 3) & 7;
+    // ring slots of rows j+d (8-row rings) and (4-row rings)
+    constexpr int S0 = P, SP2 = (P + 2) & 7, SP3 = (P + 3) & 7, SP5 = (P + 5) & 7;
+    constexpr int R0 = P & 3, RP1 = (P + 1) & 3, RP2 = (P + 2) & 3;
+    const int li = X.li;
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(sm + L::MBAR);
+
+    // ---- wait for the copies issued at the previous step, then the step barrier
+    bool tmo = false;
+    if (j > j0) {
+        tmo = !mbar_wait(bars + (P & 1), X.ph[P & 1]);
+        X.ph[P & 1] ^= 1u;
+    }
+    if (__syncthreads_or(tmo)) {
+        if (threadIdx.x == 0) atomicCAS(&g_march_timeout, 0, j + 1);
+        return false;
+    }
+    if (threadIdx.x == 0 && j + 1 < X.xe) march_issue<VTI, GRAD, NTH>(X, sm, S, M, j, P);
+
+    // ---- derivatives of row j+2 (its curr ring row arrived three steps ago)
+    {
+        const float *ux2 = sm + L::UX + SP2 * RB + li, *uz2 = sm + L::UZ + SP2 * RB + li;
+        const float uxx = d1s(Q.ux[Q00], Q.ux[QP1], Q.ux[QP3], Q.ux[QP4], C.sdx);
+        const float uzz = d1s(uz2[-2], uz2[-1], uz2[1], uz2[2], C.sdz);
+        const float czz = d1s(ux2[-2], ux2[-1], ux2[1], ux2[2], C.sdz);
         float t0;
         if (!VTI) {
             t0 = uxx + uzz;
-            sm[L::T + RP2 * RW + li] = t0;
+            sm[L::T + RP2 * RB + li] = t0;
         } else {
-            const float vlb = Q.vlb[P & 1], vc13 = Q.vc13[P & 1], vlam = Q.vlam[P & 1];
+            const float vlb = sm[L::VL + RP2 * RB + li], vc13 = sm[L::VC + RP2 * RB + li];
+            const float vlam = sm[L::VA + RP2 * RB + li];
             t0 = vlb * uxx + vc13 * uzz;
-            sm[L::Q + RP2 * RW + li] = vlam * uzz + vc13 * uxx;
+            sm[L::T + RP2 * RB + li] = vlam * uzz + vc13 * uxx;
         }
-        Q.t0[SP2] = t0;
-        Q.cz[SP2] = czz;
+        Q.t0[QP2] = t0;
+        Q.cz[QP2] = czz;
         if (GRAD) {
-            Q.ax[SP2] = uxx;
-            Q.az[SP2] = uzz;
+            Q.ax[QP2] = uxx;
+            Q.az[QP2] = uzz;
         }
     }
     // uz_x of row j+1 from rows j-1 .. j+3
     {
-        const float bx = d1s(Q.uz[SM1], Q.uz[S0], Q.uz[SP2], Q.uz[SP3], C.sdx);
-        sm[L::BX + RP1 * RW + li] = bx;
-        if (GRAD) Q.bx[SP1] = bx;
+        const float bx = d1s(Q.uz[QM1], Q.uz[Q00], Q.uz[QP2], Q.uz[QP3], C.sdx);
+        sm[L::BX + RP1 * RB + li] = bx;
+        if (GRAD) Q.bx[QP1] = bx;
     }
 
     // ---- output row j
     if (j >= X.xb) {
-        const float *ruxj = sm + L::UX + S0 * RW + li, *ruzj = sm + L::UZ + S0 * RW + li;
-        const float *rmuj = sm + L::MU + R0 * RW + li, *rqj = sm + L::Q + R0 * RW + li;
-        const float *rtj = sm + L::T + R0 * RW + li, *rbxj = sm + L::BX + R0 * RW + li;
-        const float am2 = Q.ux[SM2], am1 = Q.ux[SM1], a00 = Q.ux[S0], ap1 = Q.ux[SP1], ap2 = Q.ux[SP2];
-        const float bm2 = Q.uz[SM2], bm1 = Q.uz[SM1], b00 = Q.uz[S0], bp1 = Q.uz[SP1], bp2 = Q.uz[SP2];
-        const float mm2 = Q.mu[SM2], mm1 = Q.mu[SM1], m00 = Q.mu[S0], mp1 = Q.mu[SP1], mp2 = Q.mu[SP2];
-        const float qm2 = Q.q[SM2], qm1 = Q.q[SM1], q00 = Q.q[S0], qp1 = Q.q[SP1], qp2 = Q.q[SP2];
-        const float tm2 = Q.t0[SM2], tm1 = Q.t0[SM1], tp1 = Q.t0[SP1], tp2 = Q.t0[SP2];
-        const float cm2 = Q.cz[SM2], cm1 = Q.cz[SM1], cp1 = Q.cz[SP1], cp2 = Q.cz[SP2];
-        const float txv = Sp->tx[j];
+        const float *ruxj = sm + L::UX + S0 * RB + li, *ruzj = sm + L::UZ + S0 * RB + li;
+        const float *rmuj = sm + L::MU + S0 * RB + li, *rqj = sm + L::Q + S0 * RB + li;
+        const float *rtj = sm + L::T + R0 * RB + li, *rbxj = sm + L::BX + R0 * RB + li;
+        const float *own = sm + L::OWN + (P & 1) * L::NOWN * RB + li;
+        const MarchRow R = *reinterpret_cast<const MarchRow *>(sm + L::ROWREC + (P & 1) * 8);
+        const float am2 = Q.ux[QM2], am1 = Q.ux[QM1], a00 = Q.ux[Q00], ap1 = Q.ux[QP1], ap2 = Q.ux[QP2];
+        const float bm2 = Q.uz[QM2], bm1 = Q.uz[QM1], b00 = Q.uz[Q00], bp1 = Q.uz[QP1], bp2 = Q.uz[QP2];
+        const float mm2 = Q.mu[QM2], mm1 = Q.mu[QM1], m00 = Q.mu[Q00], mp1 = Q.mu[QP1], mp2 = Q.mu[QP2];
+        const float qm2 = Q.q[QM2], qm1 = Q.q[QM1], q00 = Q.q[Q00], qp1 = Q.q[QP1], qp2 = Q.q[QP2];
+        const float tm2 = Q.t0[QM2], tm1 = Q.t0[QM1], tp1 = Q.t0[QP1], tp2 = Q.t0[QP2];
+        const float cm2 = Q.cz[QM2], cm1 = Q.cz[QM1], cp1 = Q.cz[QP1], cp2 = Q.cz[QP2];
+        const float txv = R.tx;
         const long long cell = (long long)j * X.ldz + X.z;
         const int gz = X.z;
-
-        // sources of this row (entries sorted by z); warps clear of them skip
-        const int *inj_roff = Sp->inj_roff;
-        const int e0 = inj_roff[X.roff + j - X.xb], e1 = inj_roff[X.roff + j - X.xb + 1];
-        bool src_here = false;
-        if (e0 < e1) src_here = Sp->inj[e0].gz < X.zw1 && Sp->inj[e1 - 1].gz >= X.zw0;
-        const float *srcrow = Sp->src + (long long)X.it * Sp->nsrc;
+        const bool src_here = R.e0 < R.e1 && R.zlo < X.zw1 && R.zhi >= X.zw0;
+        const float *srcrow = X.srcrow;
 
         const Brk bkx = brk5(mm2, mm1, m00, mp1, mp2);
         float n0, n1;
         if (!VTI) n0 = d2s(0.f, twice(bkx), am2, am1, a00, ap1, ap2, C.inv_d2x);
         else n0 = d2s(0.f, brk5(qm2, qm1, q00, qp1, qp2), am2, am1, a00, ap1, ap2, C.inv_d2x);
-        float p0 = Q.pv0[P & 1], p1 = Q.pv1[P & 1];
-        const float rho = Q.rh[P & 1];
+        float p0 = own[O_PV0 * RB], p1 = own[O_PV1 * RB];
+        const float rho = own[O_RHO * RB];
         if (X.it > 0) {
             p0 = p0 * X.tzv * txv;
             p1 = p1 * X.tzv * txv;
         }
-        if (!X.zb6) {
+        {
             const float mzm2 = rmuj[-2], mzm1 = rmuj[-1], mzp1 = rmuj[1], mzp2 = rmuj[2];
             const Brk bkz = brk5(mzm2, mzm1, m00, mzp1, mzp2);
             n1 = d2s(0.f, twice(bkz), ruzj[-2], ruzj[-1], b00, ruzj[1], ruzj[2], C.inv_d2z);
@@ -217,67 +330,13 @@ __device__ __forceinline__ void march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
                 n1 += md1s(rtj[-2], rqj[-2], rtj[-1], rqj[-1], rtj[1], rqj[1], rtj[2], rqj[2], C.adz);
             } else {
                 n0 += d1s(tm2, tm1, tp1, tp2, C.sdx);
-                n1 += d1s(rqj[-2], rqj[-1], rqj[1], rqj[2], C.sdz);
+                n1 += d1s(rtj[-2], rtj[-1], rtj[1], rtj[2], C.sdz);
             }
             n1 += md1s(cm2, mm2, cm1, mm1, cp1, mp1, cp2, mp2, C.adx);
             n0 += md1s(rbxj[-2], mzm2, rbxj[-1], mzm1, rbxj[1], mzp1, rbxj[2], mzp2, C.adz);
-            if (src_here) add_sources(Sp->inj, srcrow, e0, e1, gz, n0, n1);
+            if (src_here) add_sources(S.inj, srcrow, R.e0, R.e1, gz, n0, n1);
             n0 = C.dt2 * n0 / rho + 2 * a00 - p0;
             n1 = C.dt2 * n1 / rho + 2 * b00 - p1;
-        } else if (X.own) {
-            n1 = 0.f;
-            d2acc(n1, ruzj, 1, rmuj, 1, 2.f, gz, X.nz, C.inv_d2z, C.d2z);
-            n1 = d2s(n1, bkx, bm2, bm1, b00, bp1, bp2, C.inv_d2x);
-            d2acc(n0, ruxj, 1, rmuj, 1, 1.f, gz, X.nz, C.inv_d2z, C.d2z);
-            if (!VTI) {
-                n0 += md1s(tm2, qm2, tm1, qm1, tp1, qp1, tp2, qp2, C.adx);
-                n1 += md1(rtj, rqj, 1, gz, X.nz, C.adz);
-            } else {
-                n0 += d1s(tm2, tm1, tp1, tp2, C.sdx);
-                n1 += d1(rqj, 1, gz, X.nz, C.dz, C.sdz);
-            }
-            n1 += md1s(cm2, mm2, cm1, mm1, cp1, mp1, cp2, mp2, C.adx);
-            n0 += md1(rbxj, rmuj, 1, gz, X.nz, C.adz);
-            if (src_here) add_sources(Sp->inj, srcrow, e0, e1, gz, n0, n1);
-            const bool top = gz == 0, bot = gz == X.nz - 1;
-            const int bc = top ? C.bc[0] : C.bc[1];
-            if ((top || bot) && (bc == 1 || bc == 2)) {
-                // esat_neumann / esat_absorbing top or bottom (spatial_operators.hpp:160-727) and
-                // esat_Dz (:732-776); x is interior here, so the tangential sums take the interior form
-                const float mu = m00;
-                const long long mcell = X.mofs + (long long)j * X.mld;
-                const float lam = VTI ? M.p0[mcell] : q00;
-                const float c13 = VTI ? M.c13[mcell] : lam;
-                const float imp_s = 0.5f * sqrtf(mu * rho);
-                const float imp_p = 0.5f * sqrtf((lam + 2 * mu) * rho);
-                const int in = top ? 1 : -1;
-                const float sg = top ? -1.f : 1.f;
-                float tsz = 0.f, tsx = 0.f;
-                tsz += kC1[0] * (bp1 - bm1);
-                tsz += kC1[1] * (bp2 - bm2);
-                tsx += kC1[0] * (ap1 - am1);
-                tsx += kC1[1] * (ap2 - am2);
-                {
-                    float t = (sg * mu) * tsz / C.dx + mu * nsum(ruxj, in) / C.dz;
-                    if (bc == 2) t = t - imp_s * p0 / C.dt;
-                    n0 = n0 - C.sat_z * t;
-                }
-                {
-                    float t = (sg * c13) * tsx / C.dx + (2 * mu) * nsum(ruzj, in) / C.dz;
-                    if (bc == 2) t = t - imp_p * p1 / C.dt;
-                    n1 = n1 - C.sat_z * t;
-                    n1 = n1 - C.nsat_z * lam * ndsum(ruzj, in);
-                }
-            }
-            n0 = C.dt2 * n0 / rho + 2 * a00 - p0;
-            n1 = C.dt2 * n1 / rho + 2 * b00 - p1;
-            if (top || bot) {
-                const int k = top ? j : X.nx + j;
-                n0 = n0 / Sp->den[k];
-                n1 = n1 / Sp->den[2 * X.nx + 2 * X.nz + k];
-            }
-        } else {
-            n0 = n1 = 0.f;
         }
         n0 = n0 * X.tzv * txv;
         n1 = n1 * X.tzv * txv;
@@ -287,58 +346,56 @@ __device__ __forceinline__ void march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
             pn[X.nxz + cell] = n1;
             X.amax = fmaxf(X.amax, fmaxf(fabsf(n0), fabsf(n1)));
             if (X.store) {
-                const long long o = (long long)X.slot * Sp->snap_slot + cell;
-                snap_store(Sp->snap, o, X.prec, a00, X.sc);
-                snap_store(Sp->snap, o + X.nxz, X.prec, b00, X.sc);
+                const long long o = (long long)X.slot * X.slot_elems + cell;
+                snap_store(X.snap, o, X.prec, a00, X.sc);
+                snap_store(X.snap, o + X.nxz, X.prec, b00, X.sc);
             }
         }
 
         // receivers whose pivot lies on this row: curr rows j-1 .. j+1 are in the rings
         if (X.extract) {
-            const int r0 = Sp->ext_roff[X.roff + j - X.xb], r1 = Sp->ext_roff[X.roff + j - X.xb + 1];
-            for (int e = r0 + (int)threadIdx.x; e < r1; e += NTH) {
-                const ExtEntry &E = Sp->ext[e];
+            for (int e = R.r0 + (int)threadIdx.x; e < R.r1; e += NTH) {
+                const ExtEntry &E = S.ext[e];
                 const float *Rb = sm + (E.comp == 0 ? L::UX : L::UZ);
-                const int zi = E.gz0 - (X.z - li);
+                const int zi = E.gz0 - X.s0;
                 float o = 0.f;
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
-                    const float *row = Rb + ((P + 7 + a) & 7) * RW + zi;
+                    const float *row = Rb + ((P + 7 + a) & 7) * RB + zi;
 #pragma unroll
                     for (int b = 0; b < 3; b++) o += E.w[a * 3 + b] * row[b];
                 }
-                Sp->rcv[(long long)X.it * Sp->nrcv + E.row] = o;
+                S.rcv[(long long)X.it * S.nrcv + E.row] = o;
             }
         }
 
         // zero-lag imaging condition (we_op.cpp:505-562, VTI :1478-1557)
         if (GRAD && X.do_grad && X.own) {
-            const float *rf0 = sm + L::F0 + R0 * RW + li, *rf1 = sm + L::F1 + R0 * RW + li;
+            const float *rf0 = sm + L::F0 + S0 * RB, *rf1 = sm + L::F1 + S0 * RB;
             float fp0 = 0.f, fp1 = 0.f, fm0 = 0.f, fm1 = 0.f;
-            if (X.itf + 1 <= X.last) {
-                const long long o = (long long)(X.itf + 1) * Sp->snap_slot + cell;
-                fp0 = snap_load(Sp->snap, o, X.prec, X.finvp);
-                fp1 = snap_load(Sp->snap, o + X.nxz, X.prec, X.finvp);
+            if (X.has_fp) {
+                fp0 = srow(own - li + O_FP0 * RB, li, X.prec, X.finvp);
+                fp1 = srow(own - li + O_FP1 * RB, li, X.prec, X.finvp);
             }
-            if (X.itf > 0) {
-                const long long o = (long long)(X.itf - 1) * Sp->snap_slot + cell;
-                fm0 = snap_load(Sp->snap, o, X.prec, X.finvm);
-                fm1 = snap_load(Sp->snap, o + X.nxz, X.prec, X.finvm);
+            if (X.has_fm) {
+                fm0 = srow(own - li + O_FM0 * RB, li, X.prec, X.finvm);
+                fm1 = srow(own - li + O_FM1 * RB, li, X.prec, X.finvm);
             }
-            float *g0 = Sp->grad + cell, *g1 = g0 + X.nxz, *g2 = g1 + X.nxz;
-            float g0v = *g0, g1v = *g1, g2v = *g2;
-            const float ax0 = Q.ax[S0], az1 = Q.az[S0], az0 = Q.cz[S0], ax1 = Q.bx[S0];
-            const float t0 = d1s(Q.f0[SM2], Q.f0[SM1], Q.f0[SP1], Q.f0[SP2], C.sdx);
-            const float t2 = d1s(Q.f1[SM2], Q.f1[SM1], Q.f1[SP1], Q.f1[SP2], C.sdx);
+            float g0v = own[O_G0 * RB], g1v = own[O_G1 * RB], g2v = own[O_G2 * RB];
+            const float ax0 = Q.ax[Q00], az1 = Q.az[Q00], az0 = Q.cz[Q00], ax1 = Q.bx[Q00];
+            const float t0 = d1s(Q.f0[QM2], Q.f0[QM1], Q.f0[QP1], Q.f0[QP2], C.sdx);
+            const float t2 = d1s(Q.f1[QM2], Q.f1[QM1], Q.f1[QP1], Q.f1[QP2], C.sdx);
             float t1, t3;
-            if (!X.zb6) {
-                t1 = d1s(rf1[-2], rf1[-1], rf1[1], rf1[2], C.sdz);
-                t3 = d1s(rf0[-2], rf0[-1], rf0[1], rf0[2], C.sdz);
+            if (X.prec == SNAP_FP32) {
+                t1 = d1s(rf1[li - 2], rf1[li - 1], rf1[li + 1], rf1[li + 2], C.sdz);
+                t3 = d1s(rf0[li - 2], rf0[li - 1], rf0[li + 1], rf0[li + 2], C.sdz);
             } else {
-                t1 = d1(rf1, 1, gz, X.nz, C.dz, C.sdz);
-                t3 = d1(rf0, 1, gz, X.nz, C.dz, C.sdz);
+                t1 = d1s(srow(rf1, li - 2, X.prec, X.finv), srow(rf1, li - 1, X.prec, X.finv),
+                         srow(rf1, li + 1, X.prec, X.finv), srow(rf1, li + 2, X.prec, X.finv), C.sdz);
+                t3 = d1s(srow(rf0, li - 2, X.prec, X.finv), srow(rf0, li - 1, X.prec, X.finv),
+                         srow(rf0, li + 1, X.prec, X.finv), srow(rf0, li + 2, X.prec, X.finv), C.sdz);
             }
-            const float f0 = Q.f0[S0], f1 = Q.f1[S0];
+            const float f0 = Q.f0[Q00], f1 = Q.f1[Q00];
             const float a0 = n0, a1 = n1;
             const float gw = X.gw, dtg = X.dtg;
             float dl, dm;
@@ -346,9 +403,8 @@ __device__ __forceinline__ void march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
                 dl = 0.f;
                 dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
             } else {
-                const long long mo = X.mofs + (long long)j * X.mld;
-                const float e2 = 1 + 2 * M.eps[mo];
-                const float v2 = M.gv2[mo], v3 = M.gv3[mo];
+                const float e2 = 1 + 2 * own[O_EPS * RB];
+                const float v2 = own[O_V2 * RB], v3 = own[O_V3 * RB];
                 dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
                 dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
             }
@@ -368,39 +424,26 @@ __device__ __forceinline__ void march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
                 g1v = g1v + gw * dtg * dm;
                 g2v = (float)((double)g2v + X.wdt * (double)(a0 * (-f0 + fm0) + a1 * (-f1 + fm1)));
             }
-            *g0 = g0v;
-            *g1 = g1v;
-            *g2 = g2v;
+            float *g0 = X.grad + cell;
+            g0[0] = g0v;
+            g0[X.nxz] = g1v;
+            g0[2 * (long long)X.nxz] = g2v;
         }
     }
 
-    // ---- queues and rings: curr row j+5, coefficient and snapshot rows j+3
-    Q.ux[SP5] = nux;
-    Q.uz[SP5] = nuz;
-    sm[L::UX + SP5 * RW + li] = nux;
-    sm[L::UZ + SP5 * RW + li] = nuz;
-    if (X.hlo || X.hhi) {
-        const int hi = X.hlo ? 0 : RW - 2;
-        sm[L::UX + SP5 * RW + hi] = h0a;
-        sm[L::UX + SP5 * RW + hi + 1] = h0b;
-        sm[L::UZ + SP5 * RW + hi] = h1a;
-        sm[L::UZ + SP5 * RW + hi + 1] = h1b;
+    // ---- queues: shift by one row, then curr row j+6 and coefficient /
+    // snapshot rows j+4 of the next step (copied at step j-1: rows j+5, j+3)
+    if (j > j0) {
+        Q.ux[QN5] = sm[L::UX + SP5 * RB + li];
+        Q.uz[QN5] = sm[L::UZ + SP5 * RB + li];
+        Q.mu[QN3] = sm[L::MU + SP3 * RB + li];
+        Q.q[QN3] = sm[L::Q + SP3 * RB + li];
+        if (GRAD && X.do_grad) {
+            Q.f0[QN3] = srow(sm + L::F0 + SP3 * RB, li, X.prec, X.finv);
+            Q.f1[QN3] = srow(sm + L::F1 + SP3 * RB, li, X.prec, X.finv);
+        }
     }
-    Q.mu[SP3] = nmu;
-    Q.q[SP3] = nq;
-    sm[L::MU + RP3 * RW + li] = nmu;
-    if (!VTI) sm[L::Q + RP3 * RW + li] = nq;
-    if (VTI) {
-        Q.vlb[(P + 1) & 1] = nlb;
-        Q.vc13[(P + 1) & 1] = nc13;
-        Q.vlam[(P + 1) & 1] = nlam;
-    }
-    if (GRAD) {
-        Q.f0[SP3] = nf0;
-        Q.f1[SP3] = nf1;
-        sm[L::F0 + RP3 * RW + li] = nf0;
-        sm[L::F1 + RP3 * RW + li] = nf1;
-    }
+    return true;
 }
 
 template <bool VTI, bool GRAD, int NTH>
@@ -409,36 +452,43 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
               int flags, float dtg)
 {
     using L = MarchLayout<VTI, GRAD, NTH>;
-    const MarchRef U = units[blockIdx.x];
-    const ShotDev *__restrict__ Sp = shots + U.shot;
-    const int nt = Sp->nt;
-    if (it >= nt - 1) return;
+    __shared__ ShotDev S;
     extern __shared__ __align__(16) float smem[];
-
+    const MarchRef U = units[blockIdx.x];
     const int t = threadIdx.x;
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem + L::MBAR);
+    if (t == 0) {
+        S = shots[U.shot];
+        mbar_init(bars, 1);
+        mbar_init(bars + 1, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int nt = S.nt;
+    if (it >= nt - 1) return;
+
     MarchCtx X;
-    X.nx = Sp->nx;
-    X.nz = Sp->nz;
-    X.ldz = Sp->ldz;
+    X.nx = S.nx;
+    X.nz = S.nz;
+    X.ldz = S.ldz;
     X.nxz = X.nx * X.ldz;
     X.mld = M.ldz;
     X.xb = U.xb;
     X.xe = U.xe;
     X.z = U.za + t;
-    X.li = 2 + t;
+    X.s0 = (U.za - 2) & ~7;
+    X.s0c = X.s0 > 0 ? X.s0 : 0;
+    const int s1 = (U.za + NTH + 2 + 7) & ~7;
+    X.s1c = s1 < X.ldz ? s1 : X.ldz;
+    X.li = X.z - X.s0;
     X.zin = X.z >= 0 && X.z < X.nz;
     X.own = X.z >= U.oz0 && X.z < U.oz1;
-    X.zb4 = !(X.z >= 4 && X.z < X.nz - 4);
-    X.zb6 = !(X.z >= 6 && X.z < X.nz - 6);
-    X.hlo = t == 0;
-    X.hhi = t == NTH - 1;
-    X.hz = X.hlo ? U.za - 2 : U.za + NTH;
-    X.tzv = X.zin ? Sp->tz[X.z] : 0.f;
+    X.tzv = X.zin ? S.tz[X.z] : 0.f;
     X.zw0 = U.za + 32 * (t >> 5);
     X.zw1 = X.zw0 + 32;
-    X.u = Sp->u[(it + 1) & 1];
-    X.pn_off = Sp->u[it & 1] - X.u;
-    X.mofs = (long long)Sp->x0 * X.mld + X.z;
+    X.u = S.u[(it + 1) & 1];
+    X.pn_off = S.u[it & 1] - X.u;
+    X.mofs = (long long)S.x0 * X.mld;
 
     X.it = it;
     X.prec = C.snap_prec;
@@ -446,26 +496,33 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
     X.store = (flags & F_STORE) && (it % C.sub == 0);
     X.slot = it / C.sub;
     X.sc = 1.f;
-    if (X.store && X.prec != SNAP_FP32) X.sc = snap_scale(Sp->snap_amax, X.slot);
+    if (X.store && X.prec != SNAP_FP32) X.sc = snap_scale(S.snap_amax, X.slot);
     X.do_grad = GRAD && (flags & F_GRAD) && ((nt - 1 - (it + 1)) % C.sub == 0);
     X.itf = GRAD ? (nt - 1 - (it + 1)) / C.sub : 0;
     X.last = nt / C.sub;
+    X.has_fp = X.itf + 1 <= X.last;
+    X.has_fm = X.itf > 0;
     X.finv = X.finvp = X.finvm = 1.f;
     X.gw = 1.f;
     X.dtg = dtg;
     X.wdt = X.wh = 0.0;
     if (GRAD && X.do_grad) {
         if (X.prec != SNAP_FP32) {
-            X.finv = 1.f / snap_scale(Sp->snap_amax, X.itf);
-            if (X.itf + 1 <= X.last) X.finvp = 1.f / snap_scale(Sp->snap_amax, X.itf + 1);
-            if (X.itf > 0) X.finvm = 1.f / snap_scale(Sp->snap_amax, X.itf - 1);
+            X.finv = 1.f / snap_scale(S.snap_amax, X.itf);
+            if (X.has_fp) X.finvp = 1.f / snap_scale(S.snap_amax, X.itf + 1);
+            if (X.has_fm) X.finvm = 1.f / snap_scale(S.snap_amax, X.itf - 1);
         }
-        X.gw = Sp->gwt[X.itf];
+        X.gw = S.gwt[X.itf];
         X.wdt = (double)X.gw * 1.0 / (double)dtg;
         X.wh = (double)X.gw * 0.5 * (double)dtg;
     }
     X.roff = U.roff;
     X.amax = 0.f;
+    X.srcrow = S.src + (long long)it * S.nsrc;
+    X.snap = S.snap;
+    X.slot_elems = S.snap_slot;
+    X.grad = S.grad;
+    X.ph[0] = X.ph[1] = 0u;
 
     MarchQ<GRAD> Q;
 #pragma unroll
@@ -473,25 +530,23 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
         Q.ux[k] = Q.uz[k] = Q.mu[k] = Q.q[k] = Q.t0[k] = Q.cz[k] = 0.f;
         Q.ax[k] = Q.az[k] = Q.bx[k] = Q.f0[k] = Q.f1[k] = 0.f;
     }
-    Q.pv0[0] = Q.pv1[0] = Q.rh[0] = Q.pv0[1] = Q.pv1[1] = Q.rh[1] = 0.f;
-    Q.vlb[0] = Q.vc13[0] = Q.vlam[0] = Q.vlb[1] = Q.vc13[1] = Q.vlam[1] = 0.f;
 
-    for (int jb = U.xb - 9; jb < U.xe; jb += 8) {
-        march_step<VTI, GRAD, NTH, 0>(Q, X, smem, Sp, M, C, jb);
-        if (jb + 1 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 1>(Q, X, smem, Sp, M, C, jb + 1);
-        if (jb + 2 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 2>(Q, X, smem, Sp, M, C, jb + 2);
-        if (jb + 3 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 3>(Q, X, smem, Sp, M, C, jb + 3);
-        if (jb + 4 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 4>(Q, X, smem, Sp, M, C, jb + 4);
-        if (jb + 5 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 5>(Q, X, smem, Sp, M, C, jb + 5);
-        if (jb + 6 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 6>(Q, X, smem, Sp, M, C, jb + 6);
-        if (jb + 7 >= U.xe) break;
-        march_step<VTI, GRAD, NTH, 7>(Q, X, smem, Sp, M, C, jb + 7);
+    const int j0 = U.xb - 10;
+    bool ok = true;
+    for (int jb = j0; jb < U.xe; jb += 8) {
+#define MARCH_PHASE(k)                                                                              \
+    if (jb + k >= U.xe) break;                                                                      \
+    ok = march_step<VTI, GRAD, NTH, k>(Q, X, smem, S, M, C, jb + k, j0);                            \
+    if (!ok) break;
+        MARCH_PHASE(0) MARCH_PHASE(1) MARCH_PHASE(2) MARCH_PHASE(3)
+        MARCH_PHASE(4) MARCH_PHASE(5) MARCH_PHASE(6) MARCH_PHASE(7)
+#undef MARCH_PHASE
+    }
+    if (!ok) {
+        // a copy stage may still be in flight: give it a bounded wait before the
+        // shared memory is released
+        for (int s = 0; s < 2; s++) mbar_wait(bars + s, X.ph[s]);
+        return;
     }
 
     if ((flags & F_AMAX) && ((it + 1) % C.sub == 0)) {
@@ -507,7 +562,7 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
             m = t < NTH / 32 ? red[t] : 0.f;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (t == 0 && m > 0.f) atomicMax(Sp->snap_amax + (it + 1) / C.sub, __float_as_uint(m));
+            if (t == 0 && m > 0.f) atomicMax(S.snap_amax + (it + 1) / C.sub, __float_as_uint(m));
         }
     }
 }
