@@ -27,8 +27,11 @@
 //   queues      curr row j+5 and coefficient / snapshot rows j+3 (copied at
 //               step j-1) enter the register queues.
 // The first output row is preceded by 10 steps that only fill the pipeline.
-// The step body is unrolled over the 8 ring phases, so that register-queue
-// and ring slots are compile-time constants and nothing moves between steps.
+// Forward kernels unroll the step body over the 8 ring phases, so that
+// register-queue and ring slots are compile-time constants and nothing moves
+// between steps; the larger imaging-condition kernels keep one rolled body
+// (run-time ring slots, register queues shifted by one row per step) so that
+// the loop stays within the instruction cache.
 //
 // Shared memory, rows of RB = NTH + 24 floats; cell z of a row buffer sits
 // at index z - s0 with s0 = (za - 2) rounded down to a multiple of 8, so that
@@ -229,7 +232,29 @@ __device__ __forceinline__ void march_issue(const MarchCtx &X, float *sm, const 
 }
 
 // Returns false when the CTA must stop (a bounded wait gave up).
-// Register queues of 8 rows: row j+d sits at index (PH + d) & 7.
+// Register queues of 8 rows.  Unrolled (PH >= 0): row j+d sits at index
+// (PH + d) & 7.  Rolled (PH < 0): row j+d sits at index d + 2 and the queues
+// shift by one row at the end of each step.
+template <bool GRAD>
+__device__ __forceinline__ void shift_queues(MarchQ<GRAD> &Q)
+{
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        Q.ux[k] = Q.ux[k + 1];
+        Q.uz[k] = Q.uz[k + 1];
+        Q.mu[k] = Q.mu[k + 1];
+        Q.q[k] = Q.q[k + 1];
+        Q.t0[k] = Q.t0[k + 1];
+        Q.cz[k] = Q.cz[k + 1];
+        if (GRAD) {
+            Q.ax[k] = Q.ax[k + 1];
+            Q.az[k] = Q.az[k + 1];
+            Q.bx[k] = Q.bx[k + 1];
+            Q.f0[k] = Q.f0[k + 1];
+            Q.f1[k] = Q.f1[k + 1];
+        }
+    }
+}
 
 template <bool VTI, bool GRAD, int NTH, int PH>
 __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *sm, const ShotDev &S,
@@ -237,14 +262,15 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
 {
     using L = MarchLayout<VTI, GRAD, NTH>;
     constexpr int RB = L::RB;
-    constexpr int P = PH;
-    constexpr int QM2 = (PH + 6) & 7, QM1 = (PH + 7) & 7, Q00 = PH, QP1 = (PH + 1) & 7, QP2 = (PH + 2) & 7,
-                  QP3 = (PH + 3) & 7, QP4 = (PH + 4) & 7;
+    const int P = PH >= 0 ? PH : ((j - j0) & 7);
+    constexpr int QM2 = PH >= 0 ? (PH + 6) & 7 : 0, QM1 = PH >= 0 ? (PH + 7) & 7 : 1, Q00 = PH >= 0 ? PH : 2,
+                  QP1 = PH >= 0 ? (PH + 1) & 7 : 3, QP2 = PH >= 0 ? (PH + 2) & 7 : 4,
+                  QP3 = PH >= 0 ? (PH + 3) & 7 : 5, QP4 = PH >= 0 ? (PH + 4) & 7 : 6;
     // register-queue slots of the rows arriving at the end of this step
-    constexpr int QN5 = (PH + 5) & 7, QN3 = (PH + 3) & 7;
+    constexpr int QN5 = PH >= 0 ? (PH + 5) & 7 : 6, QN3 = PH >= 0 ? (PH + 3) & 7 : 4;
     // ring slots of rows j+d (8-row rings) and (4-row rings)
-    constexpr int S0 = P, SP2 = (P + 2) & 7, SP3 = (P + 3) & 7, SP5 = (P + 5) & 7;
-    constexpr int R0 = P & 3, RP1 = (P + 1) & 3, RP2 = (P + 2) & 3;
+    const int S0 = P, SP2 = (P + 2) & 7, SP3 = (P + 3) & 7, SP5 = (P + 5) & 7;
+    const int R0 = P & 3, RP1 = (P + 1) & 3, RP2 = (P + 2) & 3;
     const int li = X.li;
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(sm + L::MBAR);
 
@@ -431,8 +457,9 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
         }
     }
 
-    // ---- queues: shift by one row, then curr row j+6 and coefficient /
-    // snapshot rows j+4 of the next step (copied at step j-1: rows j+5, j+3)
+    // ---- queues: curr row j+5 and coefficient / snapshot rows j+3 (copied
+    // at step j-1) take the slots the next step reads as j+4 and j+2
+    if (PH < 0) shift_queues<GRAD>(Q);
     if (j > j0) {
         Q.ux[QN5] = sm[L::UX + SP5 * RB + li];
         Q.uz[QN5] = sm[L::UZ + SP5 * RB + li];
@@ -447,7 +474,7 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
 }
 
 template <bool VTI, bool GRAD, int NTH>
-__global__ void __launch_bounds__(NTH, 2)
+__global__ void __launch_bounds__(NTH, (GRAD || NTH > 224) ? 2 : 3)
 elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ units, ModelDev M, StepConst C, int it,
               int flags, float dtg)
 {
@@ -533,14 +560,21 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
 
     const int j0 = U.xb - 10;
     bool ok = true;
-    for (int jb = j0; jb < U.xe; jb += 8) {
+    if (GRAD) {
+        for (int j = j0; j < U.xe; j++) {
+            ok = march_step<VTI, GRAD, NTH, -1>(Q, X, smem, S, M, C, j, j0);
+            if (!ok) break;
+        }
+    } else {
+        for (int jb = j0; jb < U.xe; jb += 8) {
 #define MARCH_PHASE(k)                                                                              \
     if (jb + k >= U.xe) break;                                                                      \
     ok = march_step<VTI, GRAD, NTH, k>(Q, X, smem, S, M, C, jb + k, j0);                            \
     if (!ok) break;
-        MARCH_PHASE(0) MARCH_PHASE(1) MARCH_PHASE(2) MARCH_PHASE(3)
-        MARCH_PHASE(4) MARCH_PHASE(5) MARCH_PHASE(6) MARCH_PHASE(7)
+            MARCH_PHASE(0) MARCH_PHASE(1) MARCH_PHASE(2) MARCH_PHASE(3)
+            MARCH_PHASE(4) MARCH_PHASE(5) MARCH_PHASE(6) MARCH_PHASE(7)
 #undef MARCH_PHASE
+        }
     }
     if (!ok) {
         // a copy stage may still be in flight: give it a bounded wait before the
