@@ -806,8 +806,9 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         REQ(bc >= 1 && bc <= 3, "boundary condition must be 1, 2 or 3");
         if (M.kind != KIND_ACOUSTIC) REQ(bc <= 2, "the elastic propagators take boundary conditions 1 or 2");
     }
-    if (M.kind == KIND_ACOUSTIC || M.kind == KIND_AE)
-        throw Error(FWI2D_ERR_UNSUPPORTED, "this propagator is not built yet");
+    if (M.kind == KIND_AE) throw Error(FWI2D_ERR_UNSUPPORTED, "this propagator is not built yet");
+    const bool acoustic = M.kind == KIND_ACOUSTIC;
+    REQ(!(acoustic && p.mt), "the acoustic propagator takes point sources only (mt = 0)");
     REQ(p.checkpoint_every == 0, "checkpointing is not available in this build");
     set_device(ctx);
 
@@ -821,6 +822,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     // shape: the requested one, else the marching kernel where it has enough
     // units to fill the GPU, else the first tile shape that fits every shot
     auto shape_ok = [&](int i) {
+        if (acoustic && !acoustic_shape_ok(i)) return false;
         for (int s = 0; s < nshots; s++)
             if (!shape_fits(i, shots[s].nx, M.nz)) return false;
         return true;
@@ -829,7 +831,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     if (shape < 0 || shape >= shape_count()) {
         shape = -1;
         const int m0 = elastic_tile_count();
-        if (shape_ok(m0)) {
+        if (!acoustic && shape_ok(m0)) {
             long long units = 0;
             for (int s = 0; s < nshots; s++) units += (long long)make_units(m0, s, shots[s].nx, M.nz).marches.size();
             if (units >= 148) shape = m0;
@@ -864,14 +866,14 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->x0 = sh.x0;
         S->nx = sh.nx;
         S->nt = sh.nt;
-        S->ncomp = 2;
+        S->ncomp = acoustic ? 1 : 2;
         const ShotUnits U = make_units(shape, s, sh.nx, M.nz);
         const int nunits = U.nunits();
         S->ntr_src = sh.src.ntr;
-        S->ncomp_src = p.mt ? 3 : 2;
+        S->ncomp_src = acoustic ? 1 : (p.mt ? 3 : 2);
         S->nr = sh.rcv.ntr;
         S->nsrc_rows = S->ncomp_src * S->ntr_src;
-        S->nrcv_rows = 2 * S->nr;
+        S->nrcv_rows = S->ncomp * S->nr;
         // forward sources: force -> rows c*ntr ; moment tensor blocks (mxx, mzz, mxz)
         int ra[2], rb[2];
         if (!p.mt) {
@@ -884,19 +886,25 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             ra[1] = 2 * S->ntr_src;     // next1: inx = mxz, inz = mzz
             rb[1] = S->ntr_src;
         }
-        build_inj(sh.src, 2, ra, rb, U, S->inj_f, S->inj_f_off, S->inj_f_roff);
+        build_inj(sh.src, S->ncomp, ra, rb, U, S->inj_f, S->inj_f_off, S->inj_f_roff);
         int qa[2] = {0, S->nr}, qb[2] = {0, 0};
-        build_inj(sh.rcv, 2, qa, qb, U, S->inj_a, S->inj_a_off, S->inj_a_roff);
-        build_ext(sh.rcv, 2, U, S->ext_f, S->ext_f_off, S->ext_f_roff);
+        build_inj(sh.rcv, S->ncomp, qa, qb, U, S->inj_a, S->inj_a_off, S->inj_a_roff);
+        build_ext(sh.rcv, S->ncomp, U, S->ext_f, S->ext_f_off, S->ext_f_roff);
         S->ext_none_off.assign(nunits + 1, 0);
 
         // boundary divisors and taper on this shot's window of the model
         std::vector<float> den, tz, tx;
-        const float *lam = M.hp(0) + (size_t)sh.x0 * M.nz, *mu = M.hp(1) + (size_t)sh.x0 * M.nz,
-                    *rho = M.hp(2) + (size_t)sh.x0 * M.nz;
-        const float *eps = vti ? M.hp(4) + (size_t)sh.x0 * M.nz : nullptr;
-        elastic_scale_divisors(sh.nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, p.bc_top == 2,
-                               p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
+        if (acoustic) {
+            const float *K = M.hp(0) + (size_t)sh.x0 * M.nz, *irho = M.hp(1) + (size_t)sh.x0 * M.nz;
+            acoustic_scale_divisors(sh.nx, M.nz, M.dx, M.dz, p.dt, K, irho, M.nz, p.bc_top == 2, p.bc_bottom == 2,
+                                    p.bc_left == 2, p.bc_right == 2, den);
+        } else {
+            const float *lam = M.hp(0) + (size_t)sh.x0 * M.nz, *mu = M.hp(1) + (size_t)sh.x0 * M.nz,
+                        *rho = M.hp(2) + (size_t)sh.x0 * M.nz;
+            const float *eps = vti ? M.hp(4) + (size_t)sh.x0 * M.nz : nullptr;
+            elastic_scale_divisors(sh.nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, p.bc_top == 2,
+                                   p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
+        }
         taper_factors(sh.nx, M.nz, p.taper_top, p.taper_bottom, p.taper_left, p.taper_right, p.taper_strength,
                       true, true, true, true, tz, tx);
         S->nslot = p.sub > 0 ? 1 + sh.nt / p.sub : 0;
@@ -973,6 +981,11 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
                        cudaStream_t st)
 {
     int n = 0;
+    if (P.kind == KIND_ACOUSTIC) {
+        launch_acoustic_step(P.tshape, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C, it, flags, P.dtg,
+                             st);
+        return 1;
+    }
     if (P.marches.empty()) {
         launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md,
                             P.C, it, flags, P.dtg, st);
@@ -1100,7 +1113,11 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
     const ModelDev md = M.dev();
     for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(ctx, P, shots, md, it, flags, cst);
     if (!adj) {
-        launch_finalize(shots, nshots, P.C, 2, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
+        launch_finalize(shots, nshots, P.C, P.kind == KIND_ACOUSTIC ? 1 : 2, STEP_EXTRACT | (store ? STEP_STORE : 0),
+                        cst);
+        n++;
+    } else if (P.kind == KIND_ACOUSTIC) {
+        launch_acoustic_final_grad(shots, nshots, md, P.C, P.dtg, cst);   // snapshot 0 with the last adjoint field
         n++;
     }
     CK(cudaGetLastError());

@@ -692,6 +692,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
 }  // namespace fwi2d
 #include "march.cuh"
 #include "zband.cuh"
+#include "acoustic.cuh"
 namespace fwi2d {
 
 // ---------------------------------------------------------------------------
@@ -888,6 +889,29 @@ void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const Shot
 }
 
 int zband_rows() { return kZbRows; }
+
+// tile shapes of the acoustic kernel: (32, 16) and (32, 8), the elastic shapes 2 and 3
+bool acoustic_shape_ok(int shape) { return shape == 2 || shape == 3; }
+
+void launch_acoustic_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    const bool grad = (flags & F_GRAD) != 0;
+    if (shape == 2) {
+        if (grad) acoustic_step<16, true><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        else acoustic_step<16, false><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+    } else {
+        if (grad) acoustic_step<8, true><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        else acoustic_step<8, false><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+    }
+}
+
+void launch_acoustic_final_grad(const ShotDev *shots, int nshots, const ModelDev &M, const StepConst &C, float dtg,
+                                cudaStream_t st)
+{
+    dim3 grid(148, nshots);
+    acoustic_final_grad<<<grid, 256, 0, st>>>(shots, nshots, M, C, dtg);
+}
 
 void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
                        cudaStream_t st)

@@ -1,4 +1,4 @@
-// Host entry points of the kernels in kernels.cu / acoustic.cu.
+// Host entry points of the kernels in kernels.cu.
 #pragma once
 #include "engine.h"
 
@@ -26,9 +26,8 @@ void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, 
                        cudaStream_t st);
 void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st);
 
-// acoustic.cu
-int acoustic_tile_count();
-void acoustic_tile_shape(int i, int *tz, int *tx);
+// acoustic kernel (acoustic.cuh): tile shapes 2 and 3 only
+bool acoustic_shape_ok(int shape);
 void launch_acoustic_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
                           const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_acoustic_final_grad(const ShotDev *shots, int nshots, const ModelDev &M, const StepConst &C, float dtg,

@@ -114,10 +114,19 @@ class Propagator:
             arr[i] = C.Shot(s.x0, s.nx, s.nt, _injector(st, src), _injector(C.INJ_DELTA, rcv),
                             _injector(0, None), _injector(0, None))
             nsrc = len(s.src_x)
-            self.src_rows.append((3 if s.mt else 2) * nsrc)
-            self.rcv_rows.append(2 * len(s.rcv_x))
+            nc = self.ncomp()
+            self.src_rows.append((3 if s.mt else nc) * nsrc)
+            self.rcv_rows.append(nc * len(s.rcv_x))
         C.check(self.L.fwi2d_set_shots(self.h, ctypes.byref(params), len(shots), arr))
         self._keep = keep
+
+    def ncomp(self):
+        """Wavefield components: 1 (pressure) for the acoustic propagator, else 2."""
+        return 1 if self.kind == C.ACOUSTIC else 2
+
+    def ngrad(self):
+        """Gradient components: (K, 1/rho) acoustic, else (lambda, mu, rho)."""
+        return 2 if self.kind == C.ACOUSTIC else 3
 
     # -- host API ---------------------------------------------------------
     def _concat(self, blocks, rows):
@@ -129,27 +138,29 @@ class Propagator:
 
     def forward(self, src_blocks, store=True):
         """src_blocks[s]: [ncomp][ntr][nt] traces of shot s.  Returns the
-        receiver blocks [2][nr][nt] per shot."""
+        receiver blocks [ncomp][nr][nt] per shot (ncomp 2, or 1 acoustic)."""
         src = self._concat(src_blocks, self.src_rows)
         out = np.zeros(sum(r * s.nt for r, s in zip(self.rcv_rows, self.shots)), np.float32)
         C.check(self.L.fwi2d_forward(self.h, C.ptr(src), C.ptr(out), 1 if store else 0))
         res, o = [], 0
         for r, s in zip(self.rcv_rows, self.shots):
-            res.append(out[o:o + r * s.nt].reshape(2, r // 2, s.nt))
+            nc = self.ncomp()
+            res.append(out[o:o + r * s.nt].reshape(nc, r // nc, s.nt))
             o += r * s.nt
         return res
 
     def adjoint(self, adj_blocks):
-        """adj_blocks[s]: [2][nr][nt] adjoint sources of shot s.  Returns the
-        raw (lambda, mu, rho) imaging condition summed over shots."""
+        """adj_blocks[s]: [ncomp][nr][nt] adjoint sources of shot s.  Returns
+        the raw imaging condition summed over shots: (lambda, mu, rho), or
+        (K, 1/rho) for the acoustic propagator."""
         adj = self._concat(adj_blocks, self.rcv_rows)
-        g = np.zeros((3, self.nx, self.nz), np.float32)
+        g = np.zeros((self.ngrad(), self.nx, self.nz), np.float32)
         C.check(self.L.fwi2d_adjoint(self.h, C.ptr(adj), C.ptr(g)))
         return g
 
     def snapshot(self, shot, slot):
         s = self.shots[shot]
-        out = np.zeros((2, s.nx, self.nz), np.float32)
+        out = np.zeros((self.ncomp(), s.nx, self.nz), np.float32)
         C.check(self.L.fwi2d_snapshot(self.h, shot, slot, C.ptr(out)))
         return out
 

@@ -79,6 +79,36 @@ def test_forward_adjoint_vs_oracle(kind, mt, bc, shape, grid):
         assert K.rel_l2(g_g[c], g_o[c]) <= GRAD_TOL, "gradient component %d" % c
 
 
+@pytest.mark.parametrize("bc", [(1, 2, 2, 2), (3, 3, 2, 2), (2, 2, 2, 2), (1, 1, 3, 3)])
+@pytest.mark.parametrize("shape,grid", [(2, (72, 80)), (3, (72, 80)), (2, (120, 200)), (3, (60, 251))])
+def test_acoustic_forward_adjoint_vs_oracle(bc, shape, grid):
+    """Acoustic propagator (pressure, model (K, 1/rho)): pressure-release,
+    absorbing and rigid sides; traces, snapshots and the (K, 1/rho) imaging
+    condition against the oracle."""
+    kind = O.KIND_ACOUSTIC
+    nx, nz = grid
+    d, nt = 0.01, 200
+    mc = K.converted(kind, K.model_case(kind, nx, nz, d, seed=4))
+    sl, rl = K.geometry(nx, nz, d, nr=20)
+    pd = K.par_dict(nt=nt, dt=1e-3, bc=bc)
+    src = K.sources(1, nt, 1e-3)
+    port = O.Port(32)
+    par = O.make_par(**pd, ns=1, nr=len(rl[0]))
+    rcv_o, full_o = K.oracle_forward(port, kind, mc, src, par, nx, nz, d, sl, rl)
+    adj = np.ascontiguousarray(rcv_o[:, :, ::-1])
+    g_o = K.oracle_adjoint(port, kind, mc, adj, par, nx, nz, d, sl, rl, full_o)
+    rcv_g, g_g, snaps = run_gpu(kind, mc, src, pd, nx, nz, d, sl, rl, adj_src=adj, shape=shape)
+    e_tr = K.rel_l2(rcv_g, rcv_o)
+    idx = list(range(0, nt, max(1, nt // 5)))
+    e_sn = K.rel_l2(snaps, full_o[idx])
+    print("acoustic bc %s shape %d: traces %.3e (bitwise %.4f) snapshots %.3e gradient %.3e / %.3e" % (
+        bc, shape, e_tr, np.mean(rcv_g == rcv_o), e_sn, K.rel_l2(g_g[0], g_o[0]), K.rel_l2(g_g[1], g_o[1])))
+    assert e_tr <= TRACE_TOL
+    assert e_sn <= TRACE_TOL
+    for c in range(2):
+        assert K.rel_l2(g_g[c], g_o[c]) <= GRAD_TOL, "gradient component %d" % c
+
+
 def test_dropin_propagate_matches_oracle():
     """fwi2d_propagate: the propagate_gpu drop-in with the reference's buffers."""
     import ctypes
