@@ -192,6 +192,30 @@ class Reference(_Lib):
         f(kind, _ptr(m), m.shape[-1] * m.shape[-2], 1 if forward else 0)
         return m
 
+    def misfit_grad(self, kind, par, nx, nz, d, nt, dt, src_loc, rcv_locs, model_raw, src, obs=None):
+        """The reference operator's forward data (seismotype 1) and, with obs,
+        the solver's gradient for residual f(m) - obs (ref_misfit_grad).
+        Returns (syn [2][nr][nt], grad or None)."""
+        f = self.lib.ref_misfit_grad
+        vp = ctypes.c_void_p
+        f.argtypes = [ctypes.c_int, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                      ctypes.c_int, ctypes.c_double, self._real(), self._real(), ctypes.c_int, vp, vp, vp, vp, vp, vp, vp]
+        rx, rz = self.arr(rcv_locs[0]), self.arr(rcv_locs[1])
+        nr = len(rx)
+        m = self.arr(model_raw)
+        s = self.arr(src).reshape(2, nt)
+        syn = np.zeros((2, nr, nt), self.dtype)
+        o = None if obs is None else self.arr(obs)
+        g = None if obs is None else np.zeros(m.shape, self.dtype)
+        rc = f(kind, ctypes.byref(par), nx, nz, d, d, nt, dt, src_loc[0], src_loc[1], nr, _ptr(rx), _ptr(rz), _ptr(m),
+               _ptr(s), _ptr(o), _ptr(syn), _ptr(g))
+        if rc != 0:
+            raise RuntimeError("reference misfit/gradient failed")
+        return syn, g
+
+    def _real(self):
+        return ctypes.c_float if self.dtype == np.float32 else ctypes.c_double
+
     def propagate(self, kind, adj, model, src, rcv, par, nx, nz, dx, dz, ox, oz, inj_locs, ext_locs,
                   inj_type=0, full=None, grad=None, water_inj_locs=None, water_ext_locs=None):
         def loc(l):

@@ -4,6 +4,8 @@
 // oracle/build_ref.sh into oracle/_ref/.  Used to generate tests/golden/ and
 // to pin the restatement in oracle/fwi2d_oracle.c.
 #include <vector>
+#include <memory>
+#include <cstdio>
 #include <cstring>
 #include "we_op.hpp"
 
@@ -82,6 +84,59 @@ int ref_injector_weights(int type, int ntr, const data_t *lx, const data_t *lz, 
     std::memcpy(xw, J->_xw.data(), J->_xw.size() * sizeof(data_t));
     std::memcpy(zw, J->_zw.data(), J->_zw.size() * sizeof(data_t));
     delete J;
+    return 0;
+}
+
+// One shot through the reference's operator interface: nl_we_op_e (kind 0)
+// or nl_we_op_vti (kind 1) forward modelling of the raw model (vp, vs, rho
+// [, delta, eps]) with seismotype 1 (particle velocity), linear resampling at
+// the propagation rate (the identity), and, when obs is given, the gradient
+// the solver forms (optimization.hpp:760-890): residual r = f(m) - obs
+// weighted by applyHt, then apply_jacobianT (we_op.cpp:1057-1239).  src is
+// [2][nt] (x, z force), syn and obs [2][nr][nt], grad [npar][nx][nz].
+int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, double dz, int nt, double dt,
+                    data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *model,
+                    const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
+{
+    try {
+        param par = to_param(rp);
+        par.nt = nt;
+        par.dt = (data_t)dt;
+        par.sub = obs ? 1 : 0;
+        par.ns = 1;
+        par.nr = nr;
+        par.nmodels = kind == 1 ? 5 : 3;
+        par.seismotype = 1;
+        par.resampling = "linear";
+        data_t sl[2] = {sx, sz};
+        par.sxz = locs(1, sl, sl + 1);
+        par.rxz = {locs(nr, rx, rz)};
+        hypercube<data_t> dom(axis<data_t>(nz, 0, (data_t)dz), axis<data_t>(nx, 0, (data_t)dx),
+                              axis<data_t>(par.nmodels, 0, 1));
+        auto allsrc = std::make_shared<vecReg<data_t> >(hypercube<data_t>(axis<data_t>(nt, 0, (data_t)dt), axis<data_t>(2, 0, 1)));
+        std::memcpy(allsrc->getVals(), src, 2 * (size_t)nt * sizeof(data_t));
+        std::shared_ptr<nl_we_op> op;
+        if (kind == 0) op = std::make_shared<nl_we_op_e>(dom, allsrc, par);
+        else op = std::make_shared<nl_we_op_vti>(dom, allsrc, par);
+        auto m = std::make_shared<vecReg<data_t> >(dom);
+        std::memcpy(m->getVals(), model, m->getN123() * sizeof(data_t));
+        auto d = std::make_shared<vecReg<data_t> >(*op->getRange());
+        op->forward(false, m, d);
+        std::memcpy(syn, d->getCVals(), d->getN123() * sizeof(data_t));
+        if (obs) {
+            auto r = std::make_shared<vecReg<data_t> >(*op->getRange());
+            data_t *pr = r->getVals();
+            const long n = (long)r->getN123();
+            for (long i = 0; i < n; i++) pr[i] = syn[i] - obs[i];
+            applyHt(false, false, pr, pr, 2 * nr, nt, (data_t)dt, 0, 2 * nr);
+            auto g = std::make_shared<vecReg<data_t> >(dom);
+            op->jacobianT(false, g, m, r);
+            std::memcpy(grad, g->getCVals(), g->getN123() * sizeof(data_t));
+        }
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_misfit_grad: %s\n", e.what());
+        return -1;
+    }
     return 0;
 }
 

@@ -86,6 +86,55 @@ def ae_case(prec):
                 grad=g)
 
 
+def fwi_case(kind):
+    """The solver's gradient through the reference's operator interface
+    (nl_we_op_e / nl_we_op_vti forward + apply_jacobianT, residual weighted by
+    applyHt), with the finite-difference directional derivative and the
+    nonlinear dot-product test (nloper::dotProduct) evaluated on the reference
+    itself."""
+    lib = O.Reference(32)
+    nx, nz, d, nt, dt = 100, 80, 0.01, 400, 1e-3
+    rng = np.random.default_rng(1)
+    true = K.model_case(kind, nx, nz, d, seed=7)
+    start = true.copy()
+    from scipy.ndimage import gaussian_filter
+    for c in range(3):
+        start[c] = gaussian_filter(true[c].astype(np.float64), 4, mode="nearest").astype(np.float32)
+    sx, sz = (0.5 * (nx - 1) + 0.3) * d, 0.02
+    rx = np.linspace(3 * d, (nx - 4) * d, 30).astype(np.float32)
+    rz = np.full(30, 0.02, np.float32)
+    src = K.sources(2, nt, dt).reshape(2, nt)
+    dm = np.zeros_like(start)
+    for c in range(3):
+        f = gaussian_filter(rng.uniform(-1, 1, (nx, nz)), 5, mode="nearest")
+        dm[c] = f / np.abs(f).max() * start[c]
+    par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=30)
+    geo = ((np.float32(sx), np.float32(sz)), (rx, rz))
+    obs, _ = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], true, src)
+    w = np.full(nt, dt)
+    w[0] = w[-1] = 0.5 * dt
+
+    def phi(m):
+        syn, _ = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], m, src)
+        r = syn.astype(np.float64) - obs
+        return 0.5 * np.sum(w * r * r)
+    syn0, g = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], start, src, obs)
+    eps = 1e-3
+    fd = (phi(start + eps * dm) - phi(start - eps * dm)) / (2 * eps)
+    an = float(np.sum(g[:3].astype(np.float64) * dm[:3]))
+    # nloper::dotProduct: residual d for observed data f(m) - d
+    rd = rng.uniform(-1, 1, syn0.shape).astype(np.float32) * np.float32(np.abs(syn0).max())
+    _, gd = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], start, src, syn0 - rd)
+    sum2 = float(np.sum(gd[:3].astype(np.float64) * dm[:3]))
+    s1 = []
+    for e in (1e-2, 1e-3):
+        f1, _ = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], start + e * dm, src)
+        s1.append(float(np.sum(w * rd.astype(np.float64) * (f1.astype(np.float64) - syn0) / e)))
+    return dict(kind=kind, nx=nx, nz=nz, d=d, nt=nt, dt=dt, sx=sx, sz=sz, rx=rx, rz=rz, true=true, start=start,
+                src=src, obs=obs, dm=dm, grad=g, misfit=phi(start), fd=fd, an=an, dot_residual=rd, dot_sum1=np.array(s1),
+                dot_sum2=sum2, grad_dot=gd)
+
+
 def main():
     if not O.have_reference(32):
         sys.exit("oracle/_ref is not built (oracle/build_ref.sh needs the reference tree)")
@@ -94,6 +143,8 @@ def main():
             out = elastic_like(name, kind, mt, bc, nx, nz, nt, prec)
             np.savez_compressed(os.path.join(HERE, "%s_f%d.npz" % (name, prec)), **out)
         np.savez_compressed(os.path.join(HERE, "acoustic_elastic_f%d.npz" % prec), **ae_case(prec))
+    for kind, name in ((O.KIND_ELASTIC, "elastic"), (O.KIND_VTI, "vti")):
+        np.savez_compressed(os.path.join(HERE, "fwi_gradient_%s_f32.npz" % name), **fwi_case(kind))
     print("golden fixtures written to", HERE)
 
 
