@@ -8,6 +8,11 @@ snapshot storage, residual against observed data, adjoint sources, adjoint
 propagation with the zero-lag imaging condition, H quadrature and chain rule.
 Cell-updates per step: (nt-1) * nx * nz forward + the same adjoint.
 
+At N = 1 the line also carries "batched": the same evaluation for a batch of
+32 shots of the batch geometry (every other shot of the 64-shot line, cropped
+grids of 1.0-3.5 km apertures, 1.2-2.0 s records) on the elastic model with
+FP16 snapshots, all shots in one plan, timed the same way.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config single|batch]
 
 N > 1 runs one process per GPU (torchrun); each rank computes its own shot
@@ -40,6 +45,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="single", choices=["single", "batch"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -388,6 +394,14 @@ def run_ours(args):
                          "forward_achieved": BYTES_FWD * cells_launch / fwd_launch_s / 1e9},
             "clocks": clocks,
         }
+        if world == 1 and args.config == "single" and not args.no_batched:
+            try:
+                b = run_batched(local, 2, 1)
+                b["shots_per_s_vs_plain"] = b["shots_per_s"] / shots_s
+                b["gcell_vs_plain"] = b["value"] / value
+                line["batched"] = b
+            except Exception as e:   # the batched leg never blocks the main line
+                line["batched"] = {"error": str(e)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 nt_s = 301
@@ -404,6 +418,50 @@ def run_ours(args):
     P.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_batched(local, steps, warmup):
+    """Batched elastic gradients (FP16 snapshots) on one GPU; returns a dict."""
+    import torch
+    import fwi2d_b200 as F
+    from fwi2d_b200 import workloads as W
+    from fwi2d_b200 import _capi as C
+    wl = W.elastic_batch(every=2)
+    P, start, srcs = make_prop(wl, local)
+    obs = observed(wl, local, srcs)
+    stream = torch.cuda.Stream()
+    P.set_stream(stream.cuda_stream)
+    P.set_observed(obs)
+    P.upload(srcs, adjoint=False)
+    L = F.load()
+
+    def step():
+        C.check(L.fwi2d_fwi_gradient(P.h, None, None, None, wl["seismotype"], None, None))
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    fwd_ms, adj_ms = P.last_timing()
+    info = P.plan_info()
+    P.close()
+    cells = cells_per_step(wl)
+    return {"workload": "elastic FWI gradient, %d shots of the batch geometry on cropped grids (mean %d x %d cells, "
+                        "mean nt %d), FP16 snapshots" % (len(wl["shots"]),
+                                                          np.mean([s["nx"] for s in wl["shots"]]), wl["nz"],
+                                                          np.mean([s["nt"] for s in wl["shots"]])),
+            "shots": len(wl["shots"]), "ms_per_step": ms, "shots_per_s": len(wl["shots"]) / (ms / 1e3),
+            "value": cells / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "cell_updates_per_step": cells,
+            "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "tile_shape": info["tile_shape"],
+            "snapshot_bytes": info["snapshot_bytes"], "steps": steps, "warmup": warmup}
 
 
 def main():

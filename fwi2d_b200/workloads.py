@@ -14,6 +14,8 @@ value distributions the configurations describe, in the reference's units
 * vti_batch       -- the same grid, VTI with eps in [0.05, 0.20] and delta in
   [0, 0.10] as smooth seeded fields; 64 shots 60 m apart, each with a 1.0-3.5
   km receiver aperture on its own cropped grid and a 1.2-2.0 s record.
+* elastic_batch   -- the batch geometry of vti_batch on the isotropic model
+  of elastic_single (batched elastic gradients).
 """
 import math
 
@@ -98,14 +100,11 @@ def elastic_single(nt=5001):
                 shots=[dict(x0=0, nx=nx, sx=[2.0], sz=[0.01], rx=rx, rz=rz, nt=nt)], params=params, seismotype=1)
 
 
-def vti_batch(nshots=64, nt_max=5001, seed=2):
-    """Batched VTI workload: 64 shots on cropped grids with uneven apertures
-    and record lengths."""
-    nx, nz, d, dt = 801, 401, 0.005, 4e-4
-    true = vti_model(nx, nz, d, seed=seed)
-    start = np.concatenate([smoothed(true[:3], 50), true[3:]])
+def batch_geometry(nshots=64, nt_max=5001, seed=2, nx=801, d=0.005, dt=4e-4):
+    """Shots 60 m apart, each with a receiver aperture drawn from [1.0, 3.5] km
+    on its own cropped grid (aperture and source with a 60-cell margin) and a
+    record length drawn from [1.2, 2.0] s."""
     rng = np.random.default_rng(seed)
-    w = ricker(nt_max, dt, 10.0, 0.1)
     shots = []
     margin = 60
     for k in range(nshots):
@@ -120,9 +119,30 @@ def vti_batch(nshots=64, nt_max=5001, seed=2):
         x0 = max(0, int(math.floor(min(lo, sx) / d)) - margin)
         x1 = min(nx, int(math.ceil(max(hi, sx) / d)) + margin + 1)
         shots.append(dict(x0=x0, nx=x1 - x0, sx=[sx], sz=[0.01], rx=rx, rz=np.full(len(rx), 0.01, np.float32), nt=nts))
+    return shots
+
+
+def vti_batch(nshots=64, nt_max=5001, seed=2):
+    """Batched VTI workload: 64 shots on cropped grids with uneven apertures
+    and record lengths."""
+    nx, nz, d, dt = 801, 401, 0.005, 4e-4
+    true = vti_model(nx, nz, d, seed=seed)
+    start = np.concatenate([smoothed(true[:3], 50), true[3:]])
+    w = ricker(nt_max, dt, 10.0, 0.1)
+    shots = batch_geometry(nshots, nt_max, seed, nx, d, dt)
     ang = np.float32(1.5708)
     src = np.stack([w * np.float32(np.cos(ang)), w * np.float32(np.sin(ang))])[:, None, :].astype(np.float32)
     params = dict(nt=nt_max, sub=1, dt=dt, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2, taper_top=0,
                   taper_bottom=60, taper_left=60, taper_right=60, taper_strength=0.05)
     return dict(kind=C.VTI, nx=nx, nz=nz, d=d, dt=dt, nt=nt_max, true=true, start=start, src=src, shots=shots,
                 params=params, seismotype=1)
+
+
+def elastic_batch(nshots=64, nt_max=5001, seed=2, every=1, snapshot_precision=C.SNAP_FP16):
+    """Batched elastic workload: the vti_batch geometry (every `every`-th of its
+    shots) on the elastic_single model, with reduced-precision snapshots."""
+    wl = elastic_single(nt=nt_max)
+    shots = batch_geometry(nshots, nt_max, seed, wl["nx"], wl["d"], wl["dt"])[::every]
+    wl["shots"] = shots
+    wl["params"] = dict(wl["params"], snapshot_precision=snapshot_precision)
+    return wl
