@@ -1749,7 +1749,8 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
 {
     ABI_TRY
     REQ(par && model && inj && ext, "null argument");
-    REQ(kind == FWI2D_ELASTIC || kind == FWI2D_VTI, "fwi2d_propagate: this propagator is not built yet");
+    REQ(kind == FWI2D_ELASTIC || kind == FWI2D_VTI || kind == FWI2D_ACOUSTIC,
+        "fwi2d_propagate: this propagator is not built yet");
     (void)inja;
     (void)exta;
     int dev = 0;
@@ -1778,18 +1779,18 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
     ShotPlan &S = *P.shots[0];
     // gather the component blocks (stride ns*nt / nr*nt in the reference's buffers)
     const int in_ntr = adj ? S.nr : S.ntr_src;
-    const int in_comp = adj ? 2 : S.ncomp_src;
+    const int in_comp = adj ? S.ncomp : S.ncomp_src;
     const int stride = adj ? nr : ns;
     std::vector<float> in((size_t)in_comp * in_ntr * nt);
     for (int c = 0; c < in_comp; c++)
         for (int t = 0; t < in_ntr; t++)
             std::memcpy(&in[((size_t)c * in_ntr + t) * nt], allsrc + ((size_t)c * stride + t) * nt, nt * sizeof(float));
     if (!adj) {
-        std::vector<float> out((size_t)2 * S.nr * nt);
+        std::vector<float> out((size_t)S.ncomp * S.nr * nt);
         upload_traces(ctx, in.data(), false);
         run(ctx, false, store);
         download_rcv(ctx, out.data());
-        for (int c = 0; c < 2; c++)
+        for (int c = 0; c < S.ncomp; c++)
             for (int t = 0; t < S.nr; t++) {
                 float *dst = allrcv + ((size_t)c * nr + t) * nt;
                 const float *src = &out[((size_t)c * S.nr + t) * nt];
@@ -1798,7 +1799,7 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
         if (store) store_host_snapshots(ctx, full_wfld);
     } else {
         load_host_snapshots(ctx, full_wfld);
-        std::vector<float> g((size_t)3 * nx * nz);
+        std::vector<float> g((size_t)P.ncompg * nx * nz);
         upload_traces(ctx, in.data(), true);
         run(ctx, true, false);
         download_grad(ctx, g.data());

@@ -136,5 +136,5 @@ def test_autograd_function_backward_is_device_gradient():
     phi.backward()
     grad, phi_ref = _grad(P, kind, g, g["start"], g["obs"])
     P.close()
-    assert abs(float(phi) - phi_ref) <= 1e-12 * max(1.0, abs(phi_ref))
+    assert abs(phi.item() - phi_ref) <= 1e-12 * max(1.0, abs(phi_ref))
     assert np.array_equal(m.grad.numpy(), grad)

@@ -109,14 +109,16 @@ def test_acoustic_forward_adjoint_vs_oracle(bc, shape, grid):
         assert K.rel_l2(g_g[c], g_o[c]) <= GRAD_TOL, "gradient component %d" % c
 
 
-def test_dropin_propagate_matches_oracle():
+@pytest.mark.parametrize("kind", [O.KIND_ELASTIC, O.KIND_ACOUSTIC])
+def test_dropin_propagate_matches_oracle(kind):
     """fwi2d_propagate: the propagate_gpu drop-in with the reference's buffers."""
     import ctypes
-    kind, nx, nz, d, nt = O.KIND_ELASTIC, 64, 48, 0.01, 150
+    nx, nz, d, nt = 64, 48, 0.01, 150
+    nc = 1 if kind == O.KIND_ACOUSTIC else 2
     mc = K.converted(kind, K.model_case(kind, nx, nz, d, seed=5))
     sl, rl = K.geometry(nx, nz, d, nr=16)
     pd = K.par_dict(nt=nt, dt=1e-3)
-    src = K.sources(2, nt, 1e-3)
+    src = K.sources(nc, nt, 1e-3)
     port = O.Port(32)
     par = O.make_par(**pd, ns=1, nr=16)
     rcv_o, full_o = K.oracle_forward(port, kind, mc, src, par, nx, nz, d, sl, rl)
@@ -130,14 +132,14 @@ def test_dropin_propagate_matches_oracle():
     ji = C.Injector(0, 1, C.ptr(inj[0]), C.ptr(inj[1]), C.ptr(inj[2]), C.ptr(inj[3]))
     je = C.Injector(0, 16, C.ptr(ext[0]), C.ptr(ext[1]), C.ptr(ext[2]), C.ptr(ext[3]))
     params = F.make_params(**pd)
-    rcv = np.zeros((2, 16, nt), np.float32)
+    rcv = np.zeros((nc, 16, nt), np.float32)
     full = np.zeros_like(full_o)
-    C.check(L.fwi2d_propagate(0, 0, C.ptr(mc), C.ptr(np.ascontiguousarray(src)), C.ptr(rcv), ctypes.byref(ji),
+    C.check(L.fwi2d_propagate(kind, 0, C.ptr(mc), C.ptr(np.ascontiguousarray(src)), C.ptr(rcv), ctypes.byref(ji),
                               ctypes.byref(je), None, None, C.ptr(full), None, ctypes.byref(params), 1, 16, nx, nz, d, d))
     assert K.rel_l2(rcv, rcv_o) <= TRACE_TOL
     assert K.rel_l2(full, full_o) <= TRACE_TOL
-    g = np.zeros((3, nx, nz), np.float32)
-    dummy = np.zeros((2, 1, nt), np.float32)
-    C.check(L.fwi2d_propagate(0, 1, C.ptr(mc), C.ptr(adj), C.ptr(dummy), ctypes.byref(je), ctypes.byref(ji),
+    g = np.zeros((2 if kind == O.KIND_ACOUSTIC else 3, nx, nz), np.float32)
+    dummy = np.zeros((nc, 1, nt), np.float32)
+    C.check(L.fwi2d_propagate(kind, 1, C.ptr(mc), C.ptr(adj), C.ptr(dummy), ctypes.byref(je), ctypes.byref(ji),
                               None, None, C.ptr(full), C.ptr(g), ctypes.byref(params), 1, 16, nx, nz, d, d))
     assert K.rel_l2(g, g_o) <= GRAD_TOL
