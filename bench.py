@@ -62,12 +62,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch():
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f)
-    except Exception:
-        return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the adjoint tile kernel on the single-shot grid, from the ncu capture
+# summarised in profiles/elastic_step_adjoint_single_shot_401x801.md
+# (cold caches: ncu flushes L2 before each pass).
+ADJ_TILE_TRAFFIC_BYTES = 21.730304e6
 
 
 # ---------------------------------------------------------------------------
@@ -300,12 +299,14 @@ def run_ours(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     barrier()
+    torch.cuda.nvtx.range_push("timed")
     with torch.cuda.stream(stream):
         ev0.record(stream)
         for _ in range(args.steps):
             grad_step()
         ev1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier()
     ms = ev0.elapsed_time(ev1)
     fwd_ms, adj_ms = P.last_timing()
@@ -365,7 +366,6 @@ def run_ours(args):
     fwd_launch_s = fwd_ms / 1e3 / steps_adj
     achieved = BYTES_ADJ * cells_launch / adj_launch_s / 1e9
     peak, peak_kind = peaks()
-    tr = traffic_per_launch()
     launches = (info["launches_forward"] + info["launches_adjoint"] + 2 * nshots_rank + 1) * args.steps
     if rank == 0:
         h2d = model_h.nbytes + src_h.nbytes + obs_h.nbytes
@@ -387,7 +387,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "elastic_step (adjoint + imaging)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": (tr or {}).get("adjoint_bytes_per_launch"),
+                         "traffic": ADJ_TILE_TRAFFIC_BYTES if args.config == "single" else None,
                          "algorithmic_bytes_per_launch": BYTES_ADJ * cells_launch,
                          "launch_ms": adj_launch_s * 1e3,
                          "forward_launch_ms": fwd_launch_s * 1e3,

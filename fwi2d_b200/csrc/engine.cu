@@ -206,7 +206,8 @@ struct ShotPlan {
     int ncomp = 2;                 // field components
     int ncomp_src = 2, ntr_src = 0, nr = 0;
     int nsrc_rows = 0, nrcv_rows = 0;
-    int nslot = 0;
+    int nslot = 0;                 // snapshot time slots of the shot (1 + nt/sub)
+    int nbuf = 0;                  // slots held on the device (nslot, or the replay window)
     std::vector<InjEntry> inj_f, inj_a;
     std::vector<int> inj_f_off, inj_a_off, inj_f_roff, inj_a_roff;
     std::vector<ExtEntry> ext_f;
@@ -216,6 +217,7 @@ struct ShotPlan {
     DevBuf d_inj_f, d_inj_f_off, d_inj_a, d_inj_a_off, d_ext_f, d_ext_f_off, d_ext_none_off;
     DevBuf d_mrow_f, d_mrow_a;
     DevBuf den, tz, tx, snap, amax, grad, gwt;
+    DevBuf r0, r1, ckpt;           // checkpoint-and-recompute: replay fields and checkpoints
 };
 
 struct Plan {
@@ -232,6 +234,12 @@ struct Plan {
     std::vector<MarchRef> marches;
     std::vector<BandRef> bands;
     DevBuf d_tiles, d_march, d_bands, d_shots_f, d_shots_a;
+    // checkpoint-and-recompute: every `ckpt` steps; cuts[k] is the first
+    // imaging time of segment k (cuts.back() = nt - 1); per-segment shot
+    // tables of the replay (forward with snapshot store) and of the adjoint
+    int ckpt = 0;
+    std::vector<int> cuts;
+    DevBuf d_shots_r, d_shots_c;
     // initial-state cells per mode (0 forward, 1 adjoint)
     std::vector<InitCell> icells[2];
     std::vector<int> ioff[2], iidx[2];
@@ -809,7 +817,14 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     if (M.kind == KIND_AE) throw Error(FWI2D_ERR_UNSUPPORTED, "this propagator is not built yet");
     const bool acoustic = M.kind == KIND_ACOUSTIC;
     REQ(!(acoustic && p.mt), "the acoustic propagator takes point sources only (mt = 0)");
-    REQ(p.checkpoint_every == 0, "checkpointing is not available in this build");
+    REQ(p.checkpoint_every >= 0, "checkpoint_every must be >= 0");
+    if (p.checkpoint_every > 0) {
+        REQ(p.sub == 1, "checkpoint-and-recompute needs sub = 1");
+        for (int s = 1; s < nshots; s++)
+            if (shots[s].nt != shots[0].nt)
+                throw Error(FWI2D_ERR_UNSUPPORTED,
+                            "checkpoint-and-recompute needs every shot of the plan to have the same nt");
+    }
     set_device(ctx);
 
     auto P = std::make_unique<Plan>();
@@ -942,9 +957,19 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->grad.alloc((size_t)P->ncompg * sh.nx * M.ldz * sizeof(float));
         if (S->nslot > 0) {
             const size_t esz = p.snapshot_precision == FWI2D_SNAP_FP32 ? 4 : 2;
-            const size_t bytes = (size_t)S->nslot * field * esz;
+            const int K = p.checkpoint_every;
+            // checkpointing: a replay window of K + 2 slots (times cuts[k]-1 .. cuts[k+1])
+            S->nbuf = K > 0 ? std::min(S->nslot, K + 2) : S->nslot;
+            size_t bytes = (size_t)S->nbuf * field * esz;
             S->snap.alloc(bytes);
             S->amax.alloc((size_t)S->nslot * sizeof(unsigned));
+            if (K > 0) {
+                const int nseg = (sh.nt - 1 + K - 1) / K;
+                S->r0.alloc(field * sizeof(float));
+                S->r1.alloc(field * sizeof(float));
+                if (nseg > 1) S->ckpt.alloc((size_t)(nseg - 1) * 2 * field * sizeof(float));
+                bytes += S->r0.n + S->r1.n + S->ckpt.n;
+            }
             P->snap_bytes += bytes;
             total_bytes += bytes;
         }
@@ -963,8 +988,41 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         shot_dev(*P, *P->shots[s], M, false, sf[s]);
         shot_dev(*P, *P->shots[s], M, true, sa[s]);
     }
+    for (int s = 0; s < nshots; s++) sf[s].ckpt = P->shots[s]->ckpt.as<float>();
     P->d_shots_f.upload(sf, ctx->st);
     P->d_shots_a.upload(sa, ctx->st);
+    if (p.checkpoint_every > 0) {
+        const int K = p.checkpoint_every, nt = P->nt_max;
+        P->ckpt = K;
+        P->cuts.clear();
+        for (int t = 0; t < nt - 1; t += K) P->cuts.push_back(t);
+        P->cuts.push_back(nt - 1);
+        const int nseg = (int)P->cuts.size() - 1;
+        const size_t esz = p.snapshot_precision == FWI2D_SNAP_FP32 ? 4 : 2;
+        std::vector<ShotDev> sr((size_t)nseg * nshots), sc((size_t)nseg * nshots);
+        for (int k = 0; k < nseg; k++) {
+            // slot t of segment k lives at window index t - base (base = cuts[k] - 1, or -1 for
+            // segment 0): the tables carry the window's address shifted by -base slots, so the
+            // kernels index it with the absolute time; only slots of the window are accessed
+            const long long base = k == 0 ? -1 : P->cuts[k] - 1;
+            for (int s = 0; s < nshots; s++) {
+                ShotPlan &S = *P->shots[s];
+                char *win = (char *)S.snap.p - base * (long long)sf[s].snap_slot * (long long)esz;
+                ShotDev r = sf[s];
+                r.u[0] = S.r0.as<float>();
+                r.u[1] = S.r1.as<float>();
+                r.rcv = nullptr;
+                r.nrcv = 0;
+                r.snap = win;
+                ShotDev a = sa[s];
+                a.snap = win;
+                sr[(size_t)k * nshots + s] = r;
+                sc[(size_t)k * nshots + s] = a;
+            }
+        }
+        P->d_shots_r.upload(sr, ctx->st);
+        P->d_shots_c.upload(sc, ctx->st);
+    }
     build_init_cells(M, *P);
     upload_init_cells(*P, ctx->st);
     P->d_grad_full.alloc((size_t)P->ncompg * M.nx * M.ldz * sizeof(float));
@@ -1058,6 +1116,7 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
                 fwi2d_params q = p;
                 q.tile_shape = s;
                 q.sub = 0;
+                q.checkpoint_every = 0;
                 try {
                     set_shots_impl(ctx, &q, nshots, shots);
                 } catch (const Error &e) {
@@ -1076,6 +1135,71 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
         p.tile_shape = chosen;
     }
     set_shots_impl(ctx, &p, nshots, shots);
+}
+
+// Checkpoint-and-recompute time loops (all shots share nt, sub = 1).
+// Forward: receivers and 16-bit snapshot scales as usual, no snapshot store;
+// before launch cuts[k] - 1 (k >= 1) both field buffers of every shot are
+// saved as checkpoint k - 1.  Adjoint: segments k = last .. 0, each a replay
+// of launches cuts[k] - 1 .. cuts[k+1] - 1 from checkpoint k - 1 (segment 0
+// from the initial state) on separate fields, storing the snapshots of times
+// cuts[k] - 1 .. cuts[k+1] into the replay window, then the adjoint launches
+// whose imaging times fall in [cuts[k], cuts[k+1]).  The replay repeats the
+// forward launches exactly, so the gradient equals the stored-snapshot one.
+static long long capture_checkpointed(fwi2d_ctx *ctx, Plan &P, bool adj, cudaStream_t cst)
+{
+    const ModelDev md = ctx->M.dev();
+    const int nshots = (int)P.shots.size();
+    const int ncomp = P.kind == KIND_ACOUSTIC ? 1 : 2;
+    const int nt = P.nt_max, nseg = (int)P.cuts.size() - 1;
+    long long n = 0;
+    if (!adj) {
+        const ShotDev *shots = P.d_shots_f.as<ShotDev>();
+        int flags = STEP_EXTRACT;
+        if (P.par.snapshot_precision != FWI2D_SNAP_FP32) flags |= STEP_AMAX;
+        int kn = 1;
+        for (int it = 0; it < nt - 1; it++) {
+            if (kn < nseg && it == P.cuts[kn] - 1) {
+                launch_checkpoint(shots, nshots, ncomp, kn - 1, false, cst);
+                n++;
+                kn++;
+            }
+            n += launch_step(ctx, P, shots, md, it, flags, cst);
+        }
+        launch_finalize(shots, nshots, P.C, ncomp, STEP_EXTRACT, cst);
+        return n + 1;
+    }
+    // acoustic imaging at launch it uses time nt-1-it, the elastic one nt-2-it
+    const int a = P.kind == KIND_ACOUSTIC ? 1 : 0;
+    const ShotDev *last_adj = nullptr;
+    for (int k = nseg - 1; k >= 0; k--) {
+        const ShotDev *rs = P.d_shots_r.as<ShotDev>() + (size_t)k * nshots;
+        const ShotDev *as = P.d_shots_c.as<ShotDev>() + (size_t)k * nshots;
+        if (k == 0) {
+            for (auto &S : P.shots) {
+                CK(cudaMemsetAsync(S->r0.p, 0, S->r0.n, cst));
+                CK(cudaMemsetAsync(S->r1.p, 0, S->r1.n, cst));
+            }
+            launch_init_state(rs, nshots, P.d_icells[0].as<InitCell>(), P.d_ioff[0].as<int>(),
+                              P.d_iidx[0].as<int>(), cst);
+        } else {
+            launch_checkpoint(rs, nshots, ncomp, k - 1, true, cst);
+        }
+        n++;
+        const int t0 = k == 0 ? 0 : P.cuts[k] - 1, t1 = P.cuts[k + 1];
+        for (int it = t0; it < t1; it++) n += launch_step(ctx, P, rs, md, it, STEP_STORE, cst);
+        launch_finalize(rs, nshots, P.C, ncomp, STEP_STORE, cst, t1);
+        n++;
+        const int lo = k == nseg - 1 ? 0 : nt - 1 - P.cuts[k + 1] + a;
+        const int hi = k == 0 ? nt - 2 : nt - 2 - P.cuts[k] + a;
+        for (int it = lo; it <= hi; it++) n += launch_step(ctx, P, as, md, it, STEP_GRAD, cst);
+        last_adj = as;
+    }
+    if (P.kind == KIND_ACOUSTIC) {
+        launch_acoustic_final_grad(last_adj, nshots, md, P.C, P.dtg, cst);
+        n++;
+    }
+    return n;
 }
 
 static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
@@ -1111,14 +1235,18 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
         }
     }
     const ModelDev md = M.dev();
-    for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(ctx, P, shots, md, it, flags, cst);
-    if (!adj) {
-        launch_finalize(shots, nshots, P.C, P.kind == KIND_ACOUSTIC ? 1 : 2, STEP_EXTRACT | (store ? STEP_STORE : 0),
-                        cst);
-        n++;
-    } else if (P.kind == KIND_ACOUSTIC) {
-        launch_acoustic_final_grad(shots, nshots, md, P.C, P.dtg, cst);   // snapshot 0 with the last adjoint field
-        n++;
+    const int ncomp = P.kind == KIND_ACOUSTIC ? 1 : 2;
+    if (P.ckpt > 0 && (store || adj)) {
+        n += capture_checkpointed(ctx, P, adj, cst);
+    } else {
+        for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(ctx, P, shots, md, it, flags, cst);
+        if (!adj) {
+            launch_finalize(shots, nshots, P.C, ncomp, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
+            n++;
+        } else if (P.kind == KIND_ACOUSTIC) {
+            launch_acoustic_final_grad(shots, nshots, md, P.C, P.dtg, cst);   // snapshot 0 with the last adjoint field
+            n++;
+        }
     }
     CK(cudaGetLastError());
     CK(cudaStreamEndCapture(cst, &g));
@@ -1597,6 +1725,7 @@ int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out)
     REQ(shot >= 0 && shot < (int)P.shots.size(), "no such shot");
     ShotPlan &S = *P.shots[shot];
     REQ(P.have_snapshots && slot >= 0 && slot < S.nslot, "no such snapshot");
+    REQ(P.ckpt == 0, "snapshots are recomputed segment by segment under checkpointing and are not kept");
     set_device(ctx);
     const ModelState &M = ctx->M;
     const size_t field = (size_t)S.ncomp * S.nx * M.ldz;
@@ -1650,8 +1779,12 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     Plan &P = need_plan(ctx);
     const long long steps = P.nt_max - 1;
     const long long per = P.marches.empty() ? 1 : 3;
-    if (lf) *lf = steps * per + 2;
-    if (la) *la = steps * per + 1 + (long long)P.shots.size();
+    const long long nseg = P.ckpt > 0 ? (long long)P.cuts.size() - 1 : 0;
+    const long long acf = P.kind == KIND_ACOUSTIC ? 1 : 0;
+    // forward: init, steps, last sample (+ checkpoint copies); adjoint: init, steps,
+    // acoustic final imaging, per-shot scatter (+ replays: restore, steps, last snapshot)
+    if (lf) *lf = steps * per + 2 + (nseg > 0 ? nseg - 1 : 0);
+    if (la) *la = steps * per + 1 + acf + (long long)P.shots.size() + (nseg > 0 ? (steps + nseg - 1) * per + 2 * nseg : 0);
     if (shape) *shape = P.shape;
     if (snap_bytes) *snap_bytes = P.snap_bytes;
     ABI_END

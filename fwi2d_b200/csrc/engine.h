@@ -72,6 +72,7 @@ struct ShotDev {
     float *gcomp;         // compensation terms (compensated accumulation) or nullptr
     float *halo_save;     // interface scratch (acoustic-elastic) or nullptr
     const float *gwt;     // gradient time-damping weight per snapshot index
+    float *ckpt;          // checkpoints [k][2][ncomp][nx][ldz] (checkpoint-and-recompute) or nullptr
 };
 
 // Model on the full grid; shots index it at column x0 + ix.

@@ -723,12 +723,15 @@ __global__ void init_state(const ShotDev *__restrict__ shots, int nshots, const 
 // Last sample: receivers and the final snapshot (we_op.cpp:874-881).
 // One CTA per shot.
 // ---------------------------------------------------------------------------
-__global__ void finalize_shots(const ShotDev *__restrict__ shots, int nshots, StepConst C, int ncomp, int flags)
+__global__ void finalize_shots(const ShotDev *__restrict__ shots, int nshots, StepConst C, int ncomp, int flags,
+                               int t_store)
 {
     const int s = blockIdx.y;
     if (s >= nshots) return;
     const ShotDev &S = shots[s];
-    const int it = S.nt - 1;
+    // t_store >= 0: the field of that time sample (curr after launch t_store-1)
+    const int it = t_store >= 0 ? t_store : S.nt - 1;
+    if (it > S.nt - 1) return;
     const float *curr = S.u[(it + 1) & 1];
     const long long nxz = (long long)S.nx * S.ldz;
     if (flags & F_EXTRACT) {
@@ -749,6 +752,29 @@ __global__ void finalize_shots(const ShotDev *__restrict__ shots, int nshots, St
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
             const long long rem = i % S.ldz;
             if (rem < S.nz) snap_store(S.snap, (long long)slot * S.snap_slot + i, C.snap_prec, curr[i], sc);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoints of the time loop: both field buffers of every shot (the state
+// before a given launch: prev and curr) copied to (restore = 0) or from
+// (restore = 1) checkpoint k of the shot's store [k][2][ncomp][nx][ldz].
+// ---------------------------------------------------------------------------
+__global__ void checkpoint_fields(const ShotDev *__restrict__ shots, int nshots, int ncomp, int k, int restore)
+{
+    const int s = blockIdx.y;
+    if (s >= nshots) return;
+    const ShotDev &S = shots[s];
+    const long long n4 = (long long)ncomp * S.nx * S.ldz / 4;   // ldz is a multiple of 32
+    float4 *ck = reinterpret_cast<float4 *>(S.ckpt) + (long long)k * 2 * n4;
+    for (int b = 0; b < 2; b++) {
+        float4 *u = reinterpret_cast<float4 *>(S.u[b]);
+        float4 *c = ck + b * n4;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+             i += (long long)gridDim.x * blockDim.x) {
+            if (restore) u[i] = c[i];
+            else c[i] = u[i];
         }
     }
 }
@@ -919,10 +945,17 @@ void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, 
     init_state<<<nshots, 128, 0, st>>>(shots, nshots, cells, off, idx);
 }
 
-void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st)
+void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st,
+                     int t_store)
 {
     dim3 grid(148, nshots);
-    finalize_shots<<<grid, 256, 0, st>>>(shots, nshots, C, ncomp, flags);
+    finalize_shots<<<grid, 256, 0, st>>>(shots, nshots, C, ncomp, flags, t_store);
+}
+
+void launch_checkpoint(const ShotDev *shots, int nshots, int ncomp, int k, bool restore, cudaStream_t st)
+{
+    dim3 grid(148, nshots);
+    checkpoint_fields<<<grid, 256, 0, st>>>(shots, nshots, ncomp, k, restore ? 1 : 0);
 }
 
 void launch_vti_grad_coefs(int n, const float *lam, const float *mu, const float *c13, float *v2, float *v3, cudaStream_t st)

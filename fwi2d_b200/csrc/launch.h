@@ -24,7 +24,12 @@ void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const Shot
                           const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
                        cudaStream_t st);
-void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st);
+// Receivers of the last sample and its snapshot (t_store < 0), or only the
+// snapshot of time sample t_store (flags = STEP_STORE).
+void launch_finalize(const ShotDev *shots, int nshots, const StepConst &C, int ncomp, int flags, cudaStream_t st,
+                     int t_store = -1);
+// Copy both field buffers of every shot to / from checkpoint k (ShotDev::ckpt).
+void launch_checkpoint(const ShotDev *shots, int nshots, int ncomp, int k, bool restore, cudaStream_t st);
 
 // acoustic kernel (acoustic.cuh): tile shapes 2 and 3 only
 bool acoustic_shape_ok(int shape);

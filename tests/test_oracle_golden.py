@@ -15,7 +15,8 @@ import oracle as O
 from tests import cases as K
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-FILES = sorted(glob.glob(os.path.join(GOLD, "*.npz")))
+FILES = sorted(f for f in glob.glob(os.path.join(GOLD, "*.npz")) if not os.path.basename(f).startswith("fwi_gradient_"))
+FWI_FILES = sorted(glob.glob(os.path.join(GOLD, "fwi_gradient_*.npz")))
 
 
 def test_golden_fixtures_present():
@@ -72,3 +73,20 @@ def test_fp32_vs_fp64_distance_is_small():
     b = dict(np.load(os.path.join(GOLD, "elastic_fs_abs_f64.npz")))
     assert K.rel_l2(a["rcv"], b["rcv"]) < 1e-4
     assert K.rel_l2(a["grad"], b["grad"]) < 1e-3
+
+
+@pytest.mark.parametrize("path", FWI_FILES, ids=[os.path.basename(f) for f in FWI_FILES])
+def test_fwi_gradient_fixture_reproduced_by_reference_build(path):
+    """The FWI gradient fixtures (the reference solver's misfit gradient on a
+    100 x 80 grid) are reproduced by the reference build in oracle/_ref."""
+    if not O.have_reference(32):
+        pytest.skip("oracle/_ref is not built")
+    g = dict(np.load(path))
+    lib = O.Reference(32)
+    kind, nx, nz, d, nt, dt = int(g["kind"]), int(g["nx"]), int(g["nz"]), float(g["d"]), int(g["nt"]), float(g["dt"])
+    par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=len(g["rx"]))
+    geo = ((np.float32(g["sx"]), np.float32(g["sz"])), (g["rx"], g["rz"]))
+    syn, _ = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], g["true"], g["src"])
+    assert np.array_equal(syn, g["obs"])
+    _, grad = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], g["start"], g["src"], g["obs"])
+    assert np.array_equal(grad, g["grad"])
