@@ -466,6 +466,9 @@ def run_batched(local, steps, warmup):
 
 def main():
     args = parse()
+    # autotuner choices persist across the runs of one machine (a run under a
+    # profiler then reuses the shape measured without it)
+    os.environ.setdefault("FWI2D_TUNE_FILE", os.path.join(tempfile.gettempdir(), "fwi2d_b200_tune.txt"))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -245,7 +246,7 @@ struct Plan {
     std::vector<int> ioff[2], iidx[2];
     DevBuf d_icells[2], d_ioff[2], d_iidx[2];
     // FWI gradient: observed data, misfit partial sums
-    DevBuf d_obs, d_misfit;
+    DevBuf d_obs, d_misfit, d_part;
     DevBuf d_grad_full, d_stage;
     StepConst C;
     float dtg = 0;
@@ -1092,6 +1093,45 @@ static float time_forward_steps(fwi2d_ctx *ctx, int steps)
     return ms / std::max(nsteps, 1);
 }
 
+// Autotuner choices also persist across processes in the file named by the
+// environment variable FWI2D_TUNE_FILE (lines "<key> <shape>"), keyed by the
+// library build and the device, so that a later run -- for instance one under
+// a profiler, whose serialised launches would skew the timing -- reuses the
+// measured choice.
+static std::string tune_build_key(int device)
+{
+    cudaDeviceProp pr;
+    CK(cudaGetDeviceProperties(&pr, device));
+    std::string k = std::string(__DATE__ "_" __TIME__) + "/" + pr.name + "/" + std::to_string(pr.multiProcessorCount);
+    for (auto &c : k)
+        if (c == ' ') c = '_';
+    return k;
+}
+
+static int tune_file_lookup(const std::string &key)
+{
+    const char *path = std::getenv("FWI2D_TUNE_FILE");
+    if (!path || !*path) return -1;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return -1;
+    char k[1024];
+    int v, found = -1;
+    while (std::fscanf(f, "%1023s %d", k, &v) == 2)
+        if (key == k) found = v;
+    std::fclose(f);
+    return found;
+}
+
+static void tune_file_store(const std::string &key, int shape)
+{
+    const char *path = std::getenv("FWI2D_TUNE_FILE");
+    if (!path || !*path || key.size() >= 1024) return;
+    FILE *f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d\n", key.c_str(), shape);
+    std::fclose(f);
+}
+
 // Tile-shape autotuner: for plans that leave the shape open (tile_shape < 0),
 // time a few forward steps of every shape that tiles the grids and keep the
 // fastest.  The choice is cached per (kind, nz, shot grid widths).
@@ -1101,7 +1141,8 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
     fwi2d_params p = *par;
     if (p.tile_shape < 0 && ctx->M.kind >= 0) {
         static std::vector<std::pair<std::string, int>> cache;
-        std::string key = std::to_string(ctx->M.kind) + "/" + std::to_string(ctx->M.nz) + "/" + std::to_string(nshots);
+        std::string key = tune_build_key(ctx->device) + "/" + std::to_string(ctx->M.kind) + "/" +
+                          std::to_string(ctx->M.nz) + "/" + std::to_string(nshots);
         long long cells = 0;
         for (int i = 0; i < nshots; i++) {
             key += "/" + std::to_string(shots[i].nx);
@@ -1110,6 +1151,11 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
         int chosen = -1;
         for (auto &kv : cache)
             if (kv.first == key) chosen = kv.second;
+        if (chosen < 0 && cells >= 20000000LL) {
+            chosen = tune_file_lookup(key);
+            if (chosen >= shape_count()) chosen = -1;
+            if (chosen >= 0) cache.emplace_back(key, chosen);
+        }
         if (chosen < 0 && cells >= 20000000LL) {
             float best = 1e30f;
             for (int s = 0; s < shape_count(); s++) {
@@ -1130,7 +1176,10 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
                 }
             }
             ctx->plan.reset();
-            if (chosen >= 0) cache.emplace_back(key, chosen);
+            if (chosen >= 0) {
+                cache.emplace_back(key, chosen);
+                tune_file_store(key, chosen);
+            }
         }
         p.tile_shape = chosen;
     }
@@ -1356,17 +1405,23 @@ static void download_grad(fwi2d_ctx *ctx, float *grad)
 // adjoint-source preparation of we_op.cpp:1108-1134)
 // ---------------------------------------------------------------------------
 
-// Per trace: synthetic data (Dt of the extracted displacement when
-// seismotype = 1, misc.cpp:71-84), residual r = syn - obs, the trace's misfit
-// sum(r^2) - (r_0^2 + r_{nt-1}^2)/2 (compensated), and the adjoint source
+// Per trace sample (row r, time t; one thread per row and chunk of kResChunk
+// samples): synthetic data (Dt of the extracted displacement when
+// seismotype = 1, misc.cpp:71-84), residual r = syn - obs, the chunk's part
+// of the trace misfit sum(r^2) - (r_0^2 + r_{nt-1}^2)/2 (Neumaier summation),
+// and the adjoint source
 //   q[t] = -r[nt-1-t]  (Ht^-1 of the caller's Ht r, reversed, scaled by -1),
 //   then Dt^T (misc.cpp:85-94) when seismotype = 1.
+// k_misfit_rows adds the chunk partials of each trace in double.
+constexpr int kResChunk = 64;
+
 __global__ void k_residual(const float *__restrict__ u, const float *__restrict__ obs, float *__restrict__ adj,
-                           float *__restrict__ syn_out, double *__restrict__ misfit, int nt, int rows, float dt,
+                           float *__restrict__ syn_out, float2 *__restrict__ part, int nt, int rows, float dt,
                            int seismotype)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
+    const int t0 = blockIdx.y * kResChunk, t1 = min(nt, t0 + kResChunk);
     auto U = [&](int t) { return u[(long long)t * rows + r]; };
     auto syn = [&](int t) -> float {
         if (!seismotype) return U(t);
@@ -1375,9 +1430,8 @@ __global__ void k_residual(const float *__restrict__ u, const float *__restrict_
         return (U(t + 1) - U(t - 1)) / (2 * dt);
     };
     auto res = [&](int t) { return syn(t) - obs[(long long)t * rows + r]; };
-    // misfit with Neumaier summation
     float sum = 0.f, comp = 0.f;
-    for (int t = 0; t < nt; t++) {
+    for (int t = t0; t < t1; t++) {
         const float rv = res(t);
         float term = rv * rv;
         if (t == 0 || t == nt - 1) term = 0.5f * term;
@@ -1387,9 +1441,9 @@ __global__ void k_residual(const float *__restrict__ u, const float *__restrict_
         sum = y;
         if (syn_out) syn_out[(long long)t * rows + r] = syn(t);
     }
-    misfit[r] = (double)sum + (double)comp;
+    part[(long long)blockIdx.y * rows + r] = make_float2(sum, comp);
     auto q = [&](int t) { return -res(nt - 1 - t); };
-    for (int t = 0; t < nt; t++) {
+    for (int t = t0; t < t1; t++) {
         float a;
         if (!seismotype) a = q(t);
         else if (t == 0) a = (q(1) + q(0)) / dt;
@@ -1397,6 +1451,18 @@ __global__ void k_residual(const float *__restrict__ u, const float *__restrict_
         else a = (q(t + 1) - q(t - 1)) / (2 * dt);
         adj[(long long)t * rows + r] = a;
     }
+}
+
+__global__ void k_misfit_rows(const float2 *__restrict__ part, double *__restrict__ misfit, int rows, int nchunk)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    double m = 0.0;
+    for (int c = 0; c < nchunk; c++) {
+        const float2 p = part[(long long)c * rows + r];
+        m += (double)p.x + (double)p.y;
+    }
+    misfit[r] = m;
 }
 
 // H quadrature (spatial_operators.cpp:6-98) and the chain rule from
@@ -1465,11 +1531,21 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
     size_t rows_total = 0;
     for (auto &S : P.shots) rows_total += S->nrcv_rows;
     P.d_misfit.ensure(std::max<size_t>(rows_total, 1) * sizeof(double));
+    size_t part_max = 1;
+    for (auto &S : P.shots)
+        part_max = std::max(part_max, (size_t)((S->nt + kResChunk - 1) / kResChunk) * S->nrcv_rows);
+    // the shots share one partial buffer: their kernels run in stream order and
+    // each shot reduces its partials before the next shot writes them
+    P.d_part.ensure(part_max * sizeof(float2));
     size_t obs_off = 0, row_off = 0;
     for (auto &S : P.shots) {
-        k_residual<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
-            S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off, S->src_a.as<float>(), nullptr,
-            P.d_misfit.as<double>() + row_off, S->nt, S->nrcv_rows, P.par.dt, seismotype);
+        const int nchunk = (S->nt + kResChunk - 1) / kResChunk;
+        dim3 grid((S->nrcv_rows + 127) / 128, nchunk);
+        k_residual<<<grid, 128, 0, ctx->st>>>(S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off,
+                                              S->src_a.as<float>(), nullptr, P.d_part.as<float2>(), S->nt,
+                                              S->nrcv_rows, P.par.dt, seismotype);
+        k_misfit_rows<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
+            P.d_part.as<float2>(), P.d_misfit.as<double>() + row_off, S->nrcv_rows, nchunk);
         CK(cudaGetLastError());
         obs_off += (size_t)S->nt * S->nrcv_rows;
         row_off += S->nrcv_rows;

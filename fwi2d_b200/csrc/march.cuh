@@ -145,8 +145,10 @@ __device__ __forceinline__ float srow(const float *buf, int idx, int prec, float
     return __half2float(reinterpret_cast<const __half *>(buf)[idx]) * inv;
 }
 
-__device__ __forceinline__ void add_sources(const InjEntry *__restrict__ inj, const float *__restrict__ srcrow, int e0,
-                                            int e1, int gz, float &n0, float &n1)
+// Rare per-row paths (rows holding a source or a receiver pivot) are kept
+// out of line, so that the unrolled step bodies stay small.
+__device__ __noinline__ void add_sources(const InjEntry *__restrict__ inj, const float *__restrict__ srcrow, int e0,
+                                         int e1, int gz, float &n0, float &n1)
 {
     for (int e = e0; e < e1; e++) {
         const InjEntry &E = inj[e];
@@ -155,6 +157,27 @@ __device__ __forceinline__ void add_sources(const InjEntry *__restrict__ inj, co
             if (E.comp == 0) n0 += v;
             else n1 += v;
         }
+    }
+}
+
+// Receivers of one row: entries [r0, r1), 3x3 weights over the curr rows
+// j-1 .. j+1 of the rings (slots P+7, P, P+1).
+__device__ __noinline__ void march_extract(const ExtEntry *__restrict__ ext, float *__restrict__ rcvrow,
+                                           const float *rux, const float *ruz, int RB, int P, int s0, int r0, int r1,
+                                           int nth)
+{
+    for (int e = r0 + (int)threadIdx.x; e < r1; e += nth) {
+        const ExtEntry &E = ext[e];
+        const float *Rb = E.comp == 0 ? rux : ruz;
+        const int zi = E.gz0 - s0;
+        float o = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float *row = Rb + ((P + 7 + a) & 7) * RB + zi;
+#pragma unroll
+            for (int b = 0; b < 3; b++) o += E.w[a * 3 + b] * row[b];
+        }
+        rcvrow[E.row] = o;
     }
 }
 
@@ -379,21 +402,9 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
         }
 
         // receivers whose pivot lies on this row: curr rows j-1 .. j+1 are in the rings
-        if (X.extract) {
-            for (int e = R.r0 + (int)threadIdx.x; e < R.r1; e += NTH) {
-                const ExtEntry &E = S.ext[e];
-                const float *Rb = sm + (E.comp == 0 ? L::UX : L::UZ);
-                const int zi = E.gz0 - X.s0;
-                float o = 0.f;
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    const float *row = Rb + ((P + 7 + a) & 7) * RB + zi;
-#pragma unroll
-                    for (int b = 0; b < 3; b++) o += E.w[a * 3 + b] * row[b];
-                }
-                S.rcv[(long long)X.it * S.nrcv + E.row] = o;
-            }
-        }
+        if (X.extract && R.r0 < R.r1)
+            march_extract(S.ext, S.rcv + (long long)X.it * S.nrcv, sm + L::UX, sm + L::UZ, RB, P, X.s0, R.r0, R.r1,
+                          NTH);
 
         // zero-lag imaging condition (we_op.cpp:505-562, VTI :1478-1557)
         if (GRAD && X.do_grad && X.own) {
@@ -472,6 +483,10 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
     }
     return true;
 }
+
+#ifndef MARCH_ROLLED_GRAD
+#define MARCH_ROLLED_GRAD 0
+#endif
 
 template <bool VTI, bool GRAD, int NTH>
 __global__ void __launch_bounds__(NTH, (GRAD || NTH > 224) ? 2 : 3)
@@ -560,7 +575,7 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
 
     const int j0 = U.xb - 10;
     bool ok = true;
-    if (GRAD) {
+    if (GRAD && MARCH_ROLLED_GRAD) {
         for (int j = j0; j < U.xe; j++) {
             ok = march_step<VTI, GRAD, NTH, -1>(Q, X, smem, S, M, C, j, j0);
             if (!ok) break;
