@@ -45,7 +45,11 @@ __device__ __forceinline__ float asat_cell(float n, int side, int bc, int k, con
     return n;
 }
 
-template <int TX, bool GRAD>
+// AE: the fluid layer of the acoustic-elastic propagator (we_op.cpp:2137-2577):
+// the bottom edge is the interface (Neumann SAT, C.bc[1] = 3) applied after
+// the left and right sides, and the interface row is left untapered, with its
+// prev saved in halo_save, for ae_couple.
+template <int TX, bool GRAD, bool AE>
 __global__ void __launch_bounds__(32 * TX)
 acoustic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C, int it,
               int flags, float dtg)
@@ -165,11 +169,13 @@ acoustic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
         if (it > 0) p = p * tzv * txv;
         const float K = Km[mcell];
         if (C.bc[0] >= 1 && C.bc[0] <= 3 && gz < 4) n = asat_cell(n, 0, C.bc[0], gz, U + ui, 1, IR + wi, 1, p, K, C);
-        if (C.bc[1] >= 1 && C.bc[1] <= 3 && gz >= nz - 4)
+        if (!AE && C.bc[1] >= 1 && C.bc[1] <= 3 && gz >= nz - 4)
             n = asat_cell(n, 1, C.bc[1], nz - 1 - gz, U + ui, -1, IR + wi, -1, p, K, C);
         if (C.bc[2] >= 1 && C.bc[2] <= 3 && gx < 4) n = asat_cell(n, 2, C.bc[2], gx, U + ui, UZ, IR + wi, WZ, p, K, C);
         if (C.bc[3] >= 1 && C.bc[3] <= 3 && gx >= nx - 4)
             n = asat_cell(n, 3, C.bc[3], nx - 1 - gx, U + ui, -UZ, IR + wi, -WZ, p, K, C);
+        if (AE && C.bc[1] >= 1 && C.bc[1] <= 3 && gz >= nz - 4)
+            n = asat_cell(n, 1, C.bc[1], nz - 1 - gz, U + ui, -1, IR + wi, -1, p, K, C);
         n = C.dt2 * n * K + 2 * U[ui] - p;
         if (gz == 0 || gz == nz - 1 || gx == 0 || gx == nx - 1) {
             int k;
@@ -179,7 +185,8 @@ acoustic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
             else k = 2 * nx + nz + gz;
             n = n / Sp->den[k];
         }
-        n = n * tzv * txv;
+        if (AE && gz == nz - 1) Sp->halo_save[gx] = p;   // interface row: coupled and tapered by ae_couple
+        else n = n * tzv * txv;
         pn[cell] = n;
         amax = fabsf(n);
     }
@@ -238,6 +245,71 @@ __global__ void acoustic_final_grad(const ShotDev *__restrict__ shots, int nshot
         float *g0 = S.grad + cell, *g1 = g0 + (long long)nx * ldz;
         *g0 = (float)((double)*g0 - c * (double)(fp - f));
         *g1 = (float)((double)*g1 + (double)w * 0.5 * (double)dtg * (double)(t2 * t0 + t3 * t1));
+    }
+}
+
+}  // namespace fwi2d
+
+namespace fwi2d {
+
+// Implicit coupling of the fluid potential and the elastic uz at the
+// interface (we_op.cpp:2486-2512, the it >= 0 branch), after both launches of
+// the step, then the taper of the two interface rows.  One thread per column.
+// E, W: the elastic and fluid tables of each shot; prev of both interface rows
+// (already tapered) is in halo_save.  sign = +1 forward, -1 adjoint.  With
+// F_GRAD, the density term of the imaging condition on the interface row,
+// which needs the coupled uz (the elastic kernel leaves it out there).
+__global__ void ae_couple(const ShotDev *__restrict__ E, const ShotDev *__restrict__ W, int nshots, ModelDev M,
+                          StepConst C, int it, int flags, float dtg, float Kw, float val0, int sign)
+{
+    const int s = blockIdx.y;
+    if (s >= nshots) return;
+    const ShotDev &e = E[s], &w = W[s];
+    if (it >= e.nt - 1) return;
+    const long long nxz = (long long)e.nx * e.ldz;
+    float *n1 = e.u[it & 1] + nxz;              // next uz, row 0
+    float *na = w.u[it & 1] + (w.nz - 1);       // next potential, last fluid row
+    for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < e.nx; ix += gridDim.x * blockDim.x) {
+        const long long ie = (long long)ix * e.ldz, ia = (long long)ix * w.ldz;
+        const float p1 = e.halo_save[ix], pa = w.halo_save[ix];
+        const float rho = M.p2[(long long)(e.x0 + ix) * M.ldz];
+        const float v1 = Kw * val0 * (n1[ie] - p1 + sign * val0 / rho * pa);
+        const float v2 = 1 + val0 * val0 * Kw / rho;
+        const float a = (na[ia] + sign * v1) / v2;
+        const float b = n1[ie] - sign * val0 / rho * (a - pa);
+        na[ia] = a * w.tz[w.nz - 1] * w.tx[ix];
+        const float a1 = b * e.tz[0] * e.tx[ix];
+        n1[ie] = a1;
+        const int tt = e.nt - 1 - (it + 1);
+        if ((flags & F_GRAD) && tt % C.sub == 0 && tt / C.sub != 0) {
+            // density term at snapshot itf with the coupled next field, as the
+            // elastic kernel's (nl_we_op_e::compute_gradients, we_op.cpp:505-562)
+            const int itf = tt / C.sub, last = e.nt / C.sub, prec = C.snap_prec;
+            const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(e.snap_amax, itf);
+            const long long o = (long long)itf * e.snap_slot + ie;
+            const float f0 = snap_load(e.snap, o, prec, inv), f1 = snap_load(e.snap, o + nxz, prec, inv);
+            float fp0 = 0.f, fp1 = 0.f, fm0 = 0.f, fm1 = 0.f;
+            if (itf + 1 <= last) {
+                const float iv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(e.snap_amax, itf + 1);
+                const long long op = (long long)(itf + 1) * e.snap_slot + ie;
+                fp0 = snap_load(e.snap, op, prec, iv);
+                fp1 = snap_load(e.snap, op + nxz, prec, iv);
+            }
+            {
+                const float iv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(e.snap_amax, itf - 1);
+                const long long om = (long long)(itf - 1) * e.snap_slot + ie;
+                fm0 = snap_load(e.snap, om, prec, iv);
+                fm1 = snap_load(e.snap, om + nxz, prec, iv);
+            }
+            const float a0 = e.u[it & 1][ie];
+            const float gw = e.gwt[itf];
+            const double wdt = (double)gw * 1.0 / (double)dtg;
+            float *g2 = e.grad + 2 * nxz + ie;
+            if (itf < last)
+                *g2 = (float)((double)*g2 + wdt * (double)(a0 * (fp0 - 2 * f0 + fm0) + a1 * (fp1 - 2 * f1 + fm1)));
+            else
+                *g2 = (float)((double)*g2 + wdt * (double)(a0 * (-f0 + fm0) + a1 * (-f1 + fm1)));
+        }
     }
 }
 

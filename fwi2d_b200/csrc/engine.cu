@@ -219,6 +219,8 @@ struct ShotPlan {
     DevBuf d_mrow_f, d_mrow_a;
     DevBuf den, tz, tx, snap, amax, grad, gwt;
     DevBuf r0, r1, ckpt;           // checkpoint-and-recompute: replay fields and checkpoints
+    DevBuf halo;                   // acoustic-elastic: prev of the interface row [nx]
+    std::unique_ptr<ShotPlan> fluid;   // acoustic-elastic: the fluid layer's grid (nx x nza)
 };
 
 struct Plan {
@@ -241,6 +243,28 @@ struct Plan {
     int ckpt = 0;
     std::vector<int> cuts;
     DevBuf d_shots_r, d_shots_c;
+    // acoustic-elastic: fluid layer of nza rows (pitch ldzw) with the constant
+    // model (K, 1/rho) of the water, its tiles, shot tables and step constants
+    bool ae = false, ae_src_fluid = false;
+    int nza = 0, ldzw = 0, nx_max = 0;
+    float Kw = 0.f, val0 = 0.f;
+    StepConst Cw;
+    DevBuf wK, wIR;
+    std::vector<TileRef> wtiles;
+    DevBuf d_wtiles, d_wshots_f, d_wshots_a;
+    std::vector<InitCell> wicells[2];
+    std::vector<int> wioff[2], wiidx[2];
+    DevBuf d_wicells[2], d_wioff[2], d_wiidx[2];
+    ModelDev wdev() const
+    {
+        ModelDev m;
+        std::memset(&m, 0, sizeof(m));
+        m.nz = nza;
+        m.ldz = ldzw;
+        m.p0 = wK.as<float>();
+        m.p1 = wIR.as<float>();
+        return m;
+    }
     // initial-state cells per mode (0 forward, 1 adjoint)
     std::vector<InitCell> icells[2];
     std::vector<int> ioff[2], iidx[2];
@@ -610,14 +634,14 @@ static void build_inj(const fwi2d_injector &J, int ncomp, const int *rowbase_a, 
 
 // Receiver entries, owned by the unit of the pivot cell (the middle of the 3x3).
 static void build_ext(const fwi2d_injector &J, int ncomp, const ShotUnits &U, std::vector<ExtEntry> &out,
-                      std::vector<int> &off, std::vector<int> &roff)
+                      std::vector<int> &off, std::vector<int> &roff, int row0 = 0)
 {
     std::vector<ExtEntry> ent;
     std::vector<int> unit, row, zk;
     for (int c = 0; c < ncomp; c++)
         for (int t = 0; t < J.ntr; t++) {
             ExtEntry e;
-            e.row = c * J.ntr + t;
+            e.row = row0 + c * J.ntr + t;
             e.comp = c;
             e.gx0 = J.xind[t * 3];
             e.gz0 = J.zind[t * 3];
@@ -731,7 +755,45 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
     d.snap_amax = s.amax.as<unsigned>();
     d.grad = s.grad.as<float>();
     d.gwt = s.gwt.as<float>();
+    d.halo_save = s.halo.as<float>();
     (void)P;
+}
+
+// Tables of the fluid layer of an acoustic-elastic shot: its own grid, fields,
+// injector tables and boundary factors; its traces are the fluid rows of the
+// shot's trace buffers (rows [0, nr) of every time sample).
+static void shot_dev_fluid(const Plan &P, const ShotPlan &s, bool adjoint, ShotDev &d)
+{
+    const ShotPlan &w = *s.fluid;
+    std::memset(&d, 0, sizeof(d));
+    d.nx = w.nx;
+    d.nz = P.nza;
+    d.ldz = P.ldzw;
+    d.x0 = w.x0;
+    d.nt = w.nt;
+    d.u[0] = w.u0.as<float>();
+    d.u[1] = w.u1.as<float>();
+    if (!adjoint) {
+        d.src = s.src_f.as<float>();
+        d.nsrc = s.nsrc_rows;
+        d.rcv = s.rcv_f.as<float>();
+        d.nrcv = s.nrcv_rows;
+        d.inj = w.d_inj_f.as<InjEntry>();
+        d.inj_off = w.d_inj_f_off.as<int>();
+        d.ext = w.d_ext_f.as<ExtEntry>();
+        d.ext_off = w.d_ext_f_off.as<int>();
+        d.n_ext = (int)w.ext_f.size();
+    } else {
+        d.src = s.src_a.as<float>();
+        d.nsrc = s.nrcv_rows;
+        d.inj = w.d_inj_a.as<InjEntry>();
+        d.inj_off = w.d_inj_a_off.as<int>();
+        d.ext_off = w.d_ext_none_off.as<int>();
+    }
+    d.den = w.den.as<float>();
+    d.tz = w.tz.as<float>();
+    d.tx = w.tx.as<float>();
+    d.halo_save = w.halo.as<float>();
 }
 
 // Cells touched by the injection at time sample 0, with their entries in
@@ -751,14 +813,16 @@ static void init_factors(const ModelState &M, Plan &P)
         }
 }
 
-static void build_init_cells(const ModelState &M, Plan &P)
+static void collect_init_cells(const Plan &P, bool fluid, std::vector<InitCell> *icells, std::vector<int> *iidx,
+                               std::vector<int> *ioff)
 {
     for (int mode = 0; mode < 2; mode++) {
-        P.icells[mode].clear();
-        P.iidx[mode].clear();
-        P.ioff[mode].assign(P.shots.size() + 1, 0);
+        icells[mode].clear();
+        iidx[mode].clear();
+        ioff[mode].assign(P.shots.size() + 1, 0);
         for (size_t s = 0; s < P.shots.size(); s++) {
-            const std::vector<InjEntry> &inj = mode ? P.shots[s]->inj_a : P.shots[s]->inj_f;
+            const ShotPlan &SP = fluid ? *P.shots[s]->fluid : *P.shots[s];
+            const std::vector<InjEntry> &inj = mode ? SP.inj_a : SP.inj_f;
             std::vector<std::vector<int>> lists;
             std::vector<InitCell> cells;
             for (size_t i = 0; i < inj.size(); i++) {
@@ -778,20 +842,37 @@ static void build_init_cells(const ModelState &M, Plan &P)
                 lists[k].push_back((int)i);
             }
             for (size_t k = 0; k < cells.size(); k++) {
-                cells[k].i0 = (int)P.iidx[mode].size();
-                P.iidx[mode].insert(P.iidx[mode].end(), lists[k].begin(), lists[k].end());
-                cells[k].i1 = (int)P.iidx[mode].size();
-                P.icells[mode].push_back(cells[k]);
+                cells[k].i0 = (int)iidx[mode].size();
+                iidx[mode].insert(iidx[mode].end(), lists[k].begin(), lists[k].end());
+                cells[k].i1 = (int)iidx[mode].size();
+                icells[mode].push_back(cells[k]);
             }
-            P.ioff[mode][s + 1] = (int)P.icells[mode].size();
+            ioff[mode][s + 1] = (int)icells[mode].size();
         }
     }
+}
+
+static void build_init_cells(const ModelState &M, Plan &P)
+{
+    collect_init_cells(P, false, P.icells, P.iidx, P.ioff);
     init_factors(M, P);
+    if (P.ae) {
+        // the fluid layer's initial state: 0.5 K dt^2 in double (we_op.cpp:2230-2236)
+        collect_init_cells(P, true, P.wicells, P.wiidx, P.wioff);
+        const double dt = P.par.dt;
+        for (int mode = 0; mode < 2; mode++)
+            for (auto &q : P.wicells[mode]) q.factor = 0.5 * (double)P.Kw * dt * dt;
+    }
 }
 
 static void upload_init_cells(Plan &P, cudaStream_t st)
 {
     for (int mode = 0; mode < 2; mode++) {
+        if (P.ae) {
+            P.d_wicells[mode].upload(P.wicells[mode], st);
+            P.d_wioff[mode].upload(P.wioff[mode], st);
+            P.d_wiidx[mode].upload(P.wiidx[mode], st);
+        }
         P.d_icells[mode].upload(P.icells[mode], st);
         P.d_ioff[mode].upload(P.ioff[mode], st);
         P.d_iidx[mode].upload(P.iidx[mode], st);
@@ -809,13 +890,22 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     REQ(p.sub >= 0, "sub must be >= 0");
     REQ(p.snapshot_precision >= 0 && p.snapshot_precision <= 2, "unknown snapshot precision");
     REQ(p.taper_top >= 0 && p.taper_bottom >= 0 && p.taper_left >= 0 && p.taper_right >= 0, "negative taper");
-    REQ(p.taper_top + p.taper_bottom <= M.nz, "top and bottom tapers overlap");
+    const bool ae = M.kind == KIND_AE;
+    // acoustic-elastic: the top boundary and its taper belong to the fluid layer
+    REQ((ae ? 0 : p.taper_top) + p.taper_bottom <= M.nz, "top and bottom tapers overlap");
     for (int i = 0; i < 4; i++) {
         int bc = (&p.bc_top)[i];
         REQ(bc >= 1 && bc <= 3, "boundary condition must be 1, 2 or 3");
-        if (M.kind != KIND_ACOUSTIC) REQ(bc <= 2, "the elastic propagators take boundary conditions 1 or 2");
+        if (M.kind != KIND_ACOUSTIC && !(ae && i == 0))
+            REQ(bc <= 2, "the elastic propagators take boundary conditions 1 or 2");
     }
-    if (M.kind == KIND_AE) throw Error(FWI2D_ERR_UNSUPPORTED, "this propagator is not built yet");
+    if (ae) {
+        REQ(p.nza >= 12, "acoustic-elastic: the fluid layer needs nza >= 12 rows");
+        REQ(p.water_velocity > 0 && p.water_density > 0, "acoustic-elastic: water velocity and density must be positive");
+        REQ(p.taper_top <= p.nza, "acoustic-elastic: the top taper is longer than the fluid layer");
+        REQ(!p.mt, "acoustic-elastic: point sources only (mt = 0)");
+        REQ(p.checkpoint_every == 0, "acoustic-elastic: checkpoint-and-recompute is not available");
+    }
     const bool acoustic = M.kind == KIND_ACOUSTIC;
     REQ(!(acoustic && p.mt), "the acoustic propagator takes point sources only (mt = 0)");
     REQ(p.checkpoint_every >= 0, "checkpoint_every must be >= 0");
@@ -834,11 +924,30 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     P->ncompg = M.kind == KIND_ACOUSTIC ? 2 : 3;
     P->C = make_const(p, M.dx, M.dz);
     P->dtg = (float)(P->C.sub) * p.dt;
+    if (ae) {
+        // elastic grid: its top edge is the fluid interface (traction-free SAT);
+        // fluid layer: the reference's top, left and right conditions and a
+        // Neumann interface at its bottom (we_op.cpp:2400-2480)
+        P->C.bc[0] = 1;
+        P->Cw = make_const(p, M.dx, M.dz);
+        P->Cw.bc[1] = 3;
+        P->ae = true;
+        P->ae_src_fluid = p.acoustic_source != 0;
+        P->nza = p.nza;
+        P->ldzw = round_up(p.nza, 32);
+        const float rw = p.water_density;
+        P->Kw = rw * p.water_velocity * p.water_velocity;
+        const float h = (float)((double)M.dz * (17.0 / 48));   // interface row weight, we_op.cpp:2490
+        P->val0 = p.dt / (2 * h);
+        std::vector<float> wk((size_t)M.nx * P->ldzw, P->Kw), wir((size_t)M.nx * P->ldzw, (float)(1.0 / rw));
+        P->wK.upload(wk, ctx->st);
+        P->wIR.upload(wir, ctx->st);
+    }
 
     // shape: the requested one, else the marching kernel where it has enough
     // units to fill the GPU, else the first tile shape that fits every shot
     auto shape_ok = [&](int i) {
-        if (acoustic && !acoustic_shape_ok(i)) return false;
+        if ((acoustic || ae) && !acoustic_shape_ok(i)) return false;
         for (int s = 0; s < nshots; s++)
             if (!shape_fits(i, shots[s].nx, M.nz)) return false;
         return true;
@@ -847,7 +956,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     if (shape < 0 || shape >= shape_count()) {
         shape = -1;
         const int m0 = elastic_tile_count();
-        if (!acoustic && shape_ok(m0)) {
+        if (!acoustic && !ae && shape_ok(m0)) {
             long long units = 0;
             for (int s = 0; s < nshots; s++) units += (long long)make_units(m0, s, shots[s].nx, M.nz).marches.size();
             if (units >= 148) shape = m0;
@@ -873,11 +982,24 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         REQ(sh.x0 >= 0 && sh.nx >= 12 && sh.x0 + sh.nx <= M.nx, "shot grid outside the model");
         REQ(sh.nt >= 2 && sh.nt <= p.nt, "shot nt must be in [2, params.nt]");
         REQ(p.taper_left + p.taper_right <= sh.nx, "left and right tapers overlap");
-        REQ(sh.src.ntr > 0, "shot without source");
+        const bool src_fluid = ae && p.acoustic_source;
+        const fwi2d_injector none = {FWI2D_INJ_DELTA, 0, nullptr, nullptr, nullptr, nullptr};
+        const fwi2d_injector &esrc = src_fluid ? none : sh.src;
+        REQ((src_fluid ? sh.src_water.ntr : sh.src.ntr) > 0, "shot without source");
         REQ(sh.rcv.ntr > 0 && sh.rcv.type == FWI2D_INJ_DELTA, "shot receivers must be a delta injector");
-        REQ((sh.src.type == FWI2D_INJ_DDELTA) == (p.mt != 0), "source injector type must match params.mt");
-        check_injector(sh.src, sh.nx, M.nz, "source");
+        if (!src_fluid)
+            REQ((sh.src.type == FWI2D_INJ_DDELTA) == (p.mt != 0), "source injector type must match params.mt");
+        check_injector(esrc, sh.nx, M.nz, "source");
         check_injector(sh.rcv, sh.nx, M.nz, "receivers");
+        if (ae) {
+            REQ(sh.rcv_water.ntr == sh.rcv.ntr && sh.rcv_water.type == FWI2D_INJ_DELTA,
+                "acoustic-elastic: the fluid receivers must be a delta injector with as many traces as the elastic ones");
+            check_injector(sh.rcv_water, sh.nx, p.nza, "fluid receivers");
+            if (src_fluid) {
+                REQ(sh.src_water.type == FWI2D_INJ_DELTA, "acoustic-elastic: the fluid source must be a delta injector");
+                check_injector(sh.src_water, sh.nx, p.nza, "fluid source");
+            }
+        }
         auto S = std::make_unique<ShotPlan>();
         S->x0 = sh.x0;
         S->nx = sh.nx;
@@ -885,11 +1007,12 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->ncomp = acoustic ? 1 : 2;
         const ShotUnits U = make_units(shape, s, sh.nx, M.nz);
         const int nunits = U.nunits();
-        S->ntr_src = sh.src.ntr;
-        S->ncomp_src = acoustic ? 1 : (p.mt ? 3 : 2);
+        S->ntr_src = src_fluid ? sh.src_water.ntr : sh.src.ntr;
+        S->ncomp_src = acoustic || src_fluid ? 1 : (p.mt ? 3 : 2);
         S->nr = sh.rcv.ntr;
         S->nsrc_rows = S->ncomp_src * S->ntr_src;
-        S->nrcv_rows = S->ncomp * S->nr;
+        // acoustic-elastic traces: [fluid, x, z] blocks of nr rows (we_op.cpp:2199-2214)
+        S->nrcv_rows = (ae ? 3 : S->ncomp) * S->nr;
         // forward sources: force -> rows c*ntr ; moment tensor blocks (mxx, mzz, mxz)
         int ra[2], rb[2];
         if (!p.mt) {
@@ -902,10 +1025,11 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             ra[1] = 2 * S->ntr_src;     // next1: inx = mxz, inz = mzz
             rb[1] = S->ntr_src;
         }
-        build_inj(sh.src, S->ncomp, ra, rb, U, S->inj_f, S->inj_f_off, S->inj_f_roff);
-        int qa[2] = {0, S->nr}, qb[2] = {0, 0};
+        build_inj(esrc, S->ncomp, ra, rb, U, S->inj_f, S->inj_f_off, S->inj_f_roff);
+        const int r0 = ae ? S->nr : 0;   // first elastic row of the traces
+        int qa[2] = {r0, r0 + S->nr}, qb[2] = {0, 0};
         build_inj(sh.rcv, S->ncomp, qa, qb, U, S->inj_a, S->inj_a_off, S->inj_a_roff);
-        build_ext(sh.rcv, S->ncomp, U, S->ext_f, S->ext_f_off, S->ext_f_roff);
+        build_ext(sh.rcv, S->ncomp, U, S->ext_f, S->ext_f_off, S->ext_f_roff, r0);
         S->ext_none_off.assign(nunits + 1, 0);
 
         // boundary divisors and taper on this shot's window of the model
@@ -918,11 +1042,50 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             const float *lam = M.hp(0) + (size_t)sh.x0 * M.nz, *mu = M.hp(1) + (size_t)sh.x0 * M.nz,
                         *rho = M.hp(2) + (size_t)sh.x0 * M.nz;
             const float *eps = vti ? M.hp(4) + (size_t)sh.x0 * M.nz : nullptr;
-            elastic_scale_divisors(sh.nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, p.bc_top == 2,
+            elastic_scale_divisors(sh.nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, !ae && p.bc_top == 2,
                                    p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
         }
-        taper_factors(sh.nx, M.nz, p.taper_top, p.taper_bottom, p.taper_left, p.taper_right, p.taper_strength,
-                      true, true, true, true, tz, tx);
+        taper_factors(sh.nx, M.nz, ae ? 0 : p.taper_top, p.taper_bottom, p.taper_left, p.taper_right,
+                      p.taper_strength, true, true, true, true, tz, tx);
+        if (ae) {
+            // the fluid layer's grid of this shot: same columns, nza rows
+            auto W = std::make_unique<ShotPlan>();
+            W->x0 = sh.x0;
+            W->nx = sh.nx;
+            W->nt = sh.nt;
+            W->ncomp = 1;
+            W->nr = sh.rcv_water.ntr;
+            const ShotUnits UW = make_units(shape, s, sh.nx, p.nza);
+            int wa[2] = {0, 0}, wb[2] = {0, 0};
+            build_inj(src_fluid ? sh.src_water : none, 1, wa, wb, UW, W->inj_f, W->inj_f_off, W->inj_f_roff);
+            build_inj(sh.rcv_water, 1, wa, wb, UW, W->inj_a, W->inj_a_off, W->inj_a_roff);
+            build_ext(sh.rcv_water, 1, UW, W->ext_f, W->ext_f_off, W->ext_f_roff, 0);
+            W->ext_none_off.assign(UW.nunits() + 1, 0);
+            std::vector<float> wk((size_t)sh.nx * p.nza, P->Kw), wir((size_t)sh.nx * p.nza, (float)(1.0 / p.water_density));
+            std::vector<float> wden, wtz, wtx;
+            acoustic_scale_divisors(sh.nx, p.nza, M.dx, M.dz, p.dt, wk.data(), wir.data(), p.nza, p.bc_top == 2, false,
+                                    p.bc_left == 2, p.bc_right == 2, wden);
+            taper_factors(sh.nx, p.nza, p.taper_top, 0, p.taper_left, p.taper_right, p.taper_strength, true, true,
+                          true, true, wtz, wtx);
+            const size_t wfield = (size_t)sh.nx * P->ldzw;
+            W->u0.alloc(wfield * sizeof(float));
+            W->u1.alloc(wfield * sizeof(float));
+            W->halo.alloc((size_t)sh.nx * sizeof(float));
+            W->d_inj_f.upload(W->inj_f, ctx->st);
+            W->d_inj_f_off.upload(W->inj_f_off, ctx->st);
+            W->d_inj_a.upload(W->inj_a, ctx->st);
+            W->d_inj_a_off.upload(W->inj_a_off, ctx->st);
+            W->d_ext_f.upload(W->ext_f, ctx->st);
+            W->d_ext_f_off.upload(W->ext_f_off, ctx->st);
+            W->d_ext_none_off.upload(W->ext_none_off, ctx->st);
+            W->den.upload(wden, ctx->st);
+            W->tz.upload(wtz, ctx->st);
+            W->tx.upload(wtx, ctx->st);
+            P->wtiles.insert(P->wtiles.end(), UW.tiles.begin(), UW.tiles.end());
+            S->halo.alloc((size_t)sh.nx * sizeof(float));
+            S->fluid = std::move(W);
+            P->nx_max = std::max(P->nx_max, sh.nx);
+        }
         S->nslot = p.sub > 0 ? 1 + sh.nt / p.sub : 0;
         std::vector<float> gw(std::max(S->nslot, 1), 1.f);
         for (int i = 0; i < S->nslot; i++) {
@@ -992,6 +1155,16 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     for (int s = 0; s < nshots; s++) sf[s].ckpt = P->shots[s]->ckpt.as<float>();
     P->d_shots_f.upload(sf, ctx->st);
     P->d_shots_a.upload(sa, ctx->st);
+    if (ae) {
+        std::vector<ShotDev> wf(nshots), wa(nshots);
+        for (int s = 0; s < nshots; s++) {
+            shot_dev_fluid(*P, *P->shots[s], false, wf[s]);
+            shot_dev_fluid(*P, *P->shots[s], true, wa[s]);
+        }
+        P->d_wshots_f.upload(wf, ctx->st);
+        P->d_wshots_a.upload(wa, ctx->st);
+        P->d_wtiles.upload(P->wtiles, ctx->st);
+    }
     if (p.checkpoint_every > 0) {
         const int K = p.checkpoint_every, nt = P->nt_max;
         P->ckpt = K;
@@ -1040,6 +1213,18 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
                        cudaStream_t st)
 {
     int n = 0;
+    if (P.ae) {
+        // fluid layer, elastic grid, then the implicit interface coupling
+        const bool adj = (flags & STEP_GRAD) != 0;
+        const ShotDev *wshots = (adj ? P.d_wshots_a : P.d_wshots_f).as<ShotDev>();
+        launch_ae_fluid_step(P.tshape, wshots, P.d_wtiles.as<TileRef>(), (int)P.wtiles.size(), P.wdev(), P.Cw, it,
+                             flags & STEP_EXTRACT, st);
+        launch_ae_elastic_step(P.tshape, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C, it, flags,
+                               P.dtg, st);
+        launch_ae_couple(shots, wshots, (int)P.shots.size(), P.nx_max, md, P.C, it, flags, P.dtg, P.Kw, P.val0,
+                         adj ? -1 : 1, st);
+        return 3;
+    }
     if (P.kind == KIND_ACOUSTIC) {
         launch_acoustic_step(P.tshape, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C, it, flags, P.dtg,
                              st);
@@ -1267,12 +1452,24 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
         CK(cudaMemsetAsync(S->u1.p, 0, S->u1.n, cst));
         if (adj) CK(cudaMemsetAsync(S->grad.p, 0, S->grad.n, cst));
         if (store && S->amax.p) CK(cudaMemsetAsync(S->amax.p, 0, S->amax.n, cst));
+        if (P.ae) {
+            CK(cudaMemsetAsync(S->fluid->u0.p, 0, S->fluid->u0.n, cst));
+            CK(cudaMemsetAsync(S->fluid->u1.p, 0, S->fluid->u1.n, cst));
+        }
     }
     const ShotDev *shots = (adj ? P.d_shots_a : P.d_shots_f).as<ShotDev>();
+    const ShotDev *wshots = P.ae ? (adj ? P.d_wshots_a : P.d_wshots_f).as<ShotDev>() : nullptr;
     const int nshots = (int)P.shots.size();
     const int im = adj ? 1 : 0;
-    launch_init_state(shots, nshots, P.d_icells[im].as<InitCell>(), P.d_ioff[im].as<int>(), P.d_iidx[im].as<int>(),
-                      cst);
+    // acoustic-elastic: the initial injection goes to the fluid layer when the
+    // source is in the water, else to the elastic grid, in both directions
+    // (we_op.cpp:2220-2236)
+    if (P.ae && P.ae_src_fluid)
+        launch_init_state(wshots, nshots, P.d_wicells[im].as<InitCell>(), P.d_wioff[im].as<int>(),
+                          P.d_wiidx[im].as<int>(), cst);
+    else
+        launch_init_state(shots, nshots, P.d_icells[im].as<InitCell>(), P.d_ioff[im].as<int>(),
+                          P.d_iidx[im].as<int>(), cst);
     n++;
     int flags = 0;
     if (adj) flags = STEP_GRAD;
@@ -1292,6 +1489,10 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
         if (!adj) {
             launch_finalize(shots, nshots, P.C, ncomp, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
             n++;
+            if (P.ae) {
+                launch_finalize(wshots, nshots, P.Cw, 1, STEP_EXTRACT, cst);
+                n++;
+            }
         } else if (P.kind == KIND_ACOUSTIC) {
             launch_acoustic_final_grad(shots, nshots, md, P.C, P.dtg, cst);   // snapshot 0 with the last adjoint field
             n++;
@@ -1510,7 +1711,7 @@ static void update_model(fwi2d_ctx *ctx, const float *model)
         const float *lam = M.hp(0) + (size_t)S->x0 * M.nz, *mu = M.hp(1) + (size_t)S->x0 * M.nz,
                     *rho = M.hp(2) + (size_t)S->x0 * M.nz;
         const float *eps = M.kind == KIND_VTI ? M.hp(4) + (size_t)S->x0 * M.nz : nullptr;
-        elastic_scale_divisors(S->nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, p.bc_top == 2,
+        elastic_scale_divisors(S->nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, !P.ae && p.bc_top == 2,
                                p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
         S->den.upload(den, ctx->st);
     }
@@ -1854,12 +2055,12 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     REQ(ctx, "null context");
     Plan &P = need_plan(ctx);
     const long long steps = P.nt_max - 1;
-    const long long per = P.marches.empty() ? 1 : 3;
+    const long long per = P.marches.empty() && !P.ae ? 1 : 3;
     const long long nseg = P.ckpt > 0 ? (long long)P.cuts.size() - 1 : 0;
     const long long acf = P.kind == KIND_ACOUSTIC ? 1 : 0;
     // forward: init, steps, last sample (+ checkpoint copies); adjoint: init, steps,
     // acoustic final imaging, per-shot scatter (+ replays: restore, steps, last snapshot)
-    if (lf) *lf = steps * per + 2 + (nseg > 0 ? nseg - 1 : 0);
+    if (lf) *lf = steps * per + 2 + (P.ae ? 1 : 0) + (nseg > 0 ? nseg - 1 : 0);
     if (la) *la = steps * per + 1 + acf + (long long)P.shots.size() + (nseg > 0 ? (steps + nseg - 1) * per + 2 * nseg : 0);
     if (shape) *shape = P.shape;
     if (snap_bytes) *snap_bytes = P.snap_bytes;

@@ -102,7 +102,14 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 // tiles take the general path, which carries the boundary closures, the SAT
 // terms and the absorbing scaling.  Both paths perform the same arithmetic.
 // ---------------------------------------------------------------------------
-template <bool VTI, int RZ, int TX, bool GRAD>
+// AE: the elastic part of the acoustic-elastic propagator
+// (nl_we_op_ae::propagate, we_op.cpp:2137-2577): isotropic, version-1 split of
+// the lambda terms (Dx(lambda ux_x) + Dx(lambda uz_z), Dz(lambda uz_z) +
+// Dz(lambda ux_x)), the top edge is the fluid interface (traction-free SAT,
+// applied after the other sides), and the interface row of uz is left
+// untapered, with its prev saved in halo_save, for ae_couple.  No imaging
+// term at snapshot 0.  General path only.
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE>
 __global__ void __launch_bounds__(32 * TX)
 elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C,
              int it, int flags, float dtg)
@@ -121,7 +128,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     float *BX = T0 + WX * WZ;      // uz_x
     float *CZ = BX + WX * WZ;      // ux_z
     float *T1 = CZ + WX * WZ;      // VTI: tmp_z
-    float *F0 = T1 + (VTI ? WX * WZ : 0);
+    float *F0 = T1 + ((VTI || AE) ? WX * WZ : 0);
     float *F1 = F0 + (GRAD ? WX * WZ : 0);
     float *red = F1 + (GRAD ? WX * WZ : 0);
 
@@ -136,7 +143,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     const bool interior = wx0 >= 6 && wx0 + TX + 6 <= nx && wz0 >= 6 && wz0 + TZ + 6 <= nz;
     // the lean path writes every cell of its window: only for tiles that own all of it
     const bool full = tr.ox0 == wx0 && tr.ox1 == wx0 + TX && tr.oz0 == wz0 && tr.oz1 == wz0 + TZ;
-    const bool lean = RZ == 2 && interior && full && (wz0 & 3) == 0;
+    const bool lean = !AE && RZ == 2 && interior && full && (wz0 & 3) == 0;
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
@@ -148,7 +155,8 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     const float *__restrict__ qsrc = VTI ? M.fxx + mofs : mp0;
 
     const int itf = GRAD ? (nt - 1 - (it + 1)) / C.sub : 0;
-    const bool do_grad = GRAD && (flags & F_GRAD) && ((nt - 1 - (it + 1)) % C.sub == 0);
+    const bool do_grad = GRAD && (flags & F_GRAD) && ((nt - 1 - (it + 1)) % C.sub == 0) &&
+                         (!AE || (nt - 1 - (it + 1)) / C.sub != 0);
     const int prec = C.snap_prec;
     float finv = 1.f;
     if (GRAD && do_grad && prec != SNAP_FP32) finv = 1.f / snap_scale(Sp->snap_amax, itf);
@@ -279,7 +287,10 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 const float uz_z = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
                 bx = d1(U1 + ui, UZ, gx, nx, C.dx, C.sdx);
                 cz = d1(U0 + ui, 1, gz, nz, C.dz, C.sdz);
-                if (!VTI) {
+                if (AE) {
+                    t0 = ux_x;
+                    t1 = uz_z;
+                } else if (!VTI) {
                     t0 = ux_x + uz_z;
                 } else {
                     const long long o = mofs + (long long)gx * mld + gz;
@@ -289,7 +300,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 }
             }
             T0[i] = t0;
-            if (VTI) T1[i] = t1;
+            if (VTI || AE) T1[i] = t1;
             BX[i] = bx;
             CZ[i] = cz;
         }
@@ -518,7 +529,12 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             }
             d2acc(n1, U1 + ui, UZ, MU + wi, WZ, 1.f, gx, nx, C.inv_d2x, C.d2x);
             d2acc(n0, U0 + ui, 1, MU + wi, 1, 1.f, gz, nz, C.inv_d2z, C.d2z);
-            if (!VTI) {
+            if (AE) {
+                n0 += md1(T0 + wi, Q + wi, WZ, gx, nx, C.adx);
+                n1 += md1(T1 + wi, Q + wi, 1, gz, nz, C.adz);
+                n0 += md1(T1 + wi, Q + wi, WZ, gx, nx, C.adx);
+                n1 += md1(T0 + wi, Q + wi, 1, gz, nz, C.adz);
+            } else if (!VTI) {
                 n0 += md1(T0 + wi, Q + wi, WZ, gx, nx, C.adx);
                 n1 += md1(T0 + wi, Q + wi, 1, gz, nz, C.adz);
             } else {
@@ -557,7 +573,9 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 const float imp_p = 0.5f * sqrtf((lam + 2 * mu) * rho);
                 const float imp_px = VTI ? 0.5f * sqrtf((1 + 2 * eps) * (lam + 2 * mu) * rho) : imp_p;
 #pragma unroll
-                for (int side = 0; side < 4; side++) {
+                for (int k = 0; k < 4; k++) {
+                    // the fluid interface (top) of the acoustic-elastic propagator comes last
+                    const int side = AE ? (k + 1) & 3 : k;
                     const int bc = C.bc[side];
                     if (bc != 1 && bc != 2) continue;
                     const bool ab = bc == 2;
@@ -610,7 +628,8 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             }
 
             n0 = n0 * tzv * txv;
-            n1 = n1 * tzv * txv;
+            if (AE && gz == 0) Sp->halo_save[gx] = p1;   // interface row: coupled and tapered by ae_couple
+            else n1 = n1 * tzv * txv;
             pn[cell] = n0;
             pn[nxz + cell] = n1;
             amax = fmaxf(amax, fmaxf(fabsf(n0), fabsf(n1)));
@@ -652,11 +671,14 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
                 const float gw = Sp->gwt[itf];
                 const double wdt = (double)gw * 1.0 / (double)dtg;
+                // acoustic-elastic interface row: the density term needs the coupled uz (ae_couple)
+                const bool rho_here = !AE || gz != 0;
                 if (itf > 0 && itf < last) {
                     if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
                     else *g0 = *g0 + gw * dtg * dl;
                     *g1 = *g1 + gw * dtg * dm;
-                    *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
+                    if (rho_here)
+                        *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
                 } else if (itf == 0) {
                     const double wh = (double)gw * 0.5 * (double)dtg;
                     if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
@@ -667,7 +689,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                     if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
                     else *g0 = *g0 + gw * dtg * dl;
                     *g1 = *g1 + gw * dtg * dm;
-                    *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
+                    if (rho_here) *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
                 }
             }
         }
@@ -807,24 +829,25 @@ void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const 
     cudaMemcpyToSymbol(kHC, hc, sizeof(float) * 4);
 }
 
-template <bool VTI, int RZ, int TX, bool GRAD>
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false>
 static constexpr size_t elastic_smem_bytes()
 {
     constexpr int TZ = 32 * RZ, UZ = TZ + 8, UX = TX + 8, WZ = TZ + 4, WX = TX + 4;
-    return sizeof(float) * (2 * UX * UZ + (5 + (VTI ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX);
+    return sizeof(float) * (2 * UX * UZ + (5 + ((VTI || AE) ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX);
 }
 
-template <bool VTI, int RZ, int TX, bool GRAD>
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false>
 static void launch_elastic_g(const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
                              const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
-    constexpr size_t bytes = elastic_smem_bytes<VTI, RZ, TX, GRAD>();
+    constexpr size_t bytes = elastic_smem_bytes<VTI, RZ, TX, GRAD, AE>();
     static bool configured = false;   // per process; a kernel attribute applies to every device
     if (!configured) {
-        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD, AE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes);
         configured = true;
     }
-    elastic_step<VTI, RZ, TX, GRAD><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags, dtg);
+    elastic_step<VTI, RZ, TX, GRAD, AE><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags, dtg);
 }
 
 template <bool VTI, int RZ, int TX>
@@ -924,12 +947,42 @@ void launch_acoustic_step(int shape, const ShotDev *shots, const TileRef *tiles,
 {
     const bool grad = (flags & F_GRAD) != 0;
     if (shape == 2) {
-        if (grad) acoustic_step<16, true><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
-        else acoustic_step<16, false><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        if (grad) acoustic_step<16, true, false><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        else acoustic_step<16, false, false><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
     } else {
-        if (grad) acoustic_step<8, true><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
-        else acoustic_step<8, false><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        if (grad) acoustic_step<8, true, false><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        else acoustic_step<8, false, false><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
     }
+}
+
+// Acoustic-elastic propagator: one step of the fluid layer (tile shape 2 or
+// 3), of the elastic grid (tile shape 2 or 3, general path) and the interface
+// coupling.
+void launch_ae_fluid_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                          const StepConst &C, int it, int flags, cudaStream_t st)
+{
+    if (shape == 2) acoustic_step<16, false, true><<<ntiles, 512, 0, st>>>(shots, tiles, M, C, it, flags, 1.f);
+    else acoustic_step<8, false, true><<<ntiles, 256, 0, st>>>(shots, tiles, M, C, it, flags, 1.f);
+}
+
+void launch_ae_elastic_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                            const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    const bool grad = (flags & F_GRAD) != 0;
+    if (shape == 2) {
+        if (grad) launch_elastic_g<false, 1, 16, true, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+        else launch_elastic_g<false, 1, 16, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+    } else {
+        if (grad) launch_elastic_g<false, 1, 8, true, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+        else launch_elastic_g<false, 1, 8, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+    }
+}
+
+void launch_ae_couple(const ShotDev *elastic, const ShotDev *fluid, int nshots, int nx_max, const ModelDev &M,
+                      const StepConst &C, int it, int flags, float dtg, float Kw, float val0, int sign, cudaStream_t st)
+{
+    dim3 grid((nx_max + 127) / 128, nshots);
+    ae_couple<<<grid, 128, 0, st>>>(elastic, fluid, nshots, M, C, it, flags, dtg, Kw, val0, sign);
 }
 
 void launch_acoustic_final_grad(const ShotDev *shots, int nshots, const ModelDev &M, const StepConst &C, float dtg,

@@ -35,6 +35,12 @@ void launch_checkpoint(const ShotDev *shots, int nshots, int ncomp, int k, bool 
 bool acoustic_shape_ok(int shape);
 void launch_acoustic_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
                           const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+void launch_ae_fluid_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                          const StepConst &C, int it, int flags, cudaStream_t st);
+void launch_ae_elastic_step(int shape, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                            const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+void launch_ae_couple(const ShotDev *elastic, const ShotDev *fluid, int nshots, int nx_max, const ModelDev &M,
+                      const StepConst &C, int it, int flags, float dtg, float Kw, float val0, int sign, cudaStream_t st);
 void launch_acoustic_final_grad(const ShotDev *shots, int nshots, const ModelDev &M, const StepConst &C, float dtg,
                                 cudaStream_t st);
 

@@ -27,11 +27,11 @@
 //   queues      curr row j+5 and coefficient / snapshot rows j+3 (copied at
 //               step j-1) enter the register queues.
 // The first output row is preceded by 10 steps that only fill the pipeline.
-// Forward kernels unroll the step body over the 8 ring phases, so that
-// register-queue and ring slots are compile-time constants and nothing moves
-// between steps; the larger imaging-condition kernels keep one rolled body
-// (run-time ring slots, register queues shifted by one row per step) so that
-// the loop stays within the instruction cache.
+// The step body is unrolled over groups of UNR phases (MARCH_FWD_UNROLL,
+// MARCH_GRAD_UNROLL; 2 measured best on B200 for both): register-queue slots
+// are compile-time constants within a group and the queues shift down by UNR
+// rows once per group.  Unrolling all 8 ring phases removes the shifts but
+// overflows the instruction cache.
 //
 // Shared memory, rows of RB = NTH + 24 floats; cell z of a row buffer sits
 // at index z - s0 with s0 = (za - 2) rounded down to a multiple of 8, so that
@@ -131,10 +131,14 @@ struct MarchCtx {
     unsigned ph[2];           // mbarrier phase parity per stage
 };
 
-template <bool GRAD>
+// Register queues along x.  UNR = 8: ring of 8 slots, row j+d of phase PH at
+// (PH + d) & 7, nothing moves.  UNR < 8: row j+d of phase PH at d + 2 + PH
+// (QL = 7 + UNR slots), and the queues shift down by UNR after the last phase.
+template <bool GRAD, int UNR>
 struct MarchQ {
-    float ux[8], uz[8], mu[8], q[8], t0[8], cz[8];
-    float ax[8], az[8], bx[8], f0[8], f1[8];
+    static constexpr int QL = UNR == 8 ? 8 : 7 + UNR;
+    float ux[QL], uz[QL], mu[QL], q[QL], t0[QL], cz[QL];
+    float ax[QL], az[QL], bx[QL], f0[QL], f1[QL];
 };
 
 // sample of a snapshot row buffer (fp32, or 16-bit scaled by inv)
@@ -147,7 +151,12 @@ __device__ __forceinline__ float srow(const float *buf, int idx, int prec, float
 
 // Rare per-row paths (rows holding a source or a receiver pivot) are kept
 // out of line, so that the unrolled step bodies stay small.
-__device__ __noinline__ void add_sources(const InjEntry *__restrict__ inj, const float *__restrict__ srcrow, int e0,
+#ifndef MARCH_RARE_INLINE
+#define MARCH_RARE __noinline__
+#else
+#define MARCH_RARE __forceinline__
+#endif
+__device__ MARCH_RARE void add_sources(const InjEntry *__restrict__ inj, const float *__restrict__ srcrow, int e0,
                                          int e1, int gz, float &n0, float &n1)
 {
     for (int e = e0; e < e1; e++) {
@@ -162,7 +171,7 @@ __device__ __noinline__ void add_sources(const InjEntry *__restrict__ inj, const
 
 // Receivers of one row: entries [r0, r1), 3x3 weights over the curr rows
 // j-1 .. j+1 of the rings (slots P+7, P, P+1).
-__device__ __noinline__ void march_extract(const ExtEntry *__restrict__ ext, float *__restrict__ rcvrow,
+__device__ MARCH_RARE void march_extract(const ExtEntry *__restrict__ ext, float *__restrict__ rcvrow,
                                            const float *rux, const float *ruz, int RB, int P, int s0, int r0, int r1,
                                            int nth)
 {
@@ -258,39 +267,40 @@ __device__ __forceinline__ void march_issue(const MarchCtx &X, float *sm, const 
 // Register queues of 8 rows.  Unrolled (PH >= 0): row j+d sits at index
 // (PH + d) & 7.  Rolled (PH < 0): row j+d sits at index d + 2 and the queues
 // shift by one row at the end of each step.
-template <bool GRAD>
-__device__ __forceinline__ void shift_queues(MarchQ<GRAD> &Q)
+template <bool GRAD, int UNR>
+__device__ __forceinline__ void shift_queues(MarchQ<GRAD, UNR> &Q)
 {
 #pragma unroll
     for (int k = 0; k < 7; k++) {
-        Q.ux[k] = Q.ux[k + 1];
-        Q.uz[k] = Q.uz[k + 1];
-        Q.mu[k] = Q.mu[k + 1];
-        Q.q[k] = Q.q[k + 1];
-        Q.t0[k] = Q.t0[k + 1];
-        Q.cz[k] = Q.cz[k + 1];
+        Q.ux[k] = Q.ux[k + UNR];
+        Q.uz[k] = Q.uz[k + UNR];
+        Q.mu[k] = Q.mu[k + UNR];
+        Q.q[k] = Q.q[k + UNR];
+        Q.t0[k] = Q.t0[k + UNR];
+        Q.cz[k] = Q.cz[k + UNR];
         if (GRAD) {
-            Q.ax[k] = Q.ax[k + 1];
-            Q.az[k] = Q.az[k + 1];
-            Q.bx[k] = Q.bx[k + 1];
-            Q.f0[k] = Q.f0[k + 1];
-            Q.f1[k] = Q.f1[k + 1];
+            Q.ax[k] = Q.ax[k + UNR];
+            Q.az[k] = Q.az[k + UNR];
+            Q.bx[k] = Q.bx[k + UNR];
+            Q.f0[k] = Q.f0[k + UNR];
+            Q.f1[k] = Q.f1[k + UNR];
         }
     }
 }
 
-template <bool VTI, bool GRAD, int NTH, int PH>
-__device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *sm, const ShotDev &S,
+template <bool VTI, bool GRAD, int NTH, int PH, int UNR>
+__device__ __forceinline__ bool march_step(MarchQ<GRAD, UNR> &Q, MarchCtx &X, float *sm, const ShotDev &S,
                                            const ModelDev &M, const StepConst &C, int j, int j0)
 {
     using L = MarchLayout<VTI, GRAD, NTH>;
     constexpr int RB = L::RB;
-    const int P = PH >= 0 ? PH : ((j - j0) & 7);
-    constexpr int QM2 = PH >= 0 ? (PH + 6) & 7 : 0, QM1 = PH >= 0 ? (PH + 7) & 7 : 1, Q00 = PH >= 0 ? PH : 2,
-                  QP1 = PH >= 0 ? (PH + 1) & 7 : 3, QP2 = PH >= 0 ? (PH + 2) & 7 : 4,
-                  QP3 = PH >= 0 ? (PH + 3) & 7 : 5, QP4 = PH >= 0 ? (PH + 4) & 7 : 6;
-    // register-queue slots of the rows arriving at the end of this step
-    constexpr int QN5 = PH >= 0 ? (PH + 5) & 7 : 6, QN3 = PH >= 0 ? (PH + 3) & 7 : 4;
+    constexpr bool RING = UNR == 8;   // queue slots rotate with the 8 phases
+    const int P = RING ? PH : ((j - j0) & 7);
+#define MQ(d) (RING ? ((PH + (d) + 8) & 7) : (PH + (d) + 2))
+    constexpr int QM2 = MQ(-2), QM1 = MQ(-1), Q00 = MQ(0), QP1 = MQ(1), QP2 = MQ(2), QP3 = MQ(3), QP4 = MQ(4);
+    // register-queue slots of the rows arriving at the end of this step (j+5, j+3)
+    constexpr int QN5 = MQ(5), QN3 = MQ(3);
+#undef MQ
     // ring slots of rows j+d (8-row rings) and (4-row rings)
     const int S0 = P, SP2 = (P + 2) & 7, SP3 = (P + 3) & 7, SP5 = (P + 5) & 7;
     const int R0 = P & 3, RP1 = (P + 1) & 3, RP2 = (P + 2) & 3;
@@ -470,7 +480,6 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
 
     // ---- queues: curr row j+5 and coefficient / snapshot rows j+3 (copied
     // at step j-1) take the slots the next step reads as j+4 and j+2
-    if (PH < 0) shift_queues<GRAD>(Q);
     if (j > j0) {
         Q.ux[QN5] = sm[L::UX + SP5 * RB + li];
         Q.uz[QN5] = sm[L::UZ + SP5 * RB + li];
@@ -481,11 +490,18 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD> &Q, MarchCtx &X, float *
             Q.f1[QN3] = srow(sm + L::F1 + SP3 * RB, li, X.prec, X.finv);
         }
     }
+    if (!RING && PH == UNR - 1) shift_queues<GRAD, UNR>(Q);
     return true;
 }
 
-#ifndef MARCH_ROLLED_GRAD
-#define MARCH_ROLLED_GRAD 0
+// Phases per unrolled group (1, 2, 4 or 8) of the imaging-condition and of the
+// forward kernels: fewer phases keep the step body within the instruction
+// cache at the cost of shifting the register queues every group.
+#ifndef MARCH_GRAD_UNROLL
+#define MARCH_GRAD_UNROLL 2
+#endif
+#ifndef MARCH_FWD_UNROLL
+#define MARCH_FWD_UNROLL 2
 #endif
 
 template <bool VTI, bool GRAD, int NTH>
@@ -566,30 +582,26 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
     X.grad = S.grad;
     X.ph[0] = X.ph[1] = 0u;
 
-    MarchQ<GRAD> Q;
+    constexpr int UNR = GRAD ? MARCH_GRAD_UNROLL : MARCH_FWD_UNROLL;
+    MarchQ<GRAD, UNR> Q;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
+    for (int k = 0; k < MarchQ<GRAD, UNR>::QL; k++) {
         Q.ux[k] = Q.uz[k] = Q.mu[k] = Q.q[k] = Q.t0[k] = Q.cz[k] = 0.f;
         Q.ax[k] = Q.az[k] = Q.bx[k] = Q.f0[k] = Q.f1[k] = 0.f;
     }
 
     const int j0 = U.xb - 10;
     bool ok = true;
-    if (GRAD && MARCH_ROLLED_GRAD) {
-        for (int j = j0; j < U.xe; j++) {
-            ok = march_step<VTI, GRAD, NTH, -1>(Q, X, smem, S, M, C, j, j0);
-            if (!ok) break;
-        }
-    } else {
-        for (int jb = j0; jb < U.xe; jb += 8) {
+    for (int jb = j0; jb < U.xe; jb += UNR) {
 #define MARCH_PHASE(k)                                                                              \
-    if (jb + k >= U.xe) break;                                                                      \
-    ok = march_step<VTI, GRAD, NTH, k>(Q, X, smem, S, M, C, jb + k, j0);                            \
-    if (!ok) break;
-            MARCH_PHASE(0) MARCH_PHASE(1) MARCH_PHASE(2) MARCH_PHASE(3)
-            MARCH_PHASE(4) MARCH_PHASE(5) MARCH_PHASE(6) MARCH_PHASE(7)
+    if (k < UNR) {                                                                                  \
+        if (jb + k >= U.xe) break;                                                                  \
+        ok = march_step<VTI, GRAD, NTH, (k < UNR ? k : 0), UNR>(Q, X, smem, S, M, C, jb + k, j0);   \
+        if (!ok) break;                                                                             \
+    }
+        MARCH_PHASE(0) MARCH_PHASE(1) MARCH_PHASE(2) MARCH_PHASE(3)
+        MARCH_PHASE(4) MARCH_PHASE(5) MARCH_PHASE(6) MARCH_PHASE(7)
 #undef MARCH_PHASE
-        }
     }
     if (!ok) {
         // a copy stage may still be in flight: give it a bounded wait before the

@@ -60,7 +60,13 @@ def _injector(itype, tabs):
 @dataclass
 class ShotSpec:
     """One shot: its grid is model columns [x0, x0+nx); locations in km
-    relative to the model origin (ox, oz)."""
+    relative to the model origin (ox, oz).
+
+    Acoustic-elastic propagator (nl_we_op_ae): the fluid layer spans depths
+    0 .. oz above the elastic grid (whose first row is at oz); the fluid
+    receivers (``water_rcv_*``, as many as the elastic ones) and, with
+    ``acoustic_source`` set in the parameters, the source (``water_src_*``)
+    are located on the fluid grid, depths from 0."""
     x0: int
     nx: int
     nt: int
@@ -69,6 +75,10 @@ class ShotSpec:
     rcv_x: Sequence[float]
     rcv_z: Sequence[float]
     mt: bool = False
+    water_src_x: Optional[Sequence[float]] = None
+    water_src_z: Optional[Sequence[float]] = None
+    water_rcv_x: Optional[Sequence[float]] = None
+    water_rcv_z: Optional[Sequence[float]] = None
 
 
 class Propagator:
@@ -105,17 +115,29 @@ class Propagator:
         arr = (C.Shot * len(shots))()
         keep = []
         self.src_rows, self.rcv_rows = [], []
+        ae = self.kind == C.ACOUSTIC_ELASTIC
+        fluid_src = ae and bool(params.acoustic_source)
         for i, s in enumerate(shots):
             ox = self.ox + s.x0 * self.dx
             st = C.INJ_DDELTA if s.mt else C.INJ_DELTA
-            src = injector_tables(st, s.src_x, s.src_z, s.nx, self.nz, self.dx, self.dz, ox, self.oz)
+            src = None
+            if not fluid_src:
+                src = injector_tables(st, s.src_x, s.src_z, s.nx, self.nz, self.dx, self.dz, ox, self.oz)
             rcv = injector_tables(C.INJ_DELTA, s.rcv_x, s.rcv_z, s.nx, self.nz, self.dx, self.dz, ox, self.oz)
-            keep += [src, rcv]
+            wsrc = wrcv = None
+            if ae:
+                nza = int(params.nza)
+                if fluid_src:
+                    wsrc = injector_tables(C.INJ_DELTA, s.water_src_x, s.water_src_z, s.nx, nza, self.dx, self.dz,
+                                           ox, 0.0)
+                wrcv = injector_tables(C.INJ_DELTA, s.water_rcv_x, s.water_rcv_z, s.nx, nza, self.dx, self.dz, ox,
+                                       0.0)
+            keep += [src, rcv, wsrc, wrcv]
             arr[i] = C.Shot(s.x0, s.nx, s.nt, _injector(st, src), _injector(C.INJ_DELTA, rcv),
-                            _injector(0, None), _injector(0, None))
-            nsrc = len(s.src_x)
-            nc = self.ncomp()
-            self.src_rows.append((3 if s.mt else nc) * nsrc)
+                            _injector(C.INJ_DELTA, wsrc), _injector(C.INJ_DELTA, wrcv))
+            nsrc = len(s.water_src_x) if fluid_src else len(s.src_x)
+            nc = self.trace_ncomp()
+            self.src_rows.append((3 if s.mt else (1 if fluid_src else self.ncomp())) * nsrc)
             self.rcv_rows.append(nc * len(s.rcv_x))
         C.check(self.L.fwi2d_set_shots(self.h, ctypes.byref(params), len(shots), arr))
         self._keep = keep
@@ -123,6 +145,11 @@ class Propagator:
     def ncomp(self):
         """Wavefield components: 1 (pressure) for the acoustic propagator, else 2."""
         return 1 if self.kind == C.ACOUSTIC else 2
+
+    def trace_ncomp(self):
+        """Receiver trace components: the field's, plus the fluid trace first
+        for the acoustic-elastic propagator (we_op.cpp:2199-2214)."""
+        return 3 if self.kind == C.ACOUSTIC_ELASTIC else self.ncomp()
 
     def ngrad(self):
         """Gradient components: (K, 1/rho) acoustic, else (lambda, mu, rho)."""
@@ -144,7 +171,7 @@ class Propagator:
         C.check(self.L.fwi2d_forward(self.h, C.ptr(src), C.ptr(out), 1 if store else 0))
         res, o = [], 0
         for r, s in zip(self.rcv_rows, self.shots):
-            nc = self.ncomp()
+            nc = self.trace_ncomp()
             res.append(out[o:o + r * s.nt].reshape(nc, r // nc, s.nt))
             o += r * s.nt
         return res
