@@ -2158,11 +2158,18 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
                     int nx, int nz, float dx, float dz)
 {
     ABI_TRY
-    REQ(par && model && inj && ext, "null argument");
-    REQ(kind == FWI2D_ELASTIC || kind == FWI2D_VTI || kind == FWI2D_ACOUSTIC,
-        "fwi2d_propagate: this propagator is not built yet");
-    (void)inja;
-    (void)exta;
+    REQ(par && model, "null argument");
+    REQ(kind >= FWI2D_ELASTIC && kind <= FWI2D_ACOUSTIC_ELASTIC, "unknown propagator kind");
+    const bool ae = kind == FWI2D_ACOUSTIC_ELASTIC;
+    const bool src_fluid = ae && par->acoustic_source;
+    // acoustic-elastic: forward sources in the fluid (inja) or the solid (inj),
+    // receivers in both (ext, exta); the adjoint injects at both receiver sets
+    // (inj, inja) and needs the source side (ext or exta) only for the plan.
+    // Other propagators: inj and ext.
+    if (!ae) REQ(inj && ext, "null argument");
+    else if (!adj) REQ(ext && exta && (src_fluid ? inja : inj), "null argument");
+    else REQ(inj && inja && (src_fluid || ext), "null argument");
+    const fwi2d_injector none = {FWI2D_INJ_DELTA, 0, nullptr, nullptr, nullptr, nullptr};
     int dev = 0;
     CK(cudaGetDevice(&dev));
     fwi2d_ctx *ctx = thread_ctx(dev);
@@ -2178,9 +2185,22 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
     sh.x0 = 0;
     sh.nx = nx;
     sh.nt = nt;
-    sh.src = adj ? *ext : *inj;
-    sh.rcv = adj ? *inj : *ext;
-    if (adj) p.mt = sh.src.type == FWI2D_INJ_DDELTA;
+    if (!ae) {
+        sh.src = adj ? *ext : *inj;
+        sh.rcv = adj ? *inj : *ext;
+        if (adj) p.mt = sh.src.type == FWI2D_INJ_DDELTA;
+    } else if (!adj) {
+        sh.src = src_fluid ? none : *inj;
+        sh.src_water = src_fluid ? *inja : none;
+        sh.rcv = *ext;
+        sh.rcv_water = *exta;
+    } else {
+        // the plan needs the source side only for its forward tables
+        sh.rcv = *inj;
+        sh.rcv_water = *inja;
+        sh.src = src_fluid ? none : *ext;
+        sh.src_water = src_fluid ? (exta ? *exta : *inja) : none;
+    }
     const bool store = !adj && p.sub > 0 && full_wfld != nullptr;
     fwi2d_params pp = p;
     if (!store && !adj) pp.sub = 0;
@@ -2189,18 +2209,19 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
     ShotPlan &S = *P.shots[0];
     // gather the component blocks (stride ns*nt / nr*nt in the reference's buffers)
     const int in_ntr = adj ? S.nr : S.ntr_src;
-    const int in_comp = adj ? S.ncomp : S.ncomp_src;
+    const int out_comp = S.nrcv_rows / S.nr;   // traces per receiver: 1, 2, or 3 (fluid, x, z)
+    const int in_comp = adj ? out_comp : S.ncomp_src;
     const int stride = adj ? nr : ns;
     std::vector<float> in((size_t)in_comp * in_ntr * nt);
     for (int c = 0; c < in_comp; c++)
         for (int t = 0; t < in_ntr; t++)
             std::memcpy(&in[((size_t)c * in_ntr + t) * nt], allsrc + ((size_t)c * stride + t) * nt, nt * sizeof(float));
     if (!adj) {
-        std::vector<float> out((size_t)S.ncomp * S.nr * nt);
+        std::vector<float> out((size_t)out_comp * S.nr * nt);
         upload_traces(ctx, in.data(), false);
         run(ctx, false, store);
         download_rcv(ctx, out.data());
-        for (int c = 0; c < S.ncomp; c++)
+        for (int c = 0; c < out_comp; c++)
             for (int t = 0; t < S.nr; t++) {
                 float *dst = allrcv + ((size_t)c * nr + t) * nt;
                 const float *src = &out[((size_t)c * S.nr + t) * nt];

@@ -172,9 +172,14 @@ int fwi2d_tile_shape(int index, int *tz, int *tx);
  * meaning (we_op.hpp:82).  ns / nr are the trace counts that separate the
  * component blocks of allsrc / allrcv (par.ns and par.nr of the reference).
  * Forward accumulates into allrcv and writes full_wfld when sub > 0; adjoint
- * reads full_wfld and accumulates the imaging condition into grad.  inja /
- * exta are the water-layer injector and extractor of the acoustic-elastic
- * propagator (NULL otherwise). */
+ * reads full_wfld and accumulates the imaging condition into grad.
+ * Acoustic-elastic propagator (FWI2D_ACOUSTIC_ELASTIC, we_op.cpp:2137-2577):
+ * inja / exta are the injectors on the fluid layer's grid (nx x par->nza,
+ * depths from 0).  Forward: sources through inja (par->acoustic_source) or
+ * inj, receivers through ext (solid) and exta (fluid), traces [3][nr][nt] as
+ * (fluid, x, z).  Adjoint: the adjoint traces [3][nr][nt] are injected
+ * through inja (fluid block) and inj (x, z blocks); ext / exta are the source
+ * side.  NULL for the other propagators. */
 int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, float *allrcv,
                     const fwi2d_injector *inj, const fwi2d_injector *ext,
                     const fwi2d_injector *inja, const fwi2d_injector *exta,

@@ -115,3 +115,39 @@ def test_ae_vs_oracle(bc, acoustic_source, grid):
     assert np.abs(rcv).max() > 0 and np.abs(grad).max() > 0
     assert e_tr <= 1e-6 and e_sn <= 1e-6
     assert e_g <= 1e-5
+
+
+def test_ae_dropin_propagate_matches_reference_golden():
+    """fwi2d_propagate with the acoustic-elastic kind: the reference's
+    per-shot buffers ([fluid, x, z] traces, [nt+1][2][nx][nz] snapshots) and
+    the fluid injectors as inja / exta."""
+    import ctypes
+    from fwi2d_b200 import _capi as C
+    g = dict(np.load(os.path.join(GOLD, "acoustic_elastic_f32.npz")))
+    nx, nz, nt, d, oz, nza = int(g["nx"]), int(g["nz"]), int(g["nt"]), float(g["d"]), float(g["oz"]), int(g["nza"])
+    pd = K.par_dict(nt=nt, dt=1e-3, bc=(1, 2, 2, 2), taper=(0, 6, 6, 6), nza=nza, acoustic_source=1)
+    nr = len(g["rcv_x"])
+    erc = F.injector_tables(0, g["rcv_x"], g["rcv_ze"], nx, nz, d, d, 0.0, oz)
+    wrc = F.injector_tables(0, g["rcv_x"], g["rcv_zw"], nx, nza, d, d, 0.0, 0.0)
+    wsr = F.injector_tables(0, g["wsrc_x"], g["wsrc_z"], nx, nza, d, d, 0.0, 0.0)
+
+    def inj(t):
+        return C.Injector(0, len(t[0]), C.ptr(t[0]), C.ptr(t[1]), C.ptr(t[2]), C.ptr(t[3]))
+    je, jw, js = inj(erc), inj(wrc), inj(wsr)
+    L = F.load()
+    params = F.make_params(**pd)
+    rcv = np.zeros((3, nr, nt), np.float32)
+    full = np.zeros((nt + 1, 2, nx, nz), np.float32)
+    C.check(L.fwi2d_propagate(O.KIND_AE, 0, C.ptr(g["model"]), C.ptr(np.ascontiguousarray(g["src"])), C.ptr(rcv),
+                              None, ctypes.byref(je), ctypes.byref(js), ctypes.byref(jw), C.ptr(full), None,
+                              ctypes.byref(params), 1, nr, nx, nz, d, d))
+    assert np.array_equal(rcv, g["rcv"])
+    assert np.array_equal(full[g["snap_idx"]], g["snaps"])
+    adj = np.ascontiguousarray(g["rcv"][:, :, ::-1])
+    grad = np.zeros((3, nx, nz), np.float32)
+    dummy = np.zeros((1, 1, nt), np.float32)
+    C.check(L.fwi2d_propagate(O.KIND_AE, 1, C.ptr(g["model"]), C.ptr(adj), C.ptr(dummy), ctypes.byref(je), None,
+                              ctypes.byref(jw), ctypes.byref(js), C.ptr(full), C.ptr(grad), ctypes.byref(params), 1, nr,
+                              nx, nz, d, d))
+    print("AE drop-in gradient: bitwise %.4f, rel-L2 %.2e" % (np.mean(grad == g["grad"]), K.rel_l2(grad, g["grad"])))
+    assert K.rel_l2(grad, g["grad"]) <= 1e-5
