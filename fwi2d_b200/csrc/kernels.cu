@@ -929,11 +929,11 @@ void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const Shot
     if (nunits <= 0) return;
     const bool grad = (flags & F_GRAD) != 0;
     if (vti) {
-        if (grad) elastic_zband<true, true><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
-        else elastic_zband<true, false><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        if (grad) elastic_zband<true, true><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        else elastic_zband<true, false><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
     } else {
-        if (grad) elastic_zband<false, true><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
-        else elastic_zband<false, false><<<nunits, kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        if (grad) elastic_zband<false, true><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        else elastic_zband<false, false><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
     }
 }
 
