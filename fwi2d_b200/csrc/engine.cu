@@ -406,7 +406,8 @@ struct MarchShape {
     int nth, lx;
 };
 static const MarchShape kMarchShapes[] = {{224, 64}, {256, 64}, {192, 64}, {128, 64},
-                                          {224, 32}, {256, 32}, {192, 32}, {128, 32}};
+                                          {224, 32}, {256, 32}, {192, 32}, {128, 32},
+                                          {128, 16}, {224, 16}};
 static const int kNumMarch = sizeof(kMarchShapes) / sizeof(kMarchShapes[0]);
 static const int kBandTile = 3;    // (TZ, TX) = (32, 8): band windows of 8 columns own 6
 static const int kBand = 6;
@@ -1278,6 +1279,65 @@ static float time_forward_steps(fwi2d_ctx *ctx, int steps)
     return ms / std::max(nsteps, 1);
 }
 
+// Time `steps` adjoint steps with the imaging condition of the current plan
+// (built without snapshot storage), in milliseconds per step.  Every shot
+// images against a scratch window of 3 snapshot slots (zeroed), addressed like
+// the checkpoint windows: the shot tables carry the window shifted to the
+// snapshot index of the timed step.
+static float time_adjoint_steps(fwi2d_ctx *ctx, int steps)
+{
+    Plan &P = *ctx->plan;
+    const ModelState &M = ctx->M;
+    int nt_min = P.nt_max;
+    for (auto &S : P.shots) nt_min = std::min(nt_min, S->nt);
+    if (nt_min < 4) return 0.f;
+    const int it = nt_min - 3;   // every shot active, imaged snapshot index >= 1
+    const size_t esz = P.par.snapshot_precision == FWI2D_SNAP_FP32 ? 4 : 2;
+    std::vector<ShotDev> sd(P.shots.size());
+    CK(cudaMemcpy(sd.data(), P.d_shots_a.p, sd.size() * sizeof(ShotDev), cudaMemcpyDeviceToHost));
+    std::vector<std::unique_ptr<DevBuf>> win(P.shots.size()), amx(P.shots.size());
+    DevBuf ones;
+    ones.upload(std::vector<float>(3, 1.f), ctx->st);
+    for (size_t s = 0; s < P.shots.size(); s++) {
+        ShotPlan &S = *P.shots[s];
+        const long long slot = (long long)S.ncomp * S.nx * M.ldz;
+        // snapshot index imaged at launch it: nt-2-it (elastic), nt-1-it (acoustic)
+        const long long itf = S.nt - (P.kind == KIND_ACOUSTIC ? 1 : 2) - it;
+        win[s] = std::make_unique<DevBuf>();
+        win[s]->alloc(3 * (size_t)slot * esz);
+        amx[s] = std::make_unique<DevBuf>();
+        amx[s]->alloc(3 * sizeof(unsigned));
+        CK(cudaMemsetAsync(win[s]->p, 0, win[s]->n, ctx->st));
+        CK(cudaMemsetAsync(amx[s]->p, 0, amx[s]->n, ctx->st));
+        CK(cudaMemsetAsync(S.u0.p, 0, S.u0.n, ctx->st));
+        CK(cudaMemsetAsync(S.u1.p, 0, S.u1.n, ctx->st));
+        CK(cudaMemsetAsync(S.src_a.p, 0, S.src_a.n, ctx->st));
+        // slots itf-1 .. itf+1 of this shot map onto the window's 0 .. 2
+        sd[s].snap = (char *)win[s]->p - (itf - 1) * slot * (long long)esz;
+        sd[s].snap_slot = slot;
+        sd[s].snap_amax = amx[s]->as<unsigned>() - (itf - 1);
+        sd[s].gwt = ones.as<float>() - (itf - 1);
+    }
+    DevBuf d_sd;
+    d_sd.upload(sd, ctx->st);
+    const ModelDev md = M.dev();
+    const ShotDev *shots = d_sd.as<ShotDev>();
+    for (int k = 0; k < std::min(3, steps); k++) launch_step(ctx, P, shots, md, it, STEP_GRAD, ctx->st);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, ctx->st));
+    for (int k = 0; k < steps; k++) launch_step(ctx, P, shots, md, it, STEP_GRAD, ctx->st);
+    CK(cudaEventRecord(b, ctx->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaGetLastError());
+    return ms / std::max(steps, 1);
+}
+
 // Autotuner choices also persist across processes in the file named by the
 // environment variable FWI2D_TUNE_FILE (lines "<key> <shape>"), keyed by the
 // library build and the device, so that a later run -- for instance one under
@@ -1318,16 +1378,20 @@ static void tune_file_store(const std::string &key, int shape)
 }
 
 // Tile-shape autotuner: for plans that leave the shape open (tile_shape < 0),
-// time a few forward steps of every shape that tiles the grids and keep the
-// fastest.  The choice is cached per (kind, nz, shot grid widths).
+// time a few forward steps of every shape that tiles the grids -- plus as
+// many adjoint steps with the imaging condition for plans that keep
+// snapshots (gradients) -- and keep the fastest.  The choice is cached per
+// (kind, nz, snapshots, shot grid widths).
 static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
 {
     REQ(par != nullptr && shots != nullptr && nshots > 0, "no shots");
     fwi2d_params p = *par;
     if (p.tile_shape < 0 && ctx->M.kind >= 0) {
         static std::vector<std::pair<std::string, int>> cache;
+        const bool grad = p.sub > 0;
         std::string key = tune_build_key(ctx->device) + "/" + std::to_string(ctx->M.kind) + "/" +
-                          std::to_string(ctx->M.nz) + "/" + std::to_string(nshots);
+                          std::to_string(ctx->M.nz) + "/" + (grad ? "g" + std::to_string(p.snapshot_precision) : "f") +
+                          "/" + std::to_string(nshots);
         long long cells = 0;
         for (int i = 0; i < nshots; i++) {
             key += "/" + std::to_string(shots[i].nx);
@@ -1354,7 +1418,8 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
                     if (e.code == FWI2D_ERR_ARG) continue;   // shape does not tile these grids
                     throw;
                 }
-                const float ms = time_forward_steps(ctx, 30);
+                float ms = time_forward_steps(ctx, 30);
+                if (grad) ms += time_adjoint_steps(ctx, 30);
                 if (ms < best) {
                     best = ms;
                     chosen = s;
