@@ -454,13 +454,22 @@ def run_batched(local, steps, warmup):
     info = P.plan_info()
     P.close()
     cells = cells_per_step(wl)
+    # average algorithmic HBM bandwidth of each time loop: FP16 snapshots,
+    # 36 + 4 B per forward cell-update, 68 - 4 B per adjoint one
+    peak, peak_kind = peaks()
+    half = cells / 2
+    fwd_gbs = 40 * half / (fwd_ms / 1e3) / 1e9
+    adj_gbs = 64 * half / (adj_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": "elastic_march + band kernels (adjoint + imaging)", "achieved": adj_gbs,
+            "peak": peak, "unit": "GB/s", "frac": adj_gbs / peak, "peak_source": peak_kind,
+            "forward_achieved": fwd_gbs, "forward_frac": fwd_gbs / peak}
     return {"workload": "elastic FWI gradient, %d shots of the batch geometry on cropped grids (mean %d x %d cells, "
                         "mean nt %d), FP16 snapshots" % (len(wl["shots"]),
                                                           np.mean([s["nx"] for s in wl["shots"]]), wl["nz"],
                                                           np.mean([s["nt"] for s in wl["shots"]])),
             "shots": len(wl["shots"]), "ms_per_step": ms, "shots_per_s": len(wl["shots"]) / (ms / 1e3),
             "value": cells / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "cell_updates_per_step": cells,
-            "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "tile_shape": info["tile_shape"],
+            "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "tile_shape": info["tile_shape"], "roofline": roof,
             "snapshot_bytes": info["snapshot_bytes"], "steps": steps, "warmup": warmup}
 
 
