@@ -1678,22 +1678,28 @@ static void download_grad(fwi2d_ctx *ctx, float *grad)
 // and the adjoint source
 //   q[t] = -r[nt-1-t]  (Ht^-1 of the caller's Ht r, reversed, scaled by -1),
 //   then Dt^T (misc.cpp:85-94) when seismotype = 1.
+// Acoustic-elastic data (rows [0, neg_rows) hold the fluid traces): with
+// seismotype = 1 the fluid synthetic is -Dt of the extracted potential, and
+// its adjoint source -Dt^T (we_op.cpp:1033-1040, :1117-1124).
 // k_misfit_rows adds the chunk partials of each trace in double.
 constexpr int kResChunk = 64;
 
 __global__ void k_residual(const float *__restrict__ u, const float *__restrict__ obs, float *__restrict__ adj,
                            float *__restrict__ syn_out, float2 *__restrict__ part, int nt, int rows, float dt,
-                           int seismotype)
+                           int seismotype, int neg_rows)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
     const int t0 = blockIdx.y * kResChunk, t1 = min(nt, t0 + kResChunk);
+    const bool neg = seismotype && r < neg_rows;
     auto U = [&](int t) { return u[(long long)t * rows + r]; };
     auto syn = [&](int t) -> float {
         if (!seismotype) return U(t);
-        if (t == 0) return (U(1) - U(0)) / dt;
-        if (t == nt - 1) return (U(nt - 1) - U(nt - 2)) / dt;
-        return (U(t + 1) - U(t - 1)) / (2 * dt);
+        float v;
+        if (t == 0) v = (U(1) - U(0)) / dt;
+        else if (t == nt - 1) v = (U(nt - 1) - U(nt - 2)) / dt;
+        else v = (U(t + 1) - U(t - 1)) / (2 * dt);
+        return neg ? -v : v;
     };
     auto res = [&](int t) { return syn(t) - obs[(long long)t * rows + r]; };
     float sum = 0.f, comp = 0.f;
@@ -1715,7 +1721,7 @@ __global__ void k_residual(const float *__restrict__ u, const float *__restrict_
         else if (t == 0) a = (q(1) + q(0)) / dt;
         else if (t == nt - 1) a = (-q(nt - 1) - q(nt - 2)) / dt;
         else a = (q(t + 1) - q(t - 1)) / (2 * dt);
-        adj[(long long)t * rows + r] = a;
+        adj[(long long)t * rows + r] = neg ? -a : a;
     }
 }
 
@@ -1809,7 +1815,7 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
         dim3 grid((S->nrcv_rows + 127) / 128, nchunk);
         k_residual<<<grid, 128, 0, ctx->st>>>(S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off,
                                               S->src_a.as<float>(), nullptr, P.d_part.as<float2>(), S->nt,
-                                              S->nrcv_rows, P.par.dt, seismotype);
+                                              S->nrcv_rows, P.par.dt, seismotype, P.ae ? S->nr : 0);
         k_misfit_rows<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
             P.d_part.as<float2>(), P.d_misfit.as<double>() + row_off, S->nrcv_rows, nchunk);
         CK(cudaGetLastError());

@@ -213,6 +213,28 @@ class Reference(_Lib):
             raise RuntimeError("reference misfit/gradient failed")
         return syn, g
 
+    def misfit_grad_ae(self, par, nx, nz, d, oz, nt, dt, src_loc, rcv_x, rcv_z, rcv_zw, model_raw, src, obs=None):
+        """Acoustic-elastic forward data [3][nr][nt] (fluid, x, z; seismotype 1)
+        and, with obs, the solver's gradient (ref_misfit_grad_ae).  The model
+        grid's first row is at depth oz; the fluid layer lies above it."""
+        f = self.lib.ref_misfit_grad_ae
+        vp = ctypes.c_void_p
+        f.argtypes = [ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                      ctypes.c_double, ctypes.c_int, ctypes.c_double, self._real(), self._real(), ctypes.c_int,
+                      vp, vp, vp, vp, vp, vp, vp, vp]
+        rx, rz, rzw = self.arr(rcv_x), self.arr(rcv_z), self.arr(rcv_zw)
+        nr = len(rx)
+        m = self.arr(model_raw)
+        s = self.arr(src)
+        syn = np.zeros((3, nr, nt), self.dtype)
+        o = None if obs is None else self.arr(obs)
+        g = None if obs is None else np.zeros(m.shape, self.dtype)
+        rc = f(ctypes.byref(par), nx, nz, d, d, oz, nt, dt, src_loc[0], src_loc[1], nr, _ptr(rx), _ptr(rz),
+               _ptr(rzw), _ptr(m), _ptr(s), _ptr(o), _ptr(syn), _ptr(g))
+        if rc != 0:
+            raise RuntimeError("reference acoustic-elastic misfit/gradient failed")
+        return syn, g
+
     def _real(self):
         return ctypes.c_float if self.dtype == np.float32 else ctypes.c_double
 

@@ -140,6 +140,60 @@ int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, do
     return 0;
 }
 
+// The acoustic-elastic solver gradient (nl_we_op_ae through nl_we_op_e's
+// apply_forward / apply_jacobianT): model [3][nx][nz] (vp, vs, rho) on a grid
+// whose first row is at depth oz, the fluid layer above it; one source at
+// (sx, sz) (in the fluid when acoustic_source, its traces [1][nt], else on the
+// elastic grid, [2][nt]); nr receivers at (rx, rz) on the elastic grid and
+// (rx, rzw) in the fluid.  Data [3][nr][nt] (fluid, x, z), seismotype 1.
+int ref_misfit_grad_ae(const ref_param *rp, int nx, int nz, double dx, double dz, double oz, int nt, double dt,
+                       data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *rzw,
+                       const data_t *model, const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
+{
+    try {
+        param par = to_param(rp);
+        par.nt = nt;
+        par.dt = (data_t)dt;
+        par.sub = obs ? 1 : 0;
+        par.ns = 1;
+        par.nr = nr;
+        par.nmodels = 3;
+        par.acoustic_elastic = true;
+        par.seismotype = 1;
+        par.resampling = "linear";
+        data_t sl[2] = {sx, sz};
+        par.sxz = locs(1, sl, sl + 1);
+        par.rxz = {locs(nr, rx, rz)};
+        std::vector<data_t> rxw(rx, rx + nr);
+        par.rxza = {locs(nr, rxw.data(), rzw)};
+        hypercube<data_t> dom(axis<data_t>(nz, (data_t)oz, (data_t)dz), axis<data_t>(nx, 0, (data_t)dx),
+                              axis<data_t>(3, 0, 1));
+        const int ncs = par.acoustic_source ? 1 : 2;
+        auto allsrc = std::make_shared<vecReg<data_t> >(hypercube<data_t>(axis<data_t>(nt, 0, (data_t)dt), axis<data_t>(ncs, 0, 1)));
+        std::memcpy(allsrc->getVals(), src, ncs * (size_t)nt * sizeof(data_t));
+        auto op = std::make_shared<nl_we_op_ae>(dom, allsrc, par);
+        auto m = std::make_shared<vecReg<data_t> >(dom);
+        std::memcpy(m->getVals(), model, m->getN123() * sizeof(data_t));
+        auto d = std::make_shared<vecReg<data_t> >(*op->getRange());
+        op->forward(false, m, d);
+        std::memcpy(syn, d->getCVals(), d->getN123() * sizeof(data_t));
+        if (obs) {
+            auto r = std::make_shared<vecReg<data_t> >(*op->getRange());
+            data_t *pr = r->getVals();
+            const long n = (long)r->getN123();
+            for (long i = 0; i < n; i++) pr[i] = syn[i] - obs[i];
+            applyHt(false, false, pr, pr, 3 * nr, nt, (data_t)dt, 0, 3 * nr);
+            auto g = std::make_shared<vecReg<data_t> >(dom);
+            op->jacobianT(false, g, m, r);
+            std::memcpy(grad, g->getCVals(), g->getN123() * sizeof(data_t));
+        }
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_misfit_grad_ae: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
 // kind: 0 elastic, 1 VTI, 2 acoustic, 3 acoustic-elastic.
 // inj/ext locations are on the (elastic) grid; for kind 3 the water-layer
 // source (sa) and receiver (ra) locations are passed too.

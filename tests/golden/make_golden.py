@@ -135,6 +135,36 @@ def fwi_case(kind):
                 dot_sum2=sum2, grad_dot=gd)
 
 
+def fwi_case_ae():
+    """The acoustic-elastic solver gradient (nl_we_op_ae through the
+    operator interface, residual weighted by applyHt), fluid source."""
+    lib = O.Reference(32)
+    nx, nz, d, nt, dt = 90, 60, 0.01, 300, 1e-3
+    nza = 16
+    oz = (nza - 1) * d
+    true = K.model_case(O.KIND_ELASTIC, nx, nz, d, seed=17)
+    true[0] += 0.5
+    true[1] = true[0] / 1.8
+    start = true.copy()
+    from scipy.ndimage import gaussian_filter
+    for c in range(3):
+        start[c] = gaussian_filter(true[c].astype(np.float64), 4, mode="nearest").astype(np.float32)
+    sx, sz = np.float32(0.41 * nx * d), np.float32(0.05)
+    rx = np.linspace(3 * d, (nx - 4) * d, 24).astype(np.float32)
+    rz = np.full(24, oz + 0.02, np.float32)
+    rzw = np.full(24, 0.03, np.float32)
+    src = K.sources(1, nt, dt, f0=15.0).reshape(1, nt)
+    par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(2, 2, 2, 2), taper=(4, 10, 10, 10)), ns=1, nr=24, nza=nza,
+                     acoustic_source=1)
+    obs, _ = lib.misfit_grad_ae(par, nx, nz, d, oz, nt, dt, (sx, sz), rx, rz, rzw, true, src)
+    syn0, g = lib.misfit_grad_ae(par, nx, nz, d, oz, nt, dt, (sx, sz), rx, rz, rzw, start, src, obs)
+    w = np.full(nt, dt)
+    w[0] = w[-1] = 0.5 * dt
+    r = syn0.astype(np.float64) - obs
+    return dict(nx=nx, nz=nz, d=d, nt=nt, dt=dt, nza=nza, oz=oz, sx=sx, sz=sz, rx=rx, rz=rz, rzw=rzw, true=true,
+                start=start, src=src, obs=obs, grad=g, misfit=0.5 * np.sum(w * r * r))
+
+
 def main():
     if not O.have_reference(32):
         sys.exit("oracle/_ref is not built (oracle/build_ref.sh needs the reference tree)")
@@ -145,6 +175,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, "acoustic_elastic_f%d.npz" % prec), **ae_case(prec))
     for kind, name in ((O.KIND_ELASTIC, "elastic"), (O.KIND_VTI, "vti")):
         np.savez_compressed(os.path.join(HERE, "fwi_gradient_%s_f32.npz" % name), **fwi_case(kind))
+    np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_f32.npz"), **fwi_case_ae())
     print("golden fixtures written to", HERE)
 
 

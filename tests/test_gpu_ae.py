@@ -151,3 +151,27 @@ def test_ae_dropin_propagate_matches_reference_golden():
                               nx, nz, d, d))
     print("AE drop-in gradient: bitwise %.4f, rel-L2 %.2e" % (np.mean(grad == g["grad"]), K.rel_l2(grad, g["grad"])))
     assert K.rel_l2(grad, g["grad"]) <= 1e-5
+
+
+def test_ae_fwi_gradient_matches_reference_solver():
+    """fwi2d_fwi_gradient on the acoustic-elastic propagator against the
+    reference solver's gradient (nl_we_op_ae through nl_we_op_e's
+    apply_forward / apply_jacobianT, fluid traces -Dt of the potential),
+    tests/golden/fwi_gradient_ae_f32.npz."""
+    from fwi2d_b200 import workloads as W
+    g = dict(np.load(os.path.join(GOLD, "fwi_gradient_ae_f32.npz")))
+    nx, nz, d, nt, dt, nza, oz = (int(g["nx"]), int(g["nz"]), float(g["d"]), int(g["nt"]), float(g["dt"]),
+                                  int(g["nza"]), float(g["oz"]))
+    P = F.Propagator(0)
+    P.set_model(O.KIND_AE, W.convert(O.KIND_ELASTIC, g["start"]), d, d, 0.0, oz)
+    pd = K.par_dict(nt=nt, dt=dt, bc=(2, 2, 2, 2), taper=(4, 10, 10, 10), nza=nza, acoustic_source=1)
+    P.set_shots(F.make_params(**pd, tile_shape=3),
+                [F.ShotSpec(0, nx, nt, [0.0], [oz], g["rx"], g["rz"], water_src_x=[float(g["sx"])],
+                            water_src_z=[float(g["sz"])], water_rcv_x=g["rx"], water_rcv_z=g["rzw"])])
+    grad, phi = P.fwi_gradient(W.convert(O.KIND_ELASTIC, g["start"]), [g["src"]], [g["obs"]], seismotype=1)
+    P.close()
+    err = K.rel_l2(grad, g["grad"])
+    print("AE FWI gradient vs reference solver: rel-L2 %.3e (bitwise %.4f), misfit %.9e vs %.9e" % (
+        err, np.mean(grad == g["grad"]), phi, float(g["misfit"])))
+    assert err <= 1e-4
+    assert abs(phi - float(g["misfit"])) <= 1e-5 * float(g["misfit"])

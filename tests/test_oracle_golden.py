@@ -83,6 +83,16 @@ def test_fwi_gradient_fixture_reproduced_by_reference_build(path):
         pytest.skip("oracle/_ref is not built")
     g = dict(np.load(path))
     lib = O.Reference(32)
+    if "nza" in g:   # acoustic-elastic
+        nx, nz, d, nt, dt, nza = int(g["nx"]), int(g["nz"]), float(g["d"]), int(g["nt"]), float(g["dt"]), int(g["nza"])
+        par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(2, 2, 2, 2), taper=(4, 10, 10, 10)), ns=1, nr=len(g["rx"]),
+                         nza=nza, acoustic_source=1)
+        args = (par, nx, nz, d, float(g["oz"]), nt, dt, (g["sx"], g["sz"]), g["rx"], g["rz"], g["rzw"])
+        syn, _ = lib.misfit_grad_ae(*args, g["true"], g["src"])
+        assert np.array_equal(syn, g["obs"])
+        _, grad = lib.misfit_grad_ae(*args, g["start"], g["src"], g["obs"])
+        assert np.array_equal(grad, g["grad"])
+        return
     kind, nx, nz, d, nt, dt = int(g["kind"]), int(g["nx"]), int(g["nz"]), float(g["d"]), int(g["nt"]), float(g["dt"])
     par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=len(g["rx"]))
     geo = ((np.float32(g["sx"]), np.float32(g["sz"])), (g["rx"], g["rz"]))
