@@ -168,6 +168,7 @@ struct ModelState {
     float dx = 0, dz = 0;
     std::vector<float> host;   // converted model as given, [npar][nx][nz]
     DevBuf p0, p1, p2, c13, eps, fxx, lbis, gv2, gv3;
+    DevBuf stage;              // unpitched upload staging, [nx][nz]
     ModelDev dev() const
     {
         ModelDev m;
@@ -338,18 +339,19 @@ static void upload_model_values(fwi2d_ctx *ctx, const float *model)
     M.host.assign(model, model + nxz * M.npar);
     for (size_t i = 0; i < M.host.size(); i++) REQ(std::isfinite(M.host[i]), "model holds a non-finite value");
     const size_t pitched = (size_t)nx * M.ldz;
-    DevBuf stage;
-    stage.alloc(nxz * sizeof(float));
+    M.stage.ensure(nxz * sizeof(float));
+    // every upload goes through the one staging buffer, in stream order; the
+    // sources stay valid until the synchronisation at the end
     auto up = [&](DevBuf &dst, const float *src) {
         dst.ensure(pitched * sizeof(float));
-        CK(cudaMemcpyAsync(stage.p, src, nxz * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-        k_pitch<<<592, 256, 0, ctx->st>>>(stage.as<float>(), dst.as<float>(), nx, nz, M.ldz);
+        CK(cudaMemcpyAsync(M.stage.p, src, nxz * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        k_pitch<<<592, 256, 0, ctx->st>>>(M.stage.as<float>(), dst.as<float>(), nx, nz, M.ldz);
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(ctx->st));
     };
-    up(M.p0, M.hp(0));
-    up(M.p1, M.hp(1));
-    if (kind != KIND_ACOUSTIC) up(M.p2, M.hp(2));
+    // device copies straight from the caller's array (which may be pinned)
+    up(M.p0, model);
+    up(M.p1, model + nxz);
+    if (kind != KIND_ACOUSTIC) up(M.p2, model + 2 * nxz);
     else M.p2.release();
     M.c13.release();
     M.eps.release();
@@ -376,6 +378,7 @@ static void upload_model_values(fwi2d_ctx *ctx, const float *model)
         up(M.gv2, v2.data());
         up(M.gv3, v3.data());
     }
+    CK(cudaStreamSynchronize(ctx->st));
 }
 
 // ---- plan construction -------------------------------------------------------
@@ -1595,13 +1598,14 @@ static void upload_traces(fwi2d_ctx *ctx, const float *traces, bool adjoint)
         const size_t n = (size_t)rows * S->nt;
         for (size_t i = 0; i < n; i++)
             if (!std::isfinite(p[i])) throw Error(FWI2D_ERR_ARG, "trace array holds a non-finite value");
+        // the staging buffer is reused by the next shot in stream order
         CK(cudaMemcpyAsync(P.d_stage.p, p, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
         launch_to_time_major(P.d_stage.as<float>(), (adjoint ? S->src_a : S->src_f).as<float>(), rows, S->nt, ctx->st);
         CK(cudaGetLastError());
         blocks.push_back(p);
         p += n;
-        CK(cudaStreamSynchronize(ctx->st));   // the staging buffer is reused by the next shot
     }
+    CK(cudaStreamSynchronize(ctx->st));   // the caller's traces may be reused on return
 }
 
 static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
@@ -1779,11 +1783,17 @@ static void update_model(fwi2d_ctx *ctx, const float *model)
     const fwi2d_params &p = P.par;
     for (auto &S : P.shots) {
         std::vector<float> den;
-        const float *lam = M.hp(0) + (size_t)S->x0 * M.nz, *mu = M.hp(1) + (size_t)S->x0 * M.nz,
-                    *rho = M.hp(2) + (size_t)S->x0 * M.nz;
-        const float *eps = M.kind == KIND_VTI ? M.hp(4) + (size_t)S->x0 * M.nz : nullptr;
-        elastic_scale_divisors(S->nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, !P.ae && p.bc_top == 2,
-                               p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
+        if (M.kind == KIND_ACOUSTIC) {
+            const float *K = M.hp(0) + (size_t)S->x0 * M.nz, *irho = M.hp(1) + (size_t)S->x0 * M.nz;
+            acoustic_scale_divisors(S->nx, M.nz, M.dx, M.dz, p.dt, K, irho, M.nz, p.bc_top == 2, p.bc_bottom == 2,
+                                    p.bc_left == 2, p.bc_right == 2, den);
+        } else {
+            const float *lam = M.hp(0) + (size_t)S->x0 * M.nz, *mu = M.hp(1) + (size_t)S->x0 * M.nz,
+                        *rho = M.hp(2) + (size_t)S->x0 * M.nz;
+            const float *eps = M.kind == KIND_VTI ? M.hp(4) + (size_t)S->x0 * M.nz : nullptr;
+            elastic_scale_divisors(S->nx, M.nz, M.dx, M.dz, p.dt, lam, mu, rho, eps, M.nz, !P.ae && p.bc_top == 2,
+                                   p.bc_bottom == 2, p.bc_left == 2, p.bc_right == 2, den);
+        }
         S->den.upload(den, ctx->st);
     }
     init_factors(M, P);
@@ -1851,9 +1861,9 @@ static void set_observed(fwi2d_ctx *ctx, const float *obs)
         CK(cudaMemcpyAsync(P.d_stage.p, obs + off, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
         launch_to_time_major(P.d_stage.as<float>(), P.d_obs.as<float>() + off, S->nrcv_rows, S->nt, ctx->st);
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(ctx->st));
         off += n;
     }
+    CK(cudaStreamSynchronize(ctx->st));
 }
 
 static double read_misfit(fwi2d_ctx *ctx)
