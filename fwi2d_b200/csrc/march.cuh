@@ -504,8 +504,11 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD, UNR> &Q, MarchCtx &X, fl
 #define MARCH_FWD_UNROLL 2
 #endif
 
+#ifndef MARCH_FWD_MIN_BLOCKS
+#define MARCH_FWD_MIN_BLOCKS 3
+#endif
 template <bool VTI, bool GRAD, int NTH>
-__global__ void __launch_bounds__(NTH, (GRAD || NTH > 224) ? 2 : 3)
+__global__ void __launch_bounds__(NTH, (GRAD || NTH > 224) ? 2 : MARCH_FWD_MIN_BLOCKS)
 elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ units, ModelDev M, StepConst C, int it,
               int flags, float dtg)
 {
