@@ -150,6 +150,9 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     // the lean path writes every cell of its window: only for tiles that own all of it
     const bool full = tr.ox0 == wx0 && tr.ox1 == wx0 + TX && tr.oz0 == wz0 && tr.oz1 == wz0 + TZ;
     const bool lean = !AE && RZ == 2 && interior && full && (wz0 & 3) == 0;
+    // one cell per thread: tiles clear of the boundary bands take the scalar
+    // interior forms (no closure code, which keeps the hot loop small)
+    const bool lean1 = !AE && RZ == 1 && interior && full;
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
@@ -276,6 +279,26 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             if (VTI) *reinterpret_cast<float2 *>(T1 + wo) = t1;
             *reinterpret_cast<float2 *>(BX + wo) = bx;
             *reinterpret_cast<float2 *>(CZ + wo) = cz;
+        }
+    } else if (lean1) {
+        for (int i = threadIdx.x; i < WX * WZ; i += NT) {
+            const int sx = i / WZ, sz = i - sx * WZ;
+            const int ui = (sx + 2) * UZ + (sz + 2);
+            const float ux_x = d1i(U0 + ui, UZ, C.sdx);
+            const float uz_z = d1i(U1 + ui, 1, C.sdz);
+            float t0, t1 = 0.f;
+            if (!VTI) {
+                t0 = ux_x + uz_z;
+            } else {
+                const long long o = mofs + (long long)(wx0 - 2 + sx) * mld + wz0 - 2 + sz;
+                const float lb = M.lbis[o], c13 = M.c13[o], lam = M.p0[o];
+                t0 = lb * ux_x + c13 * uz_z;
+                t1 = lam * uz_z + c13 * ux_x;
+            }
+            T0[i] = t0;
+            if (VTI) T1[i] = t1;
+            BX[i] = d1i(U1 + ui, UZ, C.sdx);
+            CZ[i] = d1i(U0 + ui, 1, C.sdz);
         }
     } else {
         for (int i = threadIdx.x; i < WX * WZ; i += NT) {
@@ -505,6 +528,117 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             *reinterpret_cast<float2 *>(g0) = G0;
             *reinterpret_cast<float2 *>(g1) = G1;
             *reinterpret_cast<float2 *>(g2) = G2;
+        }
+    } else if (lean1) {
+        // the general path's arithmetic in its interior forms (sbp.cuh d1i,
+        // md1i, d2i): no SAT and no boundary divisor can reach these cells
+        const int gx = wx0 + warp, gz = wz0 + lane;
+        const int ui = (warp + 4) * UZ + (lane + 4);
+        const int wi = (warp + 2) * WZ + (lane + 2);
+        const int cell = gx * ldz + gz;
+        const int mcell = gx * mld + gz;
+        if (store) {
+            const int slot = it / C.sub;
+            const float sc = prec == SNAP_FP32 ? 1.f : snap_scale(Sp->snap_amax, slot);
+            const long long o = (long long)slot * slot_elems + cell;
+            snap_store(Sp->snap, o, prec, U0[ui], sc);
+            snap_store(Sp->snap, o + nxz, prec, U1[ui], sc);
+        }
+        float n0 = 0.f, n1 = 0.f;
+        if (!VTI) {
+            n0 = d2i(n0, twice(brackets(MU + wi, WZ)), U0 + ui, UZ, C.inv_d2x);
+            n1 = d2i(n1, twice(brackets(MU + wi, 1)), U1 + ui, 1, C.inv_d2z);
+        } else {
+            n0 = d2i(n0, brackets(Q + wi, WZ), U0 + ui, UZ, C.inv_d2x);
+            n1 = d2i(n1, twice(brackets(MU + wi, 1)), U1 + ui, 1, C.inv_d2z);
+        }
+        n1 = d2i(n1, brackets(MU + wi, WZ), U1 + ui, UZ, C.inv_d2x);
+        n0 = d2i(n0, brackets(MU + wi, 1), U0 + ui, 1, C.inv_d2z);
+        if (!VTI) {
+            n0 += md1i(T0 + wi, Q + wi, WZ, C.adx);
+            n1 += md1i(T0 + wi, Q + wi, 1, C.adz);
+        } else {
+            n0 += d1i(T0 + wi, WZ, C.sdx);
+            n1 += d1i(T1 + wi, 1, C.sdz);
+        }
+        n1 += md1i(CZ + wi, MU + wi, WZ, C.adx);
+        n0 += md1i(BX + wi, MU + wi, 1, C.adz);
+        for (int e = e0; e < e1; e++) {
+            const InjEntry &E = Sp->inj[e];
+            if (E.gx == gx && E.gz == gz) {
+                const float v = E.mt ? (E.wa * srcrow[E.ia] - E.wb * srcrow[E.ib]) : E.wa * srcrow[E.ia];
+                if (E.comp == 0) n0 += v;
+                else n1 += v;
+            }
+        }
+        const float tzv = Sp->tz[gz], txv = Sp->tx[gx];
+        float p0 = pn[cell], p1 = pn[nxz + cell];
+        if (it > 0) {
+            p0 = p0 * tzv * txv;
+            p1 = p1 * tzv * txv;
+        }
+        const float rho = mp2[mcell];
+        n0 = C.dt2 * n0 / rho + 2 * U0[ui] - p0;
+        n1 = C.dt2 * n1 / rho + 2 * U1[ui] - p1;
+        n0 = n0 * tzv * txv;
+        n1 = n1 * tzv * txv;
+        pn[cell] = n0;
+        pn[nxz + cell] = n1;
+        amax = fmaxf(amax, fmaxf(fabsf(n0), fabsf(n1)));
+        if (GRAD && do_grad) {
+            const float ax0 = d1i(U0 + ui, UZ, C.sdx);
+            const float az1 = d1i(U1 + ui, 1, C.sdz);
+            const float t0 = d1i(F0 + wi, WZ, C.sdx);
+            const float t1 = d1i(F1 + wi, 1, C.sdz);
+            const float t2 = d1i(F1 + wi, WZ, C.sdx);
+            const float t3 = d1i(F0 + wi, 1, C.sdz);
+            const float az0 = CZ[wi], ax1 = BX[wi];
+            const int last = nt / C.sub;
+            const float f0 = F0[wi], f1 = F1[wi];
+            float fp0 = 0.f, fp1 = 0.f, fm0 = 0.f, fm1 = 0.f;
+            if (itf + 1 <= last) {
+                const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf + 1);
+                const long long o = (long long)(itf + 1) * slot_elems + cell;
+                fp0 = snap_load(snap, o, prec, inv);
+                fp1 = snap_load(snap, o + nxz, prec, inv);
+            }
+            if (itf > 0) {
+                const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
+                const long long o = (long long)(itf - 1) * slot_elems + cell;
+                fm0 = snap_load(snap, o, prec, inv);
+                fm1 = snap_load(snap, o + nxz, prec, inv);
+            }
+            float dl, dm;
+            if (!VTI) {
+                dl = 0.f;
+                dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
+            } else {
+                const long long mo = mofs + mcell;
+                const float e2 = 1 + 2 * M.eps[mo];
+                const float v2 = M.gv2[mo], v3 = M.gv3[mo];
+                dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
+                dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
+            }
+            float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
+            const float gw = Sp->gwt[itf];
+            const double wdt = (double)gw * 1.0 / (double)dtg;
+            if (itf > 0 && itf < last) {
+                if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                else *g0 = *g0 + gw * dtg * dl;
+                *g1 = *g1 + gw * dtg * dm;
+                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
+            } else if (itf == 0) {
+                const double wh = (double)gw * 0.5 * (double)dtg;
+                if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
+                else *g0 = (float)((double)*g0 + wh * (double)dl);
+                *g1 = (float)((double)*g1 + wh * (double)dm);
+                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
+            } else {
+                if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                else *g0 = *g0 + gw * dtg * dl;
+                *g1 = *g1 + gw * dtg * dm;
+                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
+            }
         }
     } else {
 #pragma unroll
