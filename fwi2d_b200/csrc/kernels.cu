@@ -173,7 +173,8 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     const void *snap = Sp->snap;
 
     // ---- phase 1: curr with a 4-cell halo, coefficients (and snapshot) with a 2-cell halo
-    if (lean) {
+    // (vector loads for interior tiles that start on a multiple of 4 cells)
+    if (lean || (lean1 && (wz0 & 3) == 0)) {
         constexpr int Q4 = UZ / 4;   // float4 per window row
         for (int f = threadIdx.x; f < UX * Q4; f += NT) {
             const int r = f / Q4, q = f - r * Q4;
