@@ -66,7 +66,7 @@ def peaks():
 # the adjoint tile kernel on the single-shot grid, from the ncu capture
 # summarised in profiles/elastic_step_adjoint_single_shot_401x801.md
 # (cold caches: ncu flushes L2 before each pass).
-ADJ_TILE_TRAFFIC_BYTES = 21.73696e6
+ADJ_TILE_TRAFFIC_BYTES = 21.756928e6
 
 
 # ---------------------------------------------------------------------------
