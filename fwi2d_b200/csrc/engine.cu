@@ -1742,11 +1742,12 @@ __global__ void k_misfit_rows(const float2 *__restrict__ part, double *__restric
 }
 
 // H quadrature (spatial_operators.cpp:6-98) and the chain rule from
-// (lambda, mu, rho) to (vp, vs, rho) (we_op.cpp:1193-1228), in place on the
-// pitched model-grid gradient.
+// (lambda, mu, rho) to (vp, vs, rho), or from (K, 1/rho) to (vp, rho) for the
+// acoustic propagator (we_op.cpp:1193-1228), in place on the pitched
+// model-grid gradient.  Acoustic: lam = K, mu = 1/rho, rho unused.
 __global__ void k_quadrature_chain(float *__restrict__ g, const float *__restrict__ lam, const float *__restrict__ mu,
                                    const float *__restrict__ rho, int nx, int nz, int ldz, float dx, float dz,
-                                   float h0, float h1, float h2, float h3)
+                                   float h0, float h1, float h2, float h3, int acoustic)
 {
     const long long n = (long long)nx * ldz;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -1755,12 +1756,18 @@ __global__ void k_quadrature_chain(float *__restrict__ g, const float *__restric
         const float hc[4] = {h0, h1, h2, h3};
         const float wz = iz < 4 ? hc[iz] : (iz >= nz - 4 ? hc[nz - 1 - iz] : 1.f);
         const float wx = ix < 4 ? hc[ix] : (ix >= nx - 4 ? hc[nx - 1 - ix] : 1.f);
-        float g0 = g[i], g1 = g[n + i], g2 = g[2 * n + i];
+        float g0 = g[i], g1 = g[n + i], g2 = acoustic ? 0.f : g[2 * n + i];
         // applyHz then applyHx on each component
         if (iz < 4 || iz >= nz - 4) { g0 = g0 * wz * dz; g1 = g1 * wz * dz; g2 = g2 * wz * dz; }
         else { g0 = g0 * dz; g1 = g1 * dz; g2 = g2 * dz; }
         if (ix < 4 || ix >= nx - 4) { g0 = g0 * wx * dx; g1 = g1 * wx * dx; g2 = g2 * wx * dx; }
         else { g0 = g0 * dx; g1 = g1 * dx; g2 = g2 * dx; }
+        if (acoustic) {
+            const float K = lam[i], ir = mu[i];
+            g[n + i] = ir * K * g0 - ir * ir * g1;                            // rho
+            g[i] = (float)(2 * sqrt((double)(K / ir)) * (double)g0);          // vp
+            continue;
+        }
         const float l = lam[i], m = mu[i], r = rho[i];
         const float n2 = (l / r) * g0 + (m / r) * g1 + g2;
         const float n1 = (float)(2 * sqrt((double)(m * r)) * (double)(g1 - 2 * g0));
@@ -1833,12 +1840,12 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
         row_off += S->nrcv_rows;
     }
     run(ctx, true, false);
-    if (chain && P.kind != KIND_ACOUSTIC) {
+    if (chain) {
         const ModelState &M = ctx->M;
         const SbpTables &t = sbp_tables();
         k_quadrature_chain<<<592, 256, 0, ctx->st>>>(P.d_grad_full.as<float>(), M.p0.as<float>(), M.p1.as<float>(),
                                                      M.p2.as<float>(), M.nx, M.nz, M.ldz, M.dx, M.dz, t.hc[0], t.hc[1],
-                                                     t.hc[2], t.hc[3]);
+                                                     t.hc[2], t.hc[3], P.kind == KIND_ACOUSTIC ? 1 : 0);
         CK(cudaGetLastError());
     }
 }

@@ -200,12 +200,13 @@ class Propagator:
         C.check(self.L.fwi2d_set_observed(self.h, C.ptr(buf)))
 
     def fwi_gradient(self, model=None, src_blocks=None, obs_blocks=None, seismotype=1, download=True):
-        """One device FWI gradient: returns ((vp, vs, rho) gradient, misfit)
-        or (None, None) with download=False."""
+        """One device FWI gradient: returns ((vp, vs, rho) gradient -- (vp, rho)
+        for the acoustic propagator -- and the misfit), or (None, None) with
+        download=False."""
         m = None if model is None else np.ascontiguousarray(model, np.float32)
         src = None if src_blocks is None else self._concat(src_blocks, self.src_rows)
         obs = None if obs_blocks is None else self._concat(obs_blocks, self.rcv_rows)
-        g = np.zeros((3, self.nx, self.nz), np.float32) if download else None
+        g = np.zeros((self.ngrad(), self.nx, self.nz), np.float32) if download else None
         f = ctypes.c_double(0.0)
         C.check(self.L.fwi2d_fwi_gradient(self.h, C.ptr(m), C.ptr(src), C.ptr(obs), int(seismotype), C.ptr(g),
                                           ctypes.byref(f) if download else None))

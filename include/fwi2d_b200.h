@@ -138,9 +138,10 @@ int fwi2d_set_observed(fwi2d_ctx *ctx, const float *obs);
  * snapshots, residual against the observed data (seismotype 1: particle
  * velocity, the time derivative of the extracted displacement), L2 misfit
  * 1/2 dt (|r|^2 - (r_0^2 + r_end^2)/2), adjoint sources, adjoint propagation
- * with the imaging condition, H quadrature and the chain rule to (vp, vs, rho).
- * model / src / obs may be NULL to reuse what is resident; grad (host
- * [3][nx][nz]) and misfit may be NULL to leave the results on the device. */
+ * with the imaging condition, H quadrature and the chain rule to (vp, vs, rho),
+ * or (vp, rho) for the acoustic propagator.  model / src / obs may be NULL to
+ * reuse what is resident; grad (host [3 or 2][nx][nz]) and misfit may be NULL
+ * to leave the results on the device. */
 int fwi2d_fwi_gradient(fwi2d_ctx *ctx, const float *model, const float *src, const float *obs, int seismotype,
                        float *grad, double *misfit);
 

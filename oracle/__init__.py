@@ -195,7 +195,8 @@ class Reference(_Lib):
     def misfit_grad(self, kind, par, nx, nz, d, nt, dt, src_loc, rcv_locs, model_raw, src, obs=None):
         """The reference operator's forward data (seismotype 1) and, with obs,
         the solver's gradient for residual f(m) - obs (ref_misfit_grad).
-        Returns (syn [2][nr][nt], grad or None)."""
+        Returns (syn [ncomp][nr][nt], grad or None); ncomp 1 for the
+        acoustic propagator, else 2."""
         f = self.lib.ref_misfit_grad
         vp = ctypes.c_void_p
         f.argtypes = [ctypes.c_int, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
@@ -203,8 +204,9 @@ class Reference(_Lib):
         rx, rz = self.arr(rcv_locs[0]), self.arr(rcv_locs[1])
         nr = len(rx)
         m = self.arr(model_raw)
-        s = self.arr(src).reshape(2, nt)
-        syn = np.zeros((2, nr, nt), self.dtype)
+        nc = 1 if kind == KIND_ACOUSTIC else 2
+        s = self.arr(src).reshape(nc, nt)
+        syn = np.zeros((nc, nr, nt), self.dtype)
         o = None if obs is None else self.arr(obs)
         g = None if obs is None else np.zeros(m.shape, self.dtype)
         rc = f(kind, ctypes.byref(par), nx, nz, d, d, nt, dt, src_loc[0], src_loc[1], nr, _ptr(rx), _ptr(rz), _ptr(m),

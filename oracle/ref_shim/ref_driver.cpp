@@ -105,7 +105,8 @@ int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, do
         par.sub = obs ? 1 : 0;
         par.ns = 1;
         par.nr = nr;
-        par.nmodels = kind == 1 ? 5 : 3;
+        par.nmodels = kind == 1 ? 5 : (kind == 2 ? 2 : 3);
+        const int nc = kind == 2 ? 1 : 2;   // trace components (sources and receivers)
         par.seismotype = 1;
         par.resampling = "linear";
         data_t sl[2] = {sx, sz};
@@ -113,11 +114,12 @@ int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, do
         par.rxz = {locs(nr, rx, rz)};
         hypercube<data_t> dom(axis<data_t>(nz, 0, (data_t)dz), axis<data_t>(nx, 0, (data_t)dx),
                               axis<data_t>(par.nmodels, 0, 1));
-        auto allsrc = std::make_shared<vecReg<data_t> >(hypercube<data_t>(axis<data_t>(nt, 0, (data_t)dt), axis<data_t>(2, 0, 1)));
-        std::memcpy(allsrc->getVals(), src, 2 * (size_t)nt * sizeof(data_t));
+        auto allsrc = std::make_shared<vecReg<data_t> >(hypercube<data_t>(axis<data_t>(nt, 0, (data_t)dt), axis<data_t>(nc, 0, 1)));
+        std::memcpy(allsrc->getVals(), src, nc * (size_t)nt * sizeof(data_t));
         std::shared_ptr<nl_we_op> op;
         if (kind == 0) op = std::make_shared<nl_we_op_e>(dom, allsrc, par);
-        else op = std::make_shared<nl_we_op_vti>(dom, allsrc, par);
+        else if (kind == 1) op = std::make_shared<nl_we_op_vti>(dom, allsrc, par);
+        else op = std::make_shared<nl_we_op_a>(dom, allsrc, par);
         auto m = std::make_shared<vecReg<data_t> >(dom);
         std::memcpy(m->getVals(), model, m->getN123() * sizeof(data_t));
         auto d = std::make_shared<vecReg<data_t> >(*op->getRange());
@@ -128,7 +130,7 @@ int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, do
             data_t *pr = r->getVals();
             const long n = (long)r->getN123();
             for (long i = 0; i < n; i++) pr[i] = syn[i] - obs[i];
-            applyHt(false, false, pr, pr, 2 * nr, nt, (data_t)dt, 0, 2 * nr);
+            applyHt(false, false, pr, pr, nc * nr, nt, (data_t)dt, 0, nc * nr);
             auto g = std::make_shared<vecReg<data_t> >(dom);
             op->jacobianT(false, g, m, r);
             std::memcpy(grad, g->getCVals(), g->getN123() * sizeof(data_t));

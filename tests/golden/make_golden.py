@@ -88,7 +88,7 @@ def ae_case(prec):
 
 def fwi_case(kind):
     """The solver's gradient through the reference's operator interface
-    (nl_we_op_e / nl_we_op_vti forward + apply_jacobianT, residual weighted by
+    (nl_we_op_e / nl_we_op_vti / nl_we_op_a forward + apply_jacobianT, residual weighted by
     applyHt), with the finite-difference directional derivative and the
     nonlinear dot-product test (nloper::dotProduct) evaluated on the reference
     itself."""
@@ -98,14 +98,16 @@ def fwi_case(kind):
     true = K.model_case(kind, nx, nz, d, seed=7)
     start = true.copy()
     from scipy.ndimage import gaussian_filter
-    for c in range(3):
+    npm = true.shape[0] if kind != O.KIND_VTI else 3   # smoothed parameters: (vp, vs, rho) or (vp, rho)
+    for c in range(npm):
         start[c] = gaussian_filter(true[c].astype(np.float64), 4, mode="nearest").astype(np.float32)
     sx, sz = (0.5 * (nx - 1) + 0.3) * d, 0.02
     rx = np.linspace(3 * d, (nx - 4) * d, 30).astype(np.float32)
     rz = np.full(30, 0.02, np.float32)
-    src = K.sources(2, nt, dt).reshape(2, nt)
+    nc = 1 if kind == O.KIND_ACOUSTIC else 2
+    src = K.sources(nc, nt, dt).reshape(nc, nt)
     dm = np.zeros_like(start)
-    for c in range(3):
+    for c in range(npm):
         f = gaussian_filter(rng.uniform(-1, 1, (nx, nz)), 5, mode="nearest")
         dm[c] = f / np.abs(f).max() * start[c]
     par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=30)
@@ -121,11 +123,11 @@ def fwi_case(kind):
     syn0, g = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], start, src, obs)
     eps = 1e-3
     fd = (phi(start + eps * dm) - phi(start - eps * dm)) / (2 * eps)
-    an = float(np.sum(g[:3].astype(np.float64) * dm[:3]))
+    an = float(np.sum(g[:npm].astype(np.float64) * dm[:npm]))
     # nloper::dotProduct: residual d for observed data f(m) - d
     rd = rng.uniform(-1, 1, syn0.shape).astype(np.float32) * np.float32(np.abs(syn0).max())
     _, gd = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], start, src, syn0 - rd)
-    sum2 = float(np.sum(gd[:3].astype(np.float64) * dm[:3]))
+    sum2 = float(np.sum(gd[:npm].astype(np.float64) * dm[:npm]))
     s1 = []
     for e in (1e-2, 1e-3):
         f1, _ = lib.misfit_grad(kind, par, nx, nz, d, nt, dt, geo[0], geo[1], start + e * dm, src)
@@ -173,7 +175,7 @@ def main():
             out = elastic_like(name, kind, mt, bc, nx, nz, nt, prec)
             np.savez_compressed(os.path.join(HERE, "%s_f%d.npz" % (name, prec)), **out)
         np.savez_compressed(os.path.join(HERE, "acoustic_elastic_f%d.npz" % prec), **ae_case(prec))
-    for kind, name in ((O.KIND_ELASTIC, "elastic"), (O.KIND_VTI, "vti")):
+    for kind, name in ((O.KIND_ELASTIC, "elastic"), (O.KIND_VTI, "vti"), (O.KIND_ACOUSTIC, "acoustic")):
         np.savez_compressed(os.path.join(HERE, "fwi_gradient_%s_f32.npz" % name), **fwi_case(kind))
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_f32.npz"), **fwi_case_ae())
     print("golden fixtures written to", HERE)

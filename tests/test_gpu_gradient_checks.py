@@ -2,8 +2,8 @@
 adjoint propagation with the imaging condition, H quadrature and chain rule
 to (vp, vs, rho)) against the reference's solver gradient.
 
-tests/golden/fwi_gradient_{elastic,vti}_f32.npz hold, for one shot on a
-100 x 80 grid, the reference's own gradient (nl_we_op_*::apply_forward and
+tests/golden/fwi_gradient_{elastic,vti,acoustic}_f32.npz hold, for one shot
+on a 100 x 80 grid, the reference's own gradient (nl_we_op_*::apply_forward and
 apply_jacobianT on the applyHt-weighted residual, src/include/optimization.hpp:
 760-890), its misfit, and the finite-difference directional derivative and
 nonlinear dot-product test (nloper::dotProduct, src/cpp/operator.cpp:6-97)
@@ -68,13 +68,13 @@ def _data(P, kind, g, model_raw):
     return _velocity(P.forward([g["src"]], store=False)[0], float(g["dt"]))
 
 
-@pytest.mark.parametrize("name", ["elastic", "vti"])
+@pytest.mark.parametrize("name", ["elastic", "vti", "acoustic"])
 def test_fwi_gradient_matches_reference(name):
     g = _case(name)
     P, kind = _prop(g)
     grad, phi = _grad(P, kind, g, g["start"], g["obs"])
     P.close()
-    ref = g["grad"][:3]
+    ref = g["grad"][:grad.shape[0]]
     err = K.rel_l2(grad, ref)
     print("%s: gradient rel-L2 %.3e (bitwise %.4f)  misfit %.9e vs %.9e" % (
         name, err, np.mean(grad == ref), phi, float(g["misfit"])))
