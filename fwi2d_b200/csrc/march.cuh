@@ -33,10 +33,11 @@
 // rows once per group.  Unrolling all 8 ring phases removes the shifts but
 // overflows the instruction cache.
 //
-// Shared memory, rows of RB = NTH + 24 floats; cell z of a row buffer sits
+// Shared memory, rows of RB = NTH + 16 floats; cell z of a row buffer sits
 // at index z - s0 with s0 = (za - 2) rounded down to a multiple of 8, so that
 // every copy starts and ends on a 16-byte boundary (and 16-bit snapshot rows
-// on 16-byte boundaries too):
+// on 16-byte boundaries too).  za is even, so a row spans at most NTH + 16
+// cells (s0 at most 6 below za - 2, the end at most 6 above za + NTH + 2):
 //   ux, uz, mu, q, f0, f1   8-row rings (q: lambda, or (1+2eps)(lambda+2mu) for VTI)
 //   t, bx                   4-row rings of T0 (VTI: T1) and uz_x
 //   vl, vc, va              4-row rings of the VTI coefficients lbis, c13, lambda
@@ -91,7 +92,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 
 template <bool VTI, bool GRAD, int NTH>
 struct MarchLayout {
-    static constexpr int RB = NTH + 24;
+    static constexpr int RB = NTH + 16;
     static constexpr int UX = 0, UZ = UX + 8 * RB, MU = UZ + 8 * RB, Q = MU + 8 * RB;
     static constexpr int F0 = Q + 8 * RB, F1 = F0 + (GRAD ? 8 : 0) * RB;
     static constexpr int T = F1 + (GRAD ? 8 : 0) * RB, BX = T + 4 * RB;
@@ -507,8 +508,11 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD, UNR> &Q, MarchCtx &X, fl
 #ifndef MARCH_FWD_MIN_BLOCKS
 #define MARCH_FWD_MIN_BLOCKS 3
 #endif
+#ifndef MARCH_GRAD_MIN_BLOCKS
+#define MARCH_GRAD_MIN_BLOCKS 2
+#endif
 template <bool VTI, bool GRAD, int NTH>
-__global__ void __launch_bounds__(NTH, (GRAD || NTH > 224) ? 2 : MARCH_FWD_MIN_BLOCKS)
+__global__ void __launch_bounds__(NTH, NTH > 224 ? 2 : (GRAD ? MARCH_GRAD_MIN_BLOCKS : MARCH_FWD_MIN_BLOCKS))
 elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ units, ModelDev M, StepConst C, int it,
               int flags, float dtg)
 {
