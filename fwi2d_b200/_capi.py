@@ -18,8 +18,12 @@ SYMBOLS = [
     "fwi2d_last_error", "fwi2d_version", "fwi2d_injector_weights", "fwi2d_ctx_create", "fwi2d_ctx_destroy",
     "fwi2d_set_model", "fwi2d_set_shots", "fwi2d_forward", "fwi2d_adjoint", "fwi2d_upload_traces", "fwi2d_run",
     "fwi2d_sync", "fwi2d_snapshot", "fwi2d_plan_info", "fwi2d_tile_shape_count", "fwi2d_tile_shape",
-    "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing", "fwi2d_set_stream", "fwi2d_copy_gradient", "fwi2d_propagate_noalloc", "fwi2d_noalloc_last_error",
+    "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing",
+    "fwi2d_set_stream", "fwi2d_copy_gradient", "fwi2d_set_data_axis", "fwi2d_resample", "fwi2d_propagate_noalloc",
+    "fwi2d_noalloc_last_error",
 ]
+
+RESAMPLE_SINC, RESAMPLE_LINEAR = 0, 1
 
 
 class Params(ctypes.Structure):
@@ -97,6 +101,8 @@ def load(build_if_missing=False):
     L.fwi2d_last_timing.argtypes = [vp, vp, vp]
     L.fwi2d_set_stream.argtypes = [vp, vp]
     L.fwi2d_copy_gradient.argtypes = [vp, vp]
+    L.fwi2d_set_data_axis.argtypes = [vp, f, i, i, vp]
+    L.fwi2d_resample.argtypes = [i, i, i, i, i, f, i, f, vp, vp]
     _lib = L
     return L
 

@@ -19,6 +19,7 @@
 #include "engine.h"
 #include "host_tables.h"
 #include "launch.h"
+#include "resample.cuh"
 #include "../../include/fwi2d_b200.h"
 
 namespace fwi2d {
@@ -272,6 +273,13 @@ struct Plan {
     DevBuf d_icells[2], d_ioff[2], d_iidx[2];
     // FWI gradient: observed data, misfit partial sums
     DevBuf d_obs, d_misfit, d_part;
+    // data time axis of fwi2d_fwi_gradient (fwi2d_set_data_axis): dd > 0 when
+    // sources and data are sampled at dd and resampled to dt; nd per shot;
+    // d_rs0 / d_rs1 hold one shot's trace block in the trace pipeline
+    float dd = 0.f;
+    int rs_linear = 0, rs_hl = 11;
+    std::vector<int> nd;
+    DevBuf d_rs0, d_rs1;
     DevBuf d_grad_full, d_stage;
     StepConst C;
     float dtg = 0;
@@ -1608,6 +1616,40 @@ static void upload_traces(fwi2d_ctx *ctx, const float *traces, bool adjoint)
     CK(cudaStreamSynchronize(ctx->st));   // the caller's traces may be reused on return
 }
 
+// Sources on the data axis (fwi2d_set_data_axis): concatenated per-shot
+// blocks [rows][nd], resampled to the propagation axis as apply_forward does
+// (we_op.cpp:953-957: sinc or linear interpolation, no scaling).
+static void upload_sources_axis(fwi2d_ctx *ctx, const float *traces)
+{
+    Plan &P = need_plan(ctx);
+    REQ(traces != nullptr, "null trace array");
+    set_device(ctx);
+    size_t maxd = 1, maxp = 1;
+    for (size_t k = 0; k < P.shots.size(); k++) {
+        maxd = std::max(maxd, (size_t)P.shots[k]->nsrc_rows * P.nd[k]);
+        maxp = std::max(maxp, (size_t)P.shots[k]->nsrc_rows * P.shots[k]->nt);
+    }
+    if (P.d_stage.n < maxd * sizeof(float)) P.d_stage.alloc(maxd * sizeof(float));
+    if (P.d_rs1.n < maxp * sizeof(float)) P.d_rs1.alloc(maxp * sizeof(float));
+    const float *p = traces;
+    for (size_t k = 0; k < P.shots.size(); k++) {
+        ShotPlan &S = *P.shots[k];
+        const int rows = S.nsrc_rows, nd = P.nd[k];
+        const size_t n = (size_t)rows * nd;
+        for (size_t i = 0; i < n; i++)
+            if (!std::isfinite(p[i])) throw Error(FWI2D_ERR_ARG, "trace array holds a non-finite value");
+        if (rows > 0) {
+            CK(cudaMemcpyAsync(P.d_stage.p, p, n * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+            k_resample_fwd<<<dim3((S.nt + 127) / 128, rows), 128, 0, ctx->st>>>(
+                P.d_stage.as<float>(), P.d_rs1.as<float>(), nd, P.dd, S.nt, P.par.dt, P.rs_hl, P.rs_linear);
+            launch_to_time_major(P.d_rs1.as<float>(), S.src_f.as<float>(), rows, S.nt, ctx->st);
+            CK(cudaGetLastError());
+        }
+        p += n;
+    }
+    CK(cudaStreamSynchronize(ctx->st));   // the caller's traces may be reused on return
+}
+
 static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
 {
     Plan &P = need_plan(ctx);
@@ -1827,17 +1869,54 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
     // each shot reduces its partials before the next shot writes them
     P.d_part.ensure(part_max * sizeof(float2));
     size_t obs_off = 0, row_off = 0;
-    for (auto &S : P.shots) {
-        const int nchunk = (S->nt + kResChunk - 1) / kResChunk;
-        dim3 grid((S->nrcv_rows + 127) / 128, nchunk);
-        k_residual<<<grid, 128, 0, ctx->st>>>(S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off,
-                                              S->src_a.as<float>(), nullptr, P.d_part.as<float2>(), S->nt,
-                                              S->nrcv_rows, P.par.dt, seismotype, P.ae ? S->nr : 0);
-        k_misfit_rows<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
-            P.d_part.as<float2>(), P.d_misfit.as<double>() + row_off, S->nrcv_rows, nchunk);
-        CK(cudaGetLastError());
-        obs_off += (size_t)S->nt * S->nrcv_rows;
-        row_off += S->nrcv_rows;
+    if (P.dd > 0.f) {
+        // data on their own axis: receivers -> alpha Dt -> adjoint resampling to
+        // the data axis; residual, misfit, Ht weighting there; resampling back,
+        // Ht^-1, reversal, -alpha, Dt^T (we_op.cpp:1030-1054, 1100-1124)
+        const float alpha = P.par.dt / P.dd;
+        size_t mx = 1, pm = 1;
+        for (size_t k = 0; k < P.shots.size(); k++) {
+            mx = std::max(mx, (size_t)P.shots[k]->nrcv_rows * std::max(P.shots[k]->nt, P.nd[k]));
+            pm = std::max(pm, (size_t)((P.nd[k] + kRsChunk - 1) / kRsChunk) * P.shots[k]->nrcv_rows);
+        }
+        P.d_rs0.ensure(std::max(P.d_rs0.n, mx * sizeof(float)));
+        P.d_rs1.ensure(std::max(P.d_rs1.n, mx * sizeof(float)));
+        P.d_part.ensure(std::max(P.d_part.n, pm * sizeof(float2)));
+        for (size_t k = 0; k < P.shots.size(); k++) {
+            ShotPlan &S = *P.shots[k];
+            const int rows = S.nrcv_rows, nt = S.nt, nd = P.nd[k];
+            const int neg = P.ae ? S.nr : 0;
+            const int nchunk = (nd + kRsChunk - 1) / kRsChunk;
+            float *r0 = P.d_rs0.as<float>(), *r1 = P.d_rs1.as<float>();
+            k_rcv_to_rate<<<dim3((rows + 127) / 128, nt), 128, 0, ctx->st>>>(S.rcv_f.as<float>(), r0, rows, nt,
+                                                                            P.par.dt, alpha, seismotype, neg);
+            k_resample_adj<<<dim3((nd + 127) / 128, rows), 128, 0, ctx->st>>>(r0, r1, nd, P.dd, nt, P.par.dt,
+                                                                             P.rs_hl, P.rs_linear);
+            k_residual_axis<<<dim3((rows + 127) / 128, nchunk), 128, 0, ctx->st>>>(
+                r1, P.d_obs.as<float>() + obs_off, r0, P.d_part.as<float2>(), rows, nd, P.dd);
+            k_misfit_rows<<<(rows + 127) / 128, 128, 0, ctx->st>>>(P.d_part.as<float2>(),
+                                                                  P.d_misfit.as<double>() + row_off, rows, nchunk);
+            k_resample_fwd<<<dim3((nt + 127) / 128, rows), 128, 0, ctx->st>>>(r0, r1, nd, P.dd, nt, P.par.dt,
+                                                                             P.rs_hl, P.rs_linear);
+            k_adjoint_source_axis<<<dim3((rows + 127) / 128, nt), 128, 0, ctx->st>>>(
+                r1, S.src_a.as<float>(), rows, nt, P.par.dt, alpha, seismotype, neg);
+            CK(cudaGetLastError());
+            obs_off += (size_t)nd * rows;
+            row_off += rows;
+        }
+    } else {
+        for (auto &S : P.shots) {
+            const int nchunk = (S->nt + kResChunk - 1) / kResChunk;
+            dim3 grid((S->nrcv_rows + 127) / 128, nchunk);
+            k_residual<<<grid, 128, 0, ctx->st>>>(S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off,
+                                                  S->src_a.as<float>(), nullptr, P.d_part.as<float2>(), S->nt,
+                                                  S->nrcv_rows, P.par.dt, seismotype, P.ae ? S->nr : 0);
+            k_misfit_rows<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
+                P.d_part.as<float2>(), P.d_misfit.as<double>() + row_off, S->nrcv_rows, nchunk);
+            CK(cudaGetLastError());
+            obs_off += (size_t)S->nt * S->nrcv_rows;
+            row_off += S->nrcv_rows;
+        }
     }
     run(ctx, true, false);
     if (chain) {
@@ -1856,11 +1935,18 @@ static void set_observed(fwi2d_ctx *ctx, const float *obs)
     REQ(obs != nullptr, "null observed data");
     set_device(ctx);
     size_t total = 0, maxn = 0;
-    for (auto &S : P.shots) {
-        total += (size_t)S->nt * S->nrcv_rows;
-        maxn = std::max(maxn, (size_t)S->nt * S->nrcv_rows);
+    for (size_t k = 0; k < P.shots.size(); k++) {
+        const size_t n = (size_t)(P.dd > 0.f ? P.nd[k] : P.shots[k]->nt) * P.shots[k]->nrcv_rows;
+        total += n;
+        maxn = std::max(maxn, n);
     }
-    P.d_obs.ensure(total * sizeof(float));
+    P.d_obs.ensure(std::max<size_t>(total, 1) * sizeof(float));
+    if (P.dd > 0.f) {
+        // data-axis observed data stay row-major [rows][nd] per shot
+        CK(cudaMemcpyAsync(P.d_obs.p, obs, total * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        return;
+    }
     if (P.d_stage.n < maxn * sizeof(float)) P.d_stage.alloc(maxn * sizeof(float));
     size_t off = 0;
     for (auto &S : P.shots) {
@@ -1873,6 +1959,40 @@ static void set_observed(fwi2d_ctx *ctx, const float *obs)
     CK(cudaStreamSynchronize(ctx->st));
 }
 
+// Data time axis of the FWI gradient (the time axis of the reference's
+// source and data cubes, analyzeModel, we_op.cpp:436-472): nd[k] samples at
+// dd for shot k, resampled to the plan's dt <= dd with the sinc (half length
+// hl) or linear resampler.  Each shot's nt must be the propagation length the
+// reference derives, round((nd - 1) dd / dt) + 1.  dd <= 0 returns to data on
+// the propagation axis.  The resident observed data are dropped.
+static void set_data_axis(fwi2d_ctx *ctx, float dd, int method, int hl, const int *nd)
+{
+    Plan &P = need_plan(ctx);
+    P.d_obs.release();
+    if (dd <= 0.f) {
+        P.dd = 0.f;
+        P.nd.clear();
+        return;
+    }
+    REQ(method == FWI2D_RESAMPLE_SINC || method == FWI2D_RESAMPLE_LINEAR, "unknown resampling method");
+    REQ(method == FWI2D_RESAMPLE_LINEAR || hl > 0, "the sinc half length must be positive");
+    REQ(nd != nullptr, "null data sample counts");
+    REQ(P.par.dt <= dd, "the propagation step must not exceed the data step");
+    std::vector<int> v(nd, nd + P.shots.size());
+    for (size_t k = 0; k < P.shots.size(); k++) {
+        REQ(v[k] >= 2, "a shot needs at least two data samples");
+        const float tmax = (v[k] - 1) * dd;
+        const int nt = (int)std::round(tmax / P.par.dt) + 1;
+        if (nt != P.shots[k]->nt)
+            throw Error(FWI2D_ERR_ARG, "shot " + std::to_string(k) + ": nt must be round((nd - 1) dd / dt) + 1 = " +
+                                           std::to_string(nt));
+    }
+    P.dd = dd;
+    P.rs_linear = method == FWI2D_RESAMPLE_LINEAR;
+    P.rs_hl = hl;
+    P.nd = v;
+}
+
 static double read_misfit(fwi2d_ctx *ctx)
 {
     Plan &P = need_plan(ctx);
@@ -1883,7 +2003,7 @@ static double read_misfit(fwi2d_ctx *ctx)
     CK(cudaStreamSynchronize(ctx->st));
     double f = 0.0;
     for (double v : m) f += v;
-    return 0.5 * (double)P.par.dt * f;
+    return 0.5 * (double)(P.dd > 0.f ? P.dd : P.par.dt) * f;
 }
 
 // Host snapshots [nslot][ncomp][nx][nz] (fp32) -> the device store of shot 0.
@@ -2217,6 +2337,40 @@ int fwi2d_update_model(fwi2d_ctx *ctx, const float *model)
     ABI_END
 }
 
+int fwi2d_set_data_axis(fwi2d_ctx *ctx, float dt_data, int method, int sinc_half_length, const int *nd)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    set_device(ctx);
+    set_data_axis(ctx, dt_data, method, sinc_half_length, nd);
+    ABI_END
+}
+
+int fwi2d_resample(int method, int adjoint, int sinc_half_length, int ntr, int nm, float dm, int np, float dp,
+                   const float *in, float *out)
+{
+    ABI_TRY
+    REQ(in && out, "null argument");
+    REQ(method == FWI2D_RESAMPLE_SINC || method == FWI2D_RESAMPLE_LINEAR, "unknown resampling method");
+    REQ(method == FWI2D_RESAMPLE_LINEAR || sinc_half_length > 0, "the sinc half length must be positive");
+    REQ(ntr >= 0 && ntr <= 65535 && nm > 0 && np > 0 && dm > 0.f && dp > 0.f, "bad resampling axes");
+    if (ntr == 0) return FWI2D_OK;
+    const size_t nin = (size_t)ntr * (adjoint ? np : nm), nout = (size_t)ntr * (adjoint ? nm : np);
+    DevBuf a, b;
+    a.alloc(nin * sizeof(float));
+    b.alloc(nout * sizeof(float));
+    CK(cudaMemcpy(a.p, in, nin * sizeof(float), cudaMemcpyHostToDevice));
+    if (!adjoint)
+        k_resample_fwd<<<dim3((np + 127) / 128, ntr), 128>>>(a.as<float>(), b.as<float>(), nm, dm, np, dp,
+                                                             sinc_half_length, method == FWI2D_RESAMPLE_LINEAR);
+    else
+        k_resample_adj<<<dim3((nm + 127) / 128, ntr), 128>>>(a.as<float>(), b.as<float>(), nm, dm, np, dp,
+                                                             sinc_half_length, method == FWI2D_RESAMPLE_LINEAR);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(out, b.p, nout * sizeof(float), cudaMemcpyDeviceToHost));
+    ABI_END
+}
+
 int fwi2d_set_observed(fwi2d_ctx *ctx, const float *obs)
 {
     ABI_TRY
@@ -2232,7 +2386,10 @@ int fwi2d_fwi_gradient(fwi2d_ctx *ctx, const float *model, const float *src, con
     REQ(ctx, "null context");
     REQ(seismotype == 0 || seismotype == 1, "seismotype must be 0 or 1");
     if (model) update_model(ctx, model);
-    if (src) upload_traces(ctx, src, false);
+    if (src) {
+        if (need_plan(ctx).dd > 0.f) upload_sources_axis(ctx, src);
+        else upload_traces(ctx, src, false);
+    }
     if (obs) set_observed(ctx, obs);
     fwi_gradient(ctx, seismotype, true);
     if (grad) download_grad(ctx, grad);

@@ -1,11 +1,11 @@
 // fwi2d_propagate_noalloc: the elastic forward propagation of one shot with
 // no device or host memory allocation.
 //
-// Some callers cannot allocate device memory: code that runs while a CUDA
-// graph is being captured or inside a driver callback, plug-ins loaded into a
-// host process that owns the device allocator (a framework's caching pool that
-// must see every byte), or real-time loops that forbid allocation after start
-// up.  For them this entry point keeps every device-side buffer of the
+// Some callers cannot allocate device memory: plug-ins loaded into a host
+// process that owns the device allocator (a framework's caching pool that must
+// account for every byte on the device), and real-time loops that forbid
+// allocation after start-up (cudaMalloc and cudaFree can synchronise the
+// device and take unbounded time).  For them this entry point keeps every device-side buffer of the
 // propagation -- the pitched model, the two wavefield buffers, the time-major
 // traces and the injection / extraction / boundary tables -- in one
 // file-scope static __device__ array of FWI2D_NOALLOC_SCRATCH_BYTES (64 MiB),

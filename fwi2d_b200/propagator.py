@@ -6,6 +6,7 @@ traces are ``[ncomp][ntr][nt]`` per shot, gradients are the raw imaging
 condition before the H quadrature and the chain rule.
 """
 import ctypes
+import math
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -57,6 +58,31 @@ def _injector(itype, tabs):
     return C.Injector(itype, len(xind), C.ptr(xind), C.ptr(zind), C.ptr(xw), C.ptr(zw))
 
 
+def prop_nt(nd, dt_data, dt):
+    """Propagation length the reference derives for nd data samples at
+    dt_data (analyzeModel, src/cpp/we_op.cpp:436-464): tmax = (nd - 1) dt_data in
+    single precision, nt = round(tmax / dt) + 1 with dt = min(dt, dt_data)."""
+    f = np.float32
+    dt = min(f(dt), f(dt_data))
+    tmax = f(nd - 1) * f(dt_data)
+    return int(math.floor(float(f(tmax / dt)) + 0.5)) + 1   # C round(): halves away from zero
+
+
+def resample(x, nm, dm, np_, dp, adjoint=False, method="sinc", sinc_half_length=11):
+    """The reference's time resampler on the device (sinc_resampler /
+    linear_resampler, src/cpp/operator.cpp:760-856): domain axis nm samples at
+    dm, range axis np_ samples at dp.  adjoint False: x [ntr][nm] ->
+    [ntr][np_]; True: x [ntr][np_] -> [ntr][nm]."""
+    L = C.load()
+    x = np.ascontiguousarray(x, np.float32)
+    ntr = x.shape[0]
+    out = np.zeros((ntr, nm if adjoint else np_), np.float32)
+    m = C.RESAMPLE_LINEAR if method == "linear" else C.RESAMPLE_SINC
+    C.check(L.fwi2d_resample(m, 1 if adjoint else 0, int(sinc_half_length), ntr, int(nm), float(dm), int(np_),
+                             float(dp), C.ptr(x), C.ptr(out)))
+    return out
+
+
 @dataclass
 class ShotSpec:
     """One shot: its grid is model columns [x0, x0+nx); locations in km
@@ -90,6 +116,7 @@ class Propagator:
         C.check(self.L.fwi2d_ctx_create(int(device), ctypes.byref(h)))
         self.h = h
         self.kind = None
+        self.nd = None   # per-shot data samples after set_data_axis
         self._keep = []
 
     def close(self):
@@ -112,6 +139,7 @@ class Propagator:
     def set_shots(self, params, shots: List[ShotSpec]):
         self.params = params
         self.shots = shots
+        self.nd = None   # a new plan propagates data on its own axis
         arr = (C.Shot * len(shots))()
         keep = []
         self.src_rows, self.rcv_rows = [], []
@@ -156,12 +184,28 @@ class Propagator:
         return 2 if self.kind == C.ACOUSTIC else 3
 
     # -- host API ---------------------------------------------------------
-    def _concat(self, blocks, rows):
+    def _concat(self, blocks, rows, lengths=None):
         parts = []
-        for b, r, s in zip(blocks, rows, self.shots):
-            b = np.asarray(b, np.float32).reshape(r, s.nt)
+        lengths = lengths or [s.nt for s in self.shots]
+        for b, r, n in zip(blocks, rows, lengths):
+            b = np.asarray(b, np.float32).reshape(r, n)
             parts.append(b.ravel())
         return np.ascontiguousarray(np.concatenate(parts))
+
+    def set_data_axis(self, dt_data, nd, resampling="sinc", sinc_half_length=11):
+        """Sources and observed data of fwi_gradient on their own time axis:
+        nd[s] samples at dt_data for shot s, resampled to the propagation step
+        with the reference's "sinc" or "linear" resampler (param.resampling,
+        param.sinc_half_length).  Each shot's nt must be
+        prop_nt(nd[s], dt_data, params.dt).  dt_data <= 0 clears it."""
+        if dt_data <= 0:
+            self.nd = None
+            C.check(self.L.fwi2d_set_data_axis(self.h, 0.0, 0, 0, None))
+            return
+        nd = np.ascontiguousarray(nd, np.int32)
+        method = C.RESAMPLE_LINEAR if resampling == "linear" else C.RESAMPLE_SINC
+        C.check(self.L.fwi2d_set_data_axis(self.h, float(dt_data), method, int(sinc_half_length), C.ptr(nd)))
+        self.nd = [int(v) for v in nd]
 
     def forward(self, src_blocks, store=True):
         """src_blocks[s]: [ncomp][ntr][nt] traces of shot s.  Returns the
@@ -196,7 +240,7 @@ class Propagator:
         C.check(self.L.fwi2d_update_model(self.h, C.ptr(m)))
 
     def set_observed(self, obs_blocks):
-        buf = self._concat(obs_blocks, self.rcv_rows)
+        buf = self._concat(obs_blocks, self.rcv_rows, self.nd)
         C.check(self.L.fwi2d_set_observed(self.h, C.ptr(buf)))
 
     def fwi_gradient(self, model=None, src_blocks=None, obs_blocks=None, seismotype=1, download=True):
@@ -204,8 +248,8 @@ class Propagator:
         for the acoustic propagator -- and the misfit), or (None, None) with
         download=False."""
         m = None if model is None else np.ascontiguousarray(model, np.float32)
-        src = None if src_blocks is None else self._concat(src_blocks, self.src_rows)
-        obs = None if obs_blocks is None else self._concat(obs_blocks, self.rcv_rows)
+        src = None if src_blocks is None else self._concat(src_blocks, self.src_rows, self.nd)
+        obs = None if obs_blocks is None else self._concat(obs_blocks, self.rcv_rows, self.nd)
         g = np.zeros((self.ngrad(), self.nx, self.nz), np.float32) if download else None
         f = ctypes.c_double(0.0)
         C.check(self.L.fwi2d_fwi_gradient(self.h, C.ptr(m), C.ptr(src), C.ptr(obs), int(seismotype), C.ptr(g),

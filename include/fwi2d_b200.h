@@ -129,9 +129,37 @@ int fwi2d_sync(fwi2d_ctx *ctx);
  * the batch plan, its tables and graphs stay valid. */
 int fwi2d_update_model(fwi2d_ctx *ctx, const float *model);
 
-/* Observed data of every shot, concatenated per-shot blocks [ncomp][nr][nt],
- * kept on the device for fwi2d_fwi_gradient. */
+/* Observed data of every shot, concatenated per-shot blocks [ncomp][nr][nt]
+ * ([ncomp][nr][nd] after fwi2d_set_data_axis), kept on the device for
+ * fwi2d_fwi_gradient. */
 int fwi2d_set_observed(fwi2d_ctx *ctx, const float *obs);
+
+/* time resamplers (src/cpp/operator.cpp:734-856; param.resampling) */
+#define FWI2D_RESAMPLE_SINC 0     /* sinc_resampler: cosine-windowed sinc, param.sinc_half_length */
+#define FWI2D_RESAMPLE_LINEAR 1   /* linear_resampler */
+
+/* Sources and data of fwi2d_fwi_gradient on their own time axis, as the
+ * reference's operators take them (the time axis of the source and data cubes;
+ * nl_we_op_e::apply_forward / apply_jacobianT, we_op.cpp:930-1054, 1086-1124):
+ * shot k has nd[k] samples at dt_data, and the plan propagates at its
+ * params.dt <= dt_data with nt = round((nd[k] - 1) dt_data / dt) + 1 (analyzeModel,
+ * we_op.cpp:446-464; other nt are rejected).  fwi2d_fwi_gradient then takes src
+ * as per-shot blocks [rows][nd] and obs as [ncomp][nr][nd], resamples the
+ * sources to dt, the synthetics (alpha Dt of the receivers, alpha = dt /
+ * dt_data) back to dt_data, forms the residual, the misfit 1/2 dt_data (...)
+ * and the applyHt weighting on the data axis, and the adjoint sources through
+ * the forward resampler, applyHt^-1, reversal, -alpha and Dt^T.  Call after
+ * fwi2d_set_shots (a new plan clears it); dt_data <= 0 clears it.  The
+ * resident observed data are dropped. */
+int fwi2d_set_data_axis(fwi2d_ctx *ctx, float dt_data, int method, int sinc_half_length, const int *nd);
+
+/* The reference's resampler on ntr host traces (sinc_resampler /
+ * linear_resampler::apply_forward and apply_adjoint with add = false,
+ * operator.cpp:760-856), computed on the current device.  Domain axis: nm
+ * samples at dm; range axis: np samples at dp; both from t = 0.  adjoint = 0:
+ * in [ntr][nm] -> out [ntr][np]; adjoint = 1: in [ntr][np] -> out [ntr][nm]. */
+int fwi2d_resample(int method, int adjoint, int sinc_half_length, int ntr, int nm, float dm, int np, float dp,
+                   const float *in, float *out);
 
 /* One FWI gradient evaluation on the device (nlls_fwi_eco::compute_res_and_grad,
  * optimization.hpp:590-951, with the data-side options off): forward with
@@ -188,9 +216,9 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
                     int nx, int nz, float dx, float dz);
 
 /* Allocation-free forward propagation.  No counterpart in the reference: it
- * serves callers that cannot allocate device memory (code running under CUDA
- * graph capture, plug-ins whose host framework owns the device allocator,
- * allocation-free real-time loops).  Same meaning and results as
+ * serves callers that cannot allocate device memory (plug-ins whose host
+ * framework owns the device allocator, real-time loops that forbid the
+ * device-synchronising cudaMalloc / cudaFree after start-up).  Same meaning and results as
  * fwi2d_propagate with adj = 0 and no snapshots, for the elastic isotropic
  * propagator with point-force sources: host inputs, receivers accumulated into
  * allrcv.  All device-side buffers live in one static array of

@@ -73,6 +73,26 @@ class _Lib:
     def arr(self, a):
         return np.ascontiguousarray(a, dtype=self.dtype)
 
+    _resample_symbol = None
+
+    def resample(self, method, adjoint, x, nm, dm, np_, dp, hl=11):
+        """The reference's time resampler (operator.cpp:755-856): method
+        "sinc" or "linear"; domain axis nm samples at dm, range axis np_ at dp.
+        adjoint False: x [ntr][nm] -> [ntr][np_] (interpolation); True:
+        x [ntr][np_] -> [ntr][nm] (its adjoint)."""
+        f = getattr(self.lib, self._resample_symbol)
+        f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                      ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+        x = self.arr(x)
+        ntr = x.shape[0]
+        assert x.shape == (ntr, np_ if adjoint else nm)
+        out = np.zeros((ntr, nm if adjoint else np_), self.dtype)
+        rc = f(1 if method == "linear" else 0, 1 if adjoint else 0, int(hl), ntr, int(nm), float(dm), int(np_),
+               float(dp), _ptr(x), _ptr(out))
+        if rc not in (None, 0):
+            raise RuntimeError("resampling failed")
+        return out
+
 
 def port_path(prec=32):
     return os.path.join(HERE, "liborc%d.so" % prec)
@@ -95,6 +115,7 @@ class Port(_Lib):
             raise FileNotFoundError(path + " (build with `make -C oracle`)")
         super().__init__(path, prec, "port")
         pre = "orc%d_" % prec
+        self._resample_symbol = pre + "resample"
         self._weights = getattr(self.lib, pre + "injector_weights")
         self._prop = getattr(self.lib, pre + "propagate")
         self._conv = getattr(self.lib, pre + "convert_model")
@@ -162,6 +183,7 @@ class Reference(_Lib):
         if not os.path.exists(path):
             raise FileNotFoundError(path + " (built by oracle/build_ref.sh where the reference is present)")
         super().__init__(path, prec, "reference")
+        self._resample_symbol = "ref_resample"
         self._weights = self.lib.ref_injector_weights
         self._weights.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -213,6 +235,31 @@ class Reference(_Lib):
                _ptr(s), _ptr(o), _ptr(syn), _ptr(g))
         if rc != 0:
             raise RuntimeError("reference misfit/gradient failed")
+        return syn, g
+
+    def misfit_grad_rs(self, kind, par, nx, nz, d, nd, dd, prop_dt, method, hl, src_loc, rcv_locs, model_raw, src,
+                       obs=None):
+        """misfit_grad with sources and data on their own axis (nd samples at
+        dd) and the propagation at prop_dt, through the reference's "sinc" or
+        "linear" resampler (ref_misfit_grad_rs).  Returns (syn [ncomp][nr][nd],
+        grad or None)."""
+        f = self.lib.ref_misfit_grad_rs
+        vp = ctypes.c_void_p
+        f.argtypes = [ctypes.c_int, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                      ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                      self._real(), self._real(), ctypes.c_int, vp, vp, vp, vp, vp, vp, vp]
+        rx, rz = self.arr(rcv_locs[0]), self.arr(rcv_locs[1])
+        nr = len(rx)
+        m = self.arr(model_raw)
+        nc = 1 if kind == KIND_ACOUSTIC else 2
+        s = self.arr(src).reshape(nc, nd)
+        syn = np.zeros((nc, nr, nd), self.dtype)
+        o = None if obs is None else self.arr(obs)
+        g = None if obs is None else np.zeros(m.shape, self.dtype)
+        rc = f(kind, ctypes.byref(par), nx, nz, d, d, nd, dd, prop_dt, 1 if method == "linear" else 0, int(hl),
+               src_loc[0], src_loc[1], nr, _ptr(rx), _ptr(rz), _ptr(m), _ptr(s), _ptr(o), _ptr(syn), _ptr(g))
+        if rc != 0:
+            raise RuntimeError("reference misfit/gradient with resampling failed")
         return syn, g
 
     def misfit_grad_ae(self, par, nx, nz, d, oz, nt, dt, src_loc, rcv_x, rcv_z, rcv_zw, model_raw, src, obs=None):

@@ -1343,3 +1343,66 @@ void ORC(convert_model)(int kind, void *m_, int n, int forward)
 }
 
 int ORC(real_size)(void) { return (int)sizeof(real); }
+
+/* ---------------------------------------------------------------------------
+ * Time resampling (src/cpp/operator.cpp:755-856): the windowed-sinc and the
+ * linear resampler between a domain time axis (nm samples at dm) and a range
+ * axis (np samples at dp), both from t = 0, on ntr traces, add = false.
+ *   adjoint = 0: in [ntr][nm] -> out [ntr][np]   (apply_forward, interpolation)
+ *   adjoint = 1: in [ntr][np] -> out [ntr][nm]   (apply_adjoint, decimation)
+ * Same operation order and promotions: the sinc argument and the cosine
+ * window are formed in double from single-precision times (M_PI is a double),
+ * sinc(x) = sin(x)/x with x rounded to the sample type and sin evaluated in
+ * double (the reference's unqualified sin of a float resolves to ::sin(double)),
+ * and each product pmod*sinc (sample type) times the window (double) is added
+ * in double to the output sample.  The window is a + (1-a) cos(pi (itm - t/dm)
+ * / hl) with a = 1/2 (sinc_resampler's default alpha).
+ * ------------------------------------------------------------------------- */
+static real sinc_(real x)
+{
+    if (x == 0.0) return 1.0;
+    return (real)(sin((double)x) / (double)x);
+}
+
+int ORC(resample)(int linear, int adjoint, int hl, int ntr, int nm, double dm_, int np, double dp_,
+                   const void *in_, void *out_)
+{
+    const real *in = (const real *)in_;
+    real *out = (real *)out_;
+    const real dm = (real)dm_, dp = (real)dp_, a = (real)0.5;
+    if (adjoint) memset(out, 0, (size_t)ntr * nm * sizeof(real));
+    OMP_FOR
+    for (int ix = 0; ix < ntr; ix++) {
+        const real *pm = adjoint ? NULL : in + (size_t)ix * nm;
+        const real *pd = adjoint ? in + (size_t)ix * np : NULL;
+        real *om = adjoint ? out + (size_t)ix * nm : NULL;
+        real *od = adjoint ? NULL : out + (size_t)ix * np;
+        for (int itd = 0; itd < np; itd++) {
+            if (linear) {
+                const real x = itd * dp / dm;
+                int i = (int)floor(x), j = (int)ceil(x);
+                if (i > nm - 1) i = nm - 1;
+                if (j > nm - 1) j = nm - 1;
+                const real wj = (itd * dp - i * dm) / dm, wi = 1 - wj;
+                if (!adjoint) od[itd] = wi * pm[i] + wj * pm[j];
+                else {
+                    om[i] += wi * pd[itd];
+                    om[j] += wj * pd[itd];
+                }
+                continue;
+            }
+            const real t = itd * dp;
+            const int itm0 = (int)floor(t / dm);
+            const int lo = itm0 - hl + 1 > 0 ? itm0 - hl + 1 : 0;
+            const int hi = itm0 + hl < nm - 1 ? itm0 + hl : nm - 1;
+            if (!adjoint) od[itd] = 0;
+            for (int itm = lo; itm <= hi; itm++) {
+                const real s = sinc_((real)(M_PI * (t - itm * dm) / dm));
+                const double w = a + (1 - a) * cos(M_PI * (itm - t / dm) / hl);
+                if (!adjoint) od[itd] = (real)(od[itd] + (double)(pm[itm] * s) * w);
+                else om[itm] = (real)(om[itm] + (double)(pd[itd] * s) * w);
+            }
+        }
+    }
+    return 0;
+}

@@ -94,21 +94,23 @@ int ref_injector_weights(int type, int ntr, const data_t *lx, const data_t *lz, 
 // the solver forms (optimization.hpp:760-890): residual r = f(m) - obs
 // weighted by applyHt, then apply_jacobianT (we_op.cpp:1057-1239).  src is
 // [2][nt] (x, z force), syn and obs [2][nr][nt], grad [npar][nx][nz].
-int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, double dz, int nt, double dt,
-                    data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *model,
-                    const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
+static int misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, double dz, int nt, double dt,
+                       double prop_dt, const char *resampling, int hl,
+                       data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *model,
+                       const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
 {
     try {
         param par = to_param(rp);
         par.nt = nt;
-        par.dt = (data_t)dt;
+        par.dt = (data_t)prop_dt;
         par.sub = obs ? 1 : 0;
         par.ns = 1;
         par.nr = nr;
         par.nmodels = kind == 1 ? 5 : (kind == 2 ? 2 : 3);
         const int nc = kind == 2 ? 1 : 2;   // trace components (sources and receivers)
         par.seismotype = 1;
-        par.resampling = "linear";
+        par.resampling = resampling;
+        par.sinc_half_length = hl;
         data_t sl[2] = {sx, sz};
         par.sxz = locs(1, sl, sl + 1);
         par.rxz = {locs(nr, rx, rz)};
@@ -137,6 +139,53 @@ int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, do
         }
     } catch (const std::exception &e) {
         std::fprintf(stderr, "ref_misfit_grad: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+int ref_misfit_grad(int kind, const ref_param *rp, int nx, int nz, double dx, double dz, int nt, double dt,
+                    data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *model,
+                    const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
+{
+    return misfit_grad(kind, rp, nx, nz, dx, dz, nt, dt, dt, "linear", 11, sx, sz, nr, rx, rz, model, src, obs, syn,
+                       grad);
+}
+
+// As ref_misfit_grad with sources and data on their own time axis (nd samples
+// at dd) and the propagation at prop_dt: apply_forward / apply_jacobianT
+// resample with the reference's sinc (linear = 0, half length hl) or linear
+// resampler (we_op.cpp:930-955, 1086-1103); analyzeModel sets the propagation
+// nt = round((nd-1) dd / dt) + 1 with dt = min(prop_dt, dd) (we_op.cpp:446-464).
+// syn and obs are [nc][nr][nd]; the residual weighting applyHt uses dd, as
+// compute_res_and_grad does (optimization.hpp:606-607, 780).
+int ref_misfit_grad_rs(int kind, const ref_param *rp, int nx, int nz, double dx, double dz, int nd, double dd,
+                       double prop_dt, int linear, int hl, data_t sx, data_t sz, int nr, const data_t *rx,
+                       const data_t *rz, const data_t *model, const data_t *src, const data_t *obs, data_t *syn,
+                       data_t *grad)
+{
+    return misfit_grad(kind, rp, nx, nz, dx, dz, nd, dd, prop_dt, linear ? "linear" : "sinc", hl, sx, sz, nr, rx, rz,
+                       model, src, obs, syn, grad);
+}
+
+// The reference's time resamplers (operator.cpp:760-856) on ntr traces:
+// domain axis (nm samples at dm), range axis (np samples at dp), both from
+// t = 0.  adjoint = 0: in [ntr][nm] -> out [ntr][np] (apply_forward);
+// adjoint = 1: in [ntr][np] -> out [ntr][nm] (apply_adjoint).  add = false.
+int ref_resample(int linear, int adjoint, int hl, int ntr, int nm, double dm, int np_, double dp, const data_t *in,
+                 data_t *out)
+{
+    try {
+        hypercube<data_t> dom(axis<data_t>(nm, 0, (data_t)dm), axis<data_t>(ntr, 0, 1));
+        hypercube<data_t> rng(axis<data_t>(np_, 0, (data_t)dp), axis<data_t>(ntr, 0, 1));
+        resampler *r;
+        if (linear) r = new linear_resampler(dom, rng);
+        else r = new sinc_resampler(dom, rng, hl);
+        if (!adjoint) r->apply_forward(false, in, out);
+        else r->apply_adjoint(false, out, in);
+        delete r;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_resample: %s\n", e.what());
         return -1;
     }
     return 0;

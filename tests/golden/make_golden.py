@@ -137,6 +137,58 @@ def fwi_case(kind):
                 dot_sum2=sum2, grad_dot=gd)
 
 
+def resample_case():
+    """The reference's sinc and linear resamplers (operator.cpp:760-856),
+    forward and adjoint, on seeded traces over several axis pairs."""
+    lib = O.Reference(32)
+    rng = np.random.default_rng(11)
+    out = {}
+    axes = [(101, 4e-3, 401, 1e-3), (120, 2e-3, 301, 8e-4), (64, 2.5e-3, 170, 9.5e-4), (50, 1e-3, 50, 1e-3),
+            (33, 3e-3, 211, 4.7e-4)]
+    out["axes"] = np.array([[a[0], a[1], a[2], a[3]] for a in axes], np.float64)
+    for k, (nm, dm, np_, dp) in enumerate(axes):
+        x = rng.standard_normal((5, nm)).astype(np.float32)
+        y = rng.standard_normal((5, np_)).astype(np.float32)
+        out["x%d" % k], out["y%d" % k] = x, y
+        for method, hl in (("sinc", 11), ("linear", 11), ("sinc", 4)):
+            tag = "%s%d_%d" % (method, hl, k)
+            out["fwd_" + tag] = lib.resample(method, False, x, nm, dm, np_, dp, hl)
+            out["adj_" + tag] = lib.resample(method, True, y, nm, dm, np_, dp, hl)
+    return out
+
+
+def fwi_case_resampled():
+    """The elastic solver gradient with sources and data sampled at 2.5 ms and
+    the propagation at 1 ms: the reference's apply_forward / apply_jacobianT
+    resample (sinc, then linear) around the propagation (ref_misfit_grad_rs)."""
+    lib = O.Reference(32)
+    kind = O.KIND_ELASTIC
+    nx, nz, d, dt, dd, nd = 100, 80, 0.01, 1e-3, 2.5e-3, 161
+    true = K.model_case(kind, nx, nz, d, seed=7)
+    from scipy.ndimage import gaussian_filter
+    start = true.copy()
+    for c in range(3):
+        start[c] = gaussian_filter(true[c].astype(np.float64), 4, mode="nearest").astype(np.float32)
+    sx, sz = (0.5 * (nx - 1) + 0.3) * d, 0.02
+    rx = np.linspace(3 * d, (nx - 4) * d, 30).astype(np.float32)
+    rz = np.full(30, 0.02, np.float32)
+    src = K.sources(2, nd, dd).reshape(2, nd)
+    nt = 401
+    par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=30)
+    out = dict(kind=kind, nx=nx, nz=nz, d=d, nt=nt, dt=dt, dd=dd, nd=nd, sx=sx, sz=sz, rx=rx, rz=rz, true=true,
+               start=start, src=src)
+    w = np.full(nd, dd)
+    w[0] = w[-1] = 0.5 * dd
+    for method in ("sinc", "linear"):
+        geo = ((np.float32(sx), np.float32(sz)), (rx, rz))
+        obs, _ = lib.misfit_grad_rs(kind, par, nx, nz, d, nd, dd, dt, method, 11, geo[0], geo[1], true, src)
+        syn, g = lib.misfit_grad_rs(kind, par, nx, nz, d, nd, dd, dt, method, 11, geo[0], geo[1], start, src, obs)
+        r = syn.astype(np.float64) - obs
+        out["obs_" + method], out["syn_" + method], out["grad_" + method] = obs, syn, g
+        out["misfit_" + method] = 0.5 * np.sum(w * r * r)
+    return out
+
+
 def fwi_case_ae():
     """The acoustic-elastic solver gradient (nl_we_op_ae through the
     operator interface, residual weighted by applyHt), fluid source."""
@@ -178,6 +230,8 @@ def main():
     for kind, name in ((O.KIND_ELASTIC, "elastic"), (O.KIND_VTI, "vti"), (O.KIND_ACOUSTIC, "acoustic")):
         np.savez_compressed(os.path.join(HERE, "fwi_gradient_%s_f32.npz" % name), **fwi_case(kind))
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_f32.npz"), **fwi_case_ae())
+    np.savez_compressed(os.path.join(HERE, "resample_f32.npz"), **resample_case())
+    np.savez_compressed(os.path.join(HERE, "fwi_gradient_elastic_resampled_f32.npz"), **fwi_case_resampled())
     print("golden fixtures written to", HERE)
 
 

@@ -1,8 +1,9 @@
 """fwi2d_propagate_noalloc: the allocation-free forward entry point.
 
-It serves callers that cannot allocate device memory (code under CUDA graph
-capture, plug-ins whose host framework owns the device allocator, real-time
-loops); all its device buffers live in one static array inside the library.
+It serves callers that cannot allocate device memory (plug-ins whose host
+framework owns the device allocator, real-time loops that may not call the
+device-synchronising cudaMalloc / cudaFree); all its device buffers live in
+one static array inside the library.
 The check: two calls in a row through the C ABI each reproduce the regular
 fwi2d_propagate forward (same tolerance as the other parity tests; in
 practice bitwise), so the shared scratch leaves nothing behind from the
