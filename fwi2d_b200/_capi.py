@@ -20,7 +20,7 @@ SYMBOLS = [
     "fwi2d_sync", "fwi2d_snapshot", "fwi2d_plan_info", "fwi2d_tile_shape_count", "fwi2d_tile_shape",
     "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing",
     "fwi2d_set_stream", "fwi2d_copy_gradient", "fwi2d_set_data_axis", "fwi2d_resample", "fwi2d_propagate_noalloc",
-    "fwi2d_noalloc_last_error",
+    "fwi2d_noalloc_last_error", "fwi2d_analyze_model",
 ]
 
 RESAMPLE_SINC, RESAMPLE_LINEAR = 0, 1
@@ -40,6 +40,14 @@ class Params(ctypes.Structure):
         ("snapshot_precision", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("compensated", ctypes.c_int),
         ("tile_shape", ctypes.c_int),
     ]
+
+
+class ModelCheck(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in ("vpmin", "vpmax", "vsmin", "vsmax", "rhomin", "rhomax", "deltamin",
+                                               "deltamax", "epsilonmin", "epsilonmax")] + [
+        ("soft_clip", ctypes.c_int), ("acoustic_elastic", ctypes.c_int), ("water_velocity", ctypes.c_float),
+        ("courant", ctypes.c_float), ("dt", ctypes.c_float), ("sub", ctypes.c_int), ("nt", ctypes.c_int),
+        ("tmax", ctypes.c_float), ("vmax", ctypes.c_float), ("vmin", ctypes.c_float)]
 
 
 class Injector(ctypes.Structure):
@@ -103,6 +111,7 @@ def load(build_if_missing=False):
     L.fwi2d_copy_gradient.argtypes = [vp, vp]
     L.fwi2d_set_data_axis.argtypes = [vp, f, i, i, vp]
     L.fwi2d_resample.argtypes = [i, i, i, i, i, f, i, f, vp, vp]
+    L.fwi2d_analyze_model.argtypes = [i, vp, i, i, f, f, i, f, ctypes.POINTER(ModelCheck)]
     _lib = L
     return L
 

@@ -2103,6 +2103,17 @@ int fwi2d_injector_weights(int type, int ntr, const float *locx, const float *lo
     ABI_END
 }
 
+int fwi2d_analyze_model(int npar, float *model, int nx, int nz, float dx, float dz, int data_nt, float data_dt,
+                        fwi2d_model_check *check)
+{
+    ABI_TRY
+    REQ(npar == 2 || npar == 3 || npar == 5, "the model must hold 2 (vp, rho), 3 (vp, vs, rho) or 5 parameters");
+    REQ(model && check, "null argument");
+    REQ(nx > 0 && nz > 0 && dx > 0 && dz > 0 && data_nt > 0 && data_dt > 0, "invalid grid or data axis");
+    analyze_model(npar, model, nx, nz, dx, dz, data_nt, data_dt, *check);
+    ABI_END
+}
+
 int fwi2d_ctx_create(int device, fwi2d_ctx **out)
 {
     ABI_TRY

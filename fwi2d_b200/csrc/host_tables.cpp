@@ -1,4 +1,6 @@
 #include "host_tables.h"
+#include "../../include/fwi2d_b200.h"
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -287,6 +289,88 @@ void injector_weights(int type, int ntr, const float *locx, const float *locz, i
             ze[5] = (-1 - 2 * az) / (2 * dz);
         }
     }
+}
+
+
+// analyzeModel (src/cpp/we_op.cpp:267-474), single precision as the
+// reference's FP32 build: the delta admissibility bound and the Vs fix are
+// formed in double where the reference's literals are doubles (-0.5, 2.0,
+// 0.9999, sqrt(2), sqrt(2.0001)), and the VTI horizontal velocity
+// vp sqrt(1 + 2 eps) takes the double square root of the single-precision
+// 1 + 2 eps.  Clips are max(lo, min(hi, v)) (vecReg::clip).
+void analyze_model(int npar, float *m, int nx, int nz, float dx, float dz, int data_nt, float data_dt,
+                   fwi2d_model_check &c)
+{
+    const long n = (long)nx * nz;
+    auto lo = [&](int k) { return *std::min_element(m + k * n, m + (k + 1) * n); };
+    auto hi = [&](int k) { return *std::max_element(m + k * n, m + (k + 1) * n); };
+    auto clip = [&](int k, float a, float b) {
+        for (long i = k * n; i < (k + 1) * n; i++) m[i] = std::max(a, std::min(b, m[i]));
+    };
+    if (npar >= 3) {
+        float vpmax = hi(0), vsmin = lo(1);
+        if (npar == 5) {
+            // Thomsen delta inside -0.5 (1 - vs^2/vp^2) < delta < 2 / (vp^2/vs^2 - 1) (we_op.cpp:296-316)
+            const float *vp = m, *vs = m + n;
+            float *del = m + 3 * n;
+            for (long i = 0; i < n; i++) {
+                const float v1 = (float)(-0.5 * (1 - vs[i] * vs[i] / (vp[i] * vp[i])));
+                const float v2 = (float)(2.0 / (vp[i] * vp[i] / (vs[i] * vs[i]) - 1));
+                if (del[i] < v1) del[i] = (float)(0.9999 * v1);
+                else if (del[i] > v2) del[i] = (float)(0.9999 * v2);
+            }
+        }
+        if (!c.soft_clip) {
+            clip(0, c.vpmin, c.vpmax);
+            clip(1, c.vsmin, c.vsmax);
+            clip(2, c.rhomin, c.rhomax);
+            if (npar == 5) {
+                clip(3, c.deltamin, c.deltamax);
+                clip(4, c.epsilonmin, c.epsilonmax);
+            }
+            // Vs <= Vp / sqrt(2) (we_op.cpp:352-361)
+            for (long i = 0; i < n; i++)
+                if ((double)m[i] < std::sqrt(2.0) * (double)m[n + i]) m[n + i] = (float)((double)m[i] / std::sqrt(2.0001));
+            vpmax = hi(0);
+            vsmin = lo(1);
+        }
+        c.vmax = vpmax;
+        c.vmin = vsmin;
+        if (npar == 5) {
+            float h = 0.f;
+            for (long i = 0; i < n; i++) {
+                const float v = (float)((double)m[i] * std::sqrt((double)(1 + 2 * m[4 * n + i])));
+                h = i == 0 ? v : std::max(h, v);
+            }
+            c.vmax = std::max(h, c.vmax);
+        }
+        if (c.acoustic_elastic) {
+            c.vmax = std::max(c.vmax, c.water_velocity);
+            c.vmin = std::min(c.vmin, c.water_velocity);
+        }
+    } else {
+        clip(0, c.vpmin, c.vpmax);
+        clip(1, c.rhomin, c.rhomax);
+        c.vmax = hi(0);
+        c.vmin = lo(0);
+    }
+    // time axis (we_op.cpp:436-472)
+    const float tmax = (data_nt - 1) * data_dt;
+    const float h = std::min(dx, dz);
+    if (c.dt == 0.f) {
+        c.dt = c.courant * h / c.vmax;
+    } else if (c.dt > 0.f) {
+        c.dt = std::min(c.dt, data_dt);
+        c.courant = c.dt * c.vmax / h;
+    } else {
+        c.dt = c.courant * h / c.vmax;
+        if (data_dt > c.dt) c.dt = data_dt / std::ceil(data_dt / c.dt);
+        else c.dt = data_dt;
+        c.courant = c.dt * c.vmax / h;
+    }
+    c.nt = (int)std::round(tmax / c.dt) + 1;
+    c.tmax = (c.nt - 1) * c.dt;
+    if (c.sub < 0) c.sub = (int)std::round(data_dt / c.dt);
 }
 
 }  // namespace fwi2d

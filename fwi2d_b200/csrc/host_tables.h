@@ -5,6 +5,8 @@
 #include <vector>
 #include <cstdint>
 
+struct fwi2d_model_check;   // include/fwi2d_b200.h
+
 namespace fwi2d {
 
 // SBP constants as the reference's initialisers produce them (double rational
@@ -40,6 +42,10 @@ void acoustic_scale_divisors(int nx, int nz, float dx, float dz, float dt, const
 
 // delta_m3 / ddelta_m3::findIndicesWeights (injector.cpp:3-64, 114-187).
 // xw, zw: [ntr][2][3] (type 0) or [ntr][2][6] (type 1).
+// analyzeModel (we_op.cpp:267-474) on a raw model [npar][nx][nz], in place.
+void analyze_model(int npar, float *model, int nx, int nz, float dx, float dz, int data_nt, float data_dt,
+                   fwi2d_model_check &c);
+
 void injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz, float dx, float dz,
                       float ox, float oz, int *xind, int *zind, float *xw, float *zw);
 

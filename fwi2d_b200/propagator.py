@@ -58,6 +58,28 @@ def _injector(itype, tabs):
     return C.Injector(itype, len(xind), C.ptr(xind), C.ptr(zind), C.ptr(xw), C.ptr(zw))
 
 
+# the reference's param defaults for analyzeModel (src/include/param.hpp:11-46)
+MODEL_CHECK_DEFAULTS = dict(vpmin=0.2, vpmax=8.0, vsmin=0.1, vsmax=5.0, rhomin=0.1, rhomax=8.0, deltamin=-0.5,
+                            deltamax=1.0, epsilonmin=0.0, epsilonmax=1.0, soft_clip=0, acoustic_elastic=0,
+                            water_velocity=1.5, courant=0.6, dt=-1.0, sub=0)
+
+
+def analyze_model(model_raw, dx, dz, data_nt, data_dt, **par):
+    """analyzeModel (src/cpp/we_op.cpp:267-474) through the library's host
+    restatement: returns (the clipped raw model [npar][nx][nz], a dict with the
+    propagation dt, nt, sub, courant, tmax, vmax, vmin).  par overrides the
+    reference's defaults (MODEL_CHECK_DEFAULTS, the `param` field names)."""
+    L = C.load()
+    m = np.array(model_raw, np.float32, copy=True, order="C")
+    npar, nx, nz = m.shape
+    kw = dict(MODEL_CHECK_DEFAULTS)
+    kw.update(par)
+    c = C.ModelCheck(**kw)
+    C.check(L.fwi2d_analyze_model(npar, C.ptr(m), nx, nz, float(dx), float(dz), int(data_nt), float(data_dt),
+                                  ctypes.byref(c)))
+    return m, {k: getattr(c, k) for k in ("dt", "nt", "sub", "courant", "tmax", "vmax", "vmin")}
+
+
 def prop_nt(nd, dt_data, dt):
     """Propagation length the reference derives for nd data samples at
     dt_data (analyzeModel, src/cpp/we_op.cpp:436-464): tmax = (nd - 1) dt_data in

@@ -92,6 +92,30 @@ typedef struct fwi2d_ctx fwi2d_ctx;
 const char *fwi2d_last_error(void);
 int fwi2d_version(void);
 
+/* The fields of the reference's `param` that analyzeModel reads and writes
+ * (src/include/param.hpp:11-46; defaults there: courant 0.6, dt -1, sub 0,
+ * vp 0.2-8, vs 0.1-5, rho 0.1-8, delta -0.5-1, epsilon 0-1 km/s, g/cc). */
+typedef struct fwi2d_model_check {
+    float vpmin, vpmax, vsmin, vsmax, rhomin, rhomax, deltamin, deltamax, epsilonmin, epsilonmax;
+    int soft_clip;          /* keep values outside the bounds (elastic and VTI only) */
+    int acoustic_elastic;   /* the water velocity joins vmax / vmin */
+    float water_velocity;
+    float courant;          /* in/out */
+    float dt;               /* in/out: 0 from the CFL number; > 0 min(dt, data step); < 0 the CFL step rounded down to divide the data step */
+    int sub;                /* in/out: < 0 becomes round(data step / dt) */
+    int nt;                 /* out: round(tmax / dt) + 1 */
+    float tmax, vmax, vmin; /* out */
+} fwi2d_model_check;
+
+/* analyzeModel (src/cpp/we_op.cpp:267-474) on a raw host model [npar][nx][nz]
+ * (npar 2: vp, rho; 3: vp, vs, rho; 5: + delta, epsilon), in place: the Thomsen
+ * delta admissibility clip (VTI), the hard clip to the bounds, Vs <= Vp/sqrt(2),
+ * the maximum P velocity (VTI: vp sqrt(1 + 2 eps)), then the propagation step,
+ * nt and sub from the data time axis (data_nt samples at data_dt).  Host only:
+ * needs no GPU. */
+int fwi2d_analyze_model(int npar, float *model, int nx, int nz, float dx, float dz, int data_nt, float data_dt,
+                        fwi2d_model_check *check);
+
 /* delta_m3 / ddelta_m3::findIndicesWeights (src/cpp/injector.cpp:3-64, 114-187). */
 int fwi2d_injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz,
                            float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw);

@@ -237,6 +237,20 @@ class Reference(_Lib):
             raise RuntimeError("reference misfit/gradient failed")
         return syn, g
 
+    def analyze_model(self, model_raw, nx, nz, dx, dz, data_nt, data_dt, checks):
+        """analyzeModel on a copy of the raw model [npar][nx][nz]; checks: the
+        16 inputs of ref_analyze_model.  Returns (model, outputs dict)."""
+        f = self.lib.ref_analyze_model
+        f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                      ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
+        m = self.arr(model_raw).copy()
+        c = np.zeros(20, np.float64)
+        c[:16] = checks
+        if f(m.shape[0], _ptr(m), nx, nz, dx, dz, data_nt, data_dt, _ptr(c)) != 0:
+            raise RuntimeError("reference analyzeModel failed")
+        keys = ("courant", "dt", "sub", "nt", "tmax", "vmax", "vmin")
+        return m, dict(zip(keys, c[13:20]))
+
     def misfit_grad_rs(self, kind, par, nx, nz, d, nd, dd, prop_dt, method, hl, src_loc, rcv_locs, model_raw, src,
                        obs=None):
         """misfit_grad with sources and data on their own axis (nd samples at

@@ -168,6 +168,42 @@ int ref_misfit_grad_rs(int kind, const ref_param *rp, int nx, int nz, double dx,
                        model, src, obs, syn, grad);
 }
 
+// analyzeModel (we_op.cpp:267-474) on a raw model [npar][nx][nz] in place,
+// with the data time axis (data_nt samples at data_dt).  c holds, in order:
+// vpmin, vpmax, vsmin, vsmax, rhomin, rhomax, deltamin, deltamax, epsilonmin,
+// epsilonmax, soft_clip, acoustic_elastic, water_velocity, courant, dt, sub
+// (inputs) and receives courant, dt, sub, nt, tmax, vmax, vmin in c[13..19].
+int ref_analyze_model(int npar, data_t *model, int nx, int nz, double dx, double dz, int data_nt, double data_dt,
+                      double *c)
+{
+    try {
+        param par;
+        par.verbose = 0;
+        par.nmodels = npar;
+        par.vpmin = (data_t)c[0]; par.vpmax = (data_t)c[1]; par.vsmin = (data_t)c[2]; par.vsmax = (data_t)c[3];
+        par.rhomin = (data_t)c[4]; par.rhomax = (data_t)c[5]; par.deltamin = (data_t)c[6]; par.deltamax = (data_t)c[7];
+        par.epsilonmin = (data_t)c[8]; par.epsilonmax = (data_t)c[9];
+        par.soft_clip = c[10] != 0;
+        par.acoustic_elastic = c[11] != 0;
+        par.water_velocity = (data_t)c[12];
+        par.courant = (data_t)c[13];
+        par.dt = (data_t)c[14];
+        par.sub = (int)c[15];
+        hypercube<data_t> dom(axis<data_t>(nz, 0, (data_t)dz), axis<data_t>(nx, 0, (data_t)dx), axis<data_t>(npar, 0, 1));
+        auto m = std::make_shared<vecReg<data_t> >(dom);
+        std::memcpy(m->getVals(), model, (size_t)npar * nx * nz * sizeof(data_t));
+        hypercube<data_t> T(axis<data_t>(data_nt, 0, (data_t)data_dt), axis<data_t>(1, 0, 1));
+        analyzeModel(T, m, par);
+        std::memcpy(model, m->getCVals(), (size_t)npar * nx * nz * sizeof(data_t));
+        c[13] = par.courant; c[14] = par.dt; c[15] = par.sub; c[16] = par.nt; c[17] = par.tmax;
+        c[18] = par.vmax; c[19] = par.vmin;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_analyze_model: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
 // The reference's time resamplers (operator.cpp:760-856) on ntr traces:
 // domain axis (nm samples at dm), range axis (np samples at dp), both from
 // t = 0.  adjoint = 0: in [ntr][nm] -> out [ntr][np] (apply_forward);

@@ -189,6 +189,51 @@ def fwi_case_resampled():
     return out
 
 
+# analyzeModel inputs: vpmin, vpmax, vsmin, vsmax, rhomin, rhomax, deltamin, deltamax, epsilonmin,
+# epsilonmax, soft_clip, acoustic_elastic, water_velocity, courant, dt, sub (param.hpp defaults first)
+CHECK_DEFAULTS = [0.2, 8, 0.1, 5, 0.1, 8, -0.5, 1, 0, 1, 0, 0, 1.5, 0.6, -1, 0]
+ANALYZE_CASES = [
+    # name, kind, overrides (index: value), data_nt, data_dt
+    ("elastic_cfl_rounded", O.KIND_ELASTIC, {15: -1}, 1251, 2e-3),
+    ("elastic_cfl", O.KIND_ELASTIC, {14: 0}, 1251, 2e-3),
+    ("elastic_given_soft", O.KIND_ELASTIC, {14: 4e-4, 10: 1, 15: -1}, 501, 1e-3),
+    ("elastic_tight_bounds", O.KIND_ELASTIC, {0: 2.1, 1: 2.6, 3: 1.2, 5: 2.2}, 801, 1.5e-3),
+    ("vti", O.KIND_VTI, {7: 0.08, 9: 0.15, 15: -1}, 1001, 2e-3),
+    ("acoustic", O.KIND_ACOUSTIC, {0: 2.05, 14: -1}, 1001, 4e-4),
+    ("acoustic_elastic", O.KIND_ELASTIC, {11: 1, 12: 1.5, 13: 0.5}, 1201, 2e-3),
+    ("data_finer_than_cfl", O.KIND_ELASTIC, {}, 2001, 2e-4),
+]
+
+
+def analyze_case():
+    """analyzeModel of the reference (we_op.cpp:267-474) on seeded raw models
+    that trip its clips (Vs above Vp/sqrt(2), values outside the bounds, VTI
+    delta outside its admissible range) over the dt / sub branches."""
+    lib = O.Reference(32)
+    out = {}
+    nx, nz, d = 40, 30, 0.01
+    for k, (name, kind, ov, dnt, ddt) in enumerate(ANALYZE_CASES):
+        m = K.model_case(kind, nx, nz, d, seed=20 + k)
+        rng = np.random.default_rng(40 + k)
+        if kind != O.KIND_ACOUSTIC:
+            m[1].flat[rng.integers(0, nx * nz, 30)] *= 1.6          # Vs above Vp/sqrt(2) here and there
+        m[0].flat[rng.integers(0, nx * nz, 10)] = 9.0               # above vpmax
+        if kind == O.KIND_VTI:
+            m[3].flat[rng.integers(0, nx * nz, 20)] = rng.uniform(-0.9, 3.0, 20)   # inadmissible delta
+        chk = list(CHECK_DEFAULTS)
+        for i, v in ov.items():
+            chk[i] = v
+        mo, res = lib.analyze_model(m, nx, nz, d, d, dnt, ddt, chk)
+        out["name%d" % k] = np.array(name)
+        out["in%d" % k] = m.astype(np.float32)
+        out["check%d" % k] = np.array(chk, np.float64)
+        out["axis%d" % k] = np.array([dnt, ddt], np.float64)
+        out["out%d" % k] = mo
+        out["res%d" % k] = np.array([res[key] for key in ("courant", "dt", "sub", "nt", "tmax", "vmax", "vmin")])
+    out["grid"] = np.array([nx, nz, d])
+    return out
+
+
 def fwi_case_ae():
     """The acoustic-elastic solver gradient (nl_we_op_ae through the
     operator interface, residual weighted by applyHt), fluid source."""
@@ -231,6 +276,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, "fwi_gradient_%s_f32.npz" % name), **fwi_case(kind))
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_f32.npz"), **fwi_case_ae())
     np.savez_compressed(os.path.join(HERE, "resample_f32.npz"), **resample_case())
+    np.savez_compressed(os.path.join(HERE, "analyze_model_f32.npz"), **analyze_case())
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_elastic_resampled_f32.npz"), **fwi_case_resampled())
     print("golden fixtures written to", HERE)
 

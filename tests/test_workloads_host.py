@@ -49,3 +49,32 @@ def test_shard_shots_partitions_and_balances():
         assert flat == list(range(17))
         loads = [sum(D.shot_cost(shots[i], 1) for i in p) for p in parts]
         assert max(loads) - min(loads) <= max(D.shot_cost(s, 1) for s in shots)
+
+
+def test_analyze_model_matches_reference():
+    """The library's host analyzeModel (fwi2d_analyze_model) reproduces the
+    reference's (we_op.cpp:267-474, fixtures written by its own build): the
+    clipped model bit for bit and the derived dt, nt, sub, courant, tmax, vmax
+    and vmin, over the dt / sub branches and the VTI, acoustic and
+    acoustic-elastic cases."""
+    import os
+    import fwi2d_b200 as F
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "analyze_model_f32.npz")))
+    nx, nz, d = int(g["grid"][0]), int(g["grid"][1]), float(g["grid"][2])
+    keys = ("vpmin", "vpmax", "vsmin", "vsmax", "rhomin", "rhomax", "deltamin", "deltamax", "epsilonmin",
+            "epsilonmax", "soft_clip", "acoustic_elastic", "water_velocity", "courant", "dt", "sub")
+    k = 0
+    while "in%d" % k in g:
+        chk = dict(zip(keys, g["check%d" % k]))
+        for key in ("soft_clip", "acoustic_elastic", "sub"):
+            chk[key] = int(chk[key])
+        dnt, ddt = int(g["axis%d" % k][0]), float(g["axis%d" % k][1])
+        m, r = F.analyze_model(g["in%d" % k], d, d, dnt, ddt, **chk)
+        name = str(g["name%d" % k])
+        assert np.array_equal(m, g["out%d" % k]), name
+        ref = dict(zip(("courant", "dt", "sub", "nt", "tmax", "vmax", "vmin"), g["res%d" % k]))
+        for key in ("courant", "dt", "tmax", "vmax", "vmin"):
+            assert np.float32(r[key]) == np.float32(ref[key]), (name, key, r[key], ref[key])
+        assert r["nt"] == int(ref["nt"]) and r["sub"] == int(ref["sub"]), name
+        k += 1
+    assert k == 8
