@@ -11,7 +11,10 @@ Cell-updates per step: (nt-1) * nx * nz forward + the same adjoint.
 At N = 1 the line also carries "batched": the same evaluation for a batch of
 32 shots of the batch geometry (every other shot of the 64-shot line, cropped
 grids of 1.0-3.5 km apertures, 1.2-2.0 s records) on the elastic model with
-FP16 snapshots, all shots in one plan, timed the same way.
+FP16 snapshots, all shots in one plan, timed the same way.  It also carries
+"reference_gpu": the reference's own GPU implementation (src/cuda, built for
+sm_100a into oracle/_ref by oracle/build_ref.sh) timed on a bounded sample of
+the same shot, with "e2e_speedup" = this library's end-to-end value over it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config single|batch]
 
@@ -184,13 +187,17 @@ def cells_per_step(wl):
 # ---------------------------------------------------------------------------
 # CPU reference timing (reference sources built in oracle/_ref, else the port)
 # ---------------------------------------------------------------------------
-def cpu_sample(wl, nt_sample):
+def cpu_sample(wl, nt_sample, lib=None):
     """Forward with snapshots + adjoint with imaging on the full grid of the
-    first shot, nt_sample time samples.  Returns (seconds, cell-updates, kind)."""
+    first shot, nt_sample time samples.  Returns (seconds, cell-updates, kind).
+    lib: the reference build (default: oracle/_ref, else the port)."""
     import oracle as O
     from fwi2d_b200 import workloads as W
-    kind = "reference" if O.have_reference(32) else "port"
-    lib = O.Reference(32) if kind == "reference" else O.Port(32)
+    if lib is None:
+        kind = "reference" if O.have_reference(32) else "port"
+        lib = O.Reference(32) if kind == "reference" else O.Port(32)
+    else:
+        kind = lib.kind
     s = wl["shots"][0]
     nx, nz, d = s["nx"], wl["nz"], wl["d"]
     k = wl["kind"]
@@ -213,6 +220,28 @@ def cpu_sample(wl, nt_sample):
     lib.propagate(k, 1, model, adj, srcb, par, nx, nz, d, d, 0.0, 0.0, rl, sl, full=full, grad=g)
     dtime = time.perf_counter() - t0
     return dtime, 2 * (nt_sample - 1) * nx * nz, kind
+
+
+def reference_gpu_sample(wl, nt_sample=1001, reps=2):
+    """The reference's own GPU path (src/cuda, propagate_gpu, built into
+    oracle/_ref/libfwi2d_ref32_cuda.so) on the same shot: forward with
+    snapshots copied to host memory, then the adjoint with imaging, nt_sample
+    time samples, wall clock (the path is synchronous with the host).  Best of
+    reps after one warm-up.  None when that build is absent."""
+    import oracle as O
+    if not O.have_reference_gpu():
+        return None
+    lib = O.ReferenceGPU()
+    cpu_sample(wl, 21, lib)
+    best, cells = None, 0
+    for _ in range(reps):
+        t, cells, _ = cpu_sample(wl, nt_sample, lib)
+        best = t if best is None else min(best, t)
+    g = cells / best / 1e9
+    return {"value": g, "unit": "Gcell-updates/s", "kind": "reference GPU path (src/cuda, propagate_gpu, sm_100a)",
+            "sample": "forward+adjoint gradient of shot 0, %d of %d time samples, host snapshots as the reference"
+                      % (nt_sample, wl["nt"]),
+            "shots_per_s": g * 1e9 / cells_per_step(wl) * len(wl["shots"])}
 
 
 def cpu_cores():
@@ -246,6 +275,13 @@ def run_reference(args):
             "cpu_baseline": {"value": gcell, "unit": "Gcell-updates/s", "cores": cpu_cores(), "kind": kind,
                              "sample": sample},
             "e2e": {"value": gcell, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.config == "single":
+        try:   # the reference's GPU path beside its CPU path, for context (not this line's value)
+            rg = reference_gpu_sample(wl)
+            if rg is not None:
+                line["reference_gpu"] = rg
+        except Exception as e:
+            line["reference_gpu"] = {"value": None, "sample": "failed: %s" % e}
     print(json.dumps(line), flush=True)
 
 
@@ -402,6 +438,14 @@ def run_ours(args):
                 line["batched"] = b
             except Exception as e:   # the batched leg never blocks the main line
                 line["batched"] = {"error": str(e)}
+        if world == 1 and args.config == "single":
+            try:
+                rg = reference_gpu_sample(wl)
+                if rg is not None:
+                    rg["e2e_speedup"] = line["e2e"]["value"] / rg["value"]
+                    line["reference_gpu"] = rg
+            except Exception as e:   # the comparison never blocks the GPU line
+                line["reference_gpu"] = {"value": None, "sample": "failed: %s" % e}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 nt_s = 301

@@ -32,4 +32,31 @@ for prec in 32 64; do
     done
     g++ -shared -fopenmp -o "$OUT/libfwi2d_ref$prec.so" $OBJS -Wl,--no-undefined
 done
+# The reference's GPU path (src/cuda/cudaKernels.cu, cudaWeOp.cpp; the
+# reference's CMake adds -DCUDA and compiles the .cu with -std=c++11 -O3 -w
+# -Xcompiler -fopenmp), FP32, for sm_100a: libfwi2d_ref32_cuda.so, used only to
+# time the reference's own GPU implementation beside this library.
+CUDA_HOME=${CUDA_HOME:-/usr/local/cuda}
+if [ -x "$CUDA_HOME/bin/nvcc" ]; then
+    B="$OUT/objcuda"
+    mkdir -p "$B"
+    INC="-I$HERE/ref_shim -I$REF/src/include -I$REF/src/cuda -I$CUDA_HOME/include"
+    OBJS=""
+    for s in we_op.cpp spatial_operators.cpp injector.cpp misc.cpp operator.cpp; do
+        o="$B/${s%.cpp}.o"
+        g++ -std=c++11 -O3 -fopenmp -fPIC -fpermissive -w -DCUDA $INC -c "$REF/src/cpp/$s" -o "$o"
+        OBJS="$OBJS $o"
+    done
+    g++ -std=c++11 -O3 -fopenmp -fPIC -fpermissive -w -DCUDA $INC -c "$REF/src/cuda/cudaWeOp.cpp" -o "$B/cudaWeOp.o"
+    "$CUDA_HOME/bin/nvcc" -std=c++11 -O3 -w -Xcompiler -fopenmp,-fPIC -gencode arch=compute_100a,code=sm_100a \
+        $INC -c "$REF/src/cuda/cudaKernels.cu" -o "$B/cudaKernels.o"
+    OBJS="$OBJS $B/cudaWeOp.o $B/cudaKernels.o"
+    for s in ispc_loops.cpp stubs.cpp ref_driver.cpp; do
+        o="$B/${s%.cpp}.o"
+        g++ -std=c++11 -O3 -fopenmp -fPIC -w -DCUDA $INC -c "$HERE/ref_shim/$s" -o "$o"
+        OBJS="$OBJS $o"
+    done
+    g++ -shared -fopenmp -o "$OUT/libfwi2d_ref32_cuda.so" $OBJS -L"$CUDA_HOME/lib64" -lcudart_static -ldl -lrt -lpthread \
+        -Wl,--no-undefined
+fi
 echo "reference oracle built in $OUT"

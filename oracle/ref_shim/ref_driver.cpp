@@ -204,6 +204,36 @@ int ref_analyze_model(int npar, data_t *model, int nx, int nz, double dx, double
     return 0;
 }
 
+#ifdef CUDA
+// The reference's own GPU path (src/cuda/cudaWeOp.cpp, built with -DCUDA):
+// nl_we_op_e / nl_we_op_vti::propagate_gpu with ref_propagate's arguments
+// (kind 0 or 1).  Used only to time the reference's GPU implementation.
+int ref_propagate_gpu(int kind, int adj, const data_t *model, const data_t *allsrc, data_t *allrcv,
+                      int inj_type, int ninj, const data_t *ix, const data_t *iz,
+                      int next, const data_t *ex, const data_t *ez,
+                      data_t *full, data_t *grad, const ref_param *rp, int nx, int nz,
+                      double dx, double dz, double ox, double oz)
+{
+    try {
+        param par = to_param(rp);
+        par.device = 0;
+        hypercube<data_t> g = grid(nx, nz, dx, dz, ox, oz);
+        injector *inj = inj_type == 0 ? (injector *)new delta_m3(g, locs(ninj, ix, iz))
+                                      : (injector *)new ddelta_m3(g, locs(ninj, ix, iz));
+        injector *ext = new delta_m3(g, locs(next, ex, ez));
+        if (kind == 0) { nl_we_op_e op; op.propagate_gpu(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, (data_t)ox, (data_t)oz, 0); }
+        else if (kind == 1) { nl_we_op_vti op; op.propagate_gpu(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, (data_t)ox, (data_t)oz, 0); }
+        else return -1;
+        delete inj;
+        delete ext;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_propagate_gpu: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+#endif
+
 // The reference's time resamplers (operator.cpp:760-856) on ntr traces:
 // domain axis (nm samples at dm), range axis (np samples at dp), both from
 // t = 0.  adjoint = 0: in [ntr][nm] -> out [ntr][np] (apply_forward);
