@@ -259,6 +259,35 @@ class Reference(_Lib):
         keys = ("courant", "dt", "sub", "nt", "tmax", "vmax", "vmin")
         return m, dict(zip(keys, c[13:20]))
 
+    def bin_write(self, header, vals, axes, datapath):
+        """binWrite of vals (axis 1 = last numpy index); axes: (o, d) per axis,
+        axis 1 first."""
+        f = self.lib.ref_bin_write
+        f.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                      ctypes.c_void_p, ctypes.c_char_p]
+        v = self.arr(vals)
+        n = np.array(v.shape[::-1], np.int32)
+        o = np.array([a[0] for a in axes], np.float64)
+        d = np.array([a[1] for a in axes], np.float64)
+        if f(header.encode(), _ptr(v), len(n), _ptr(n), _ptr(o), _ptr(d), datapath.encode()) != 0:
+            raise RuntimeError("reference binWrite failed")
+
+    def bin_read(self, header, ndim0=1, cap=1 << 24):
+        """binRead: (array with axis 1 last, [(n, o, d)] of the kept axes)."""
+        f = self.lib.ref_bin_read
+        f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        out = np.zeros(cap, self.dtype)
+        nd = np.zeros(1, np.int32)
+        n = np.zeros(6, np.int32)
+        o = np.zeros(6, np.float64)
+        d = np.zeros(6, np.float64)
+        if f(header.encode(), ndim0, _ptr(out), cap, _ptr(nd), _ptr(n), _ptr(o), _ptr(d)) != 0:
+            raise RuntimeError("reference binRead failed")
+        k = int(nd[0])
+        shape = [int(x) for x in n[:k]]
+        return out[:int(np.prod(shape))].reshape(shape[::-1]).copy(), [(shape[i], o[i], d[i]) for i in range(k)]
+
     def misfit_grad_rs(self, kind, par, nx, nz, d, nd, dd, prop_dt, method, hl, src_loc, rcv_locs, model_raw, src,
                        obs=None):
         """misfit_grad with sources and data on their own axis (nd samples at

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include "we_op.hpp"
+#include "IO.hpp"
 
 struct ref_param {
     int nt, sub;
@@ -199,6 +200,42 @@ int ref_analyze_model(int npar, data_t *model, int nx, int nz, double dx, double
         c[18] = par.vmax; c[19] = par.vmin;
     } catch (const std::exception &e) {
         std::fprintf(stderr, "ref_analyze_model: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+// binWrite (IO.hpp:179-222): vals on ndim axes (axis 1 first: n, o, d) to
+// the header file `header` and its binary <datapath>/<header>@.
+int ref_bin_write(const char *header, const data_t *vals, int ndim, const int *n, const double *o, const double *d,
+                  const char *datapath)
+{
+    try {
+        std::vector<axis<data_t> > ax;
+        for (int i = 0; i < ndim; i++) ax.push_back(axis<data_t>(n[i], (data_t)o[i], (data_t)d[i]));
+        auto v = std::make_shared<vecReg<data_t> >(hypercube<data_t>(ax));
+        std::memcpy(v->getVals(), vals, v->getN123() * sizeof(data_t));
+        binWrite<data_t>(v, header, datapath);
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_bin_write: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+// binRead (IO.hpp:226-429): the samples into out (at most cap), the kept
+// axes into ndim, n, o, d (6 entries each).
+int ref_bin_read(const char *header, int ndim0, data_t *out, long cap, int *ndim, int *n, double *o, double *d)
+{
+    try {
+        auto v = binRead<data_t>(header, ndim0);
+        const std::vector<axis<data_t> > ax = v->getHyper()->getAxes();
+        *ndim = (int)ax.size();
+        for (int i = 0; i < *ndim; i++) { n[i] = ax[i].n; o[i] = ax[i].o; d[i] = ax[i].d; }
+        if (v->getN123() > cap) return -2;
+        std::memcpy(out, v->getCVals(), v->getN123() * sizeof(data_t));
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_bin_read: %s\n", e.what());
         return -1;
     }
     return 0;

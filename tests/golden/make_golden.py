@@ -234,6 +234,27 @@ def analyze_case():
     return out
 
 
+SEP_AXES = [(0.0, 0.005), (0.5, 0.005), (0.0, 1.0)]   # (o, d): z, x, parameter
+
+
+def sep_values():
+    return np.random.default_rng(3).standard_normal((3, 20, 16)).astype(np.float32)
+
+
+def sep_case():
+    """A model cube written by the reference's binWrite (IO.hpp:179-222) into
+    tests/golden/sep/ (header model_ref.H, binary model_ref.H@, datapath ".")."""
+    lib = O.Reference(32)
+    d = os.path.join(HERE, "sep")
+    os.makedirs(d, exist_ok=True)
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        lib.bin_write("model_ref.H", sep_values(), SEP_AXES, ".")
+    finally:
+        os.chdir(cwd)
+
+
 def fwi_case_ae():
     """The acoustic-elastic solver gradient (nl_we_op_ae through the
     operator interface, residual weighted by applyHt), fluid source."""
@@ -277,6 +298,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_f32.npz"), **fwi_case_ae())
     np.savez_compressed(os.path.join(HERE, "resample_f32.npz"), **resample_case())
     np.savez_compressed(os.path.join(HERE, "analyze_model_f32.npz"), **analyze_case())
+    sep_case()
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_elastic_resampled_f32.npz"), **fwi_case_resampled())
     print("golden fixtures written to", HERE)
 
