@@ -157,29 +157,29 @@ def resample_case():
     return out
 
 
-def fwi_case_resampled():
-    """The elastic solver gradient with sources and data sampled at 2.5 ms and
-    the propagation at 1 ms: the reference's apply_forward / apply_jacobianT
+def fwi_case_resampled(kind=O.KIND_ELASTIC, methods=("sinc", "linear")):
+    """The solver gradient with sources and data sampled at 2.5 ms and the
+    propagation at 1 ms: the reference's apply_forward / apply_jacobianT
     resample (sinc, then linear) around the propagation (ref_misfit_grad_rs)."""
     lib = O.Reference(32)
-    kind = O.KIND_ELASTIC
     nx, nz, d, dt, dd, nd = 100, 80, 0.01, 1e-3, 2.5e-3, 161
     true = K.model_case(kind, nx, nz, d, seed=7)
     from scipy.ndimage import gaussian_filter
     start = true.copy()
-    for c in range(3):
+    for c in range(true.shape[0] if kind != O.KIND_VTI else 3):
         start[c] = gaussian_filter(true[c].astype(np.float64), 4, mode="nearest").astype(np.float32)
     sx, sz = (0.5 * (nx - 1) + 0.3) * d, 0.02
     rx = np.linspace(3 * d, (nx - 4) * d, 30).astype(np.float32)
     rz = np.full(30, 0.02, np.float32)
-    src = K.sources(2, nd, dd).reshape(2, nd)
+    nc = 1 if kind == O.KIND_ACOUSTIC else 2
+    src = K.sources(nc, nd, dd).reshape(nc, nd)
     nt = 401
     par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=30)
     out = dict(kind=kind, nx=nx, nz=nz, d=d, nt=nt, dt=dt, dd=dd, nd=nd, sx=sx, sz=sz, rx=rx, rz=rz, true=true,
                start=start, src=src)
     w = np.full(nd, dd)
     w[0] = w[-1] = 0.5 * dd
-    for method in ("sinc", "linear"):
+    for method in methods:
         geo = ((np.float32(sx), np.float32(sz)), (rx, rz))
         obs, _ = lib.misfit_grad_rs(kind, par, nx, nz, d, nd, dd, dt, method, 11, geo[0], geo[1], true, src)
         syn, g = lib.misfit_grad_rs(kind, par, nx, nz, d, nd, dd, dt, method, 11, geo[0], geo[1], start, src, obs)
@@ -300,6 +300,10 @@ def main():
     np.savez_compressed(os.path.join(HERE, "analyze_model_f32.npz"), **analyze_case())
     sep_case()
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_elastic_resampled_f32.npz"), **fwi_case_resampled())
+    np.savez_compressed(os.path.join(HERE, "fwi_gradient_vti_resampled_f32.npz"),
+                        **fwi_case_resampled(O.KIND_VTI, ("sinc",)))
+    np.savez_compressed(os.path.join(HERE, "fwi_gradient_acoustic_resampled_f32.npz"),
+                        **fwi_case_resampled(O.KIND_ACOUSTIC, ("linear",)))
     print("golden fixtures written to", HERE)
 
 

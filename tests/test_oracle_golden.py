@@ -88,7 +88,7 @@ def test_fwi_gradient_fixture_reproduced_by_reference_build(path):
         nx, nz, d, nt, dt = int(g["nx"]), int(g["nz"]), float(g["d"]), int(g["nt"]), float(g["dt"])
         par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(1, 2, 2, 2), taper=(0, 10, 10, 10)), ns=1, nr=len(g["rx"]))
         geo = ((np.float32(g["sx"]), np.float32(g["sz"])), (g["rx"], g["rz"]))
-        for method in ("sinc", "linear"):
+        for method in [m for m in ("sinc", "linear") if "grad_" + m in g]:
             args = (int(g["kind"]), par, nx, nz, d, int(g["nd"]), float(g["dd"]), dt, method, 11, geo[0], geo[1])
             syn, _ = lib.misfit_grad_rs(*args, g["true"], g["src"])
             assert np.array_equal(syn, g["obs_" + method])
