@@ -1981,6 +1981,10 @@ static void set_data_axis(fwi2d_ctx *ctx, float dd, int method, int hl, const in
     std::vector<int> v(nd, nd + P.shots.size());
     for (size_t k = 0; k < P.shots.size(); k++) {
         REQ(v[k] >= 2, "a shot needs at least two data samples");
+        // the trace kernels put rows or samples on grid.y
+        REQ(P.shots[k]->nt <= 65535 && v[k] <= 65535 && P.shots[k]->nrcv_rows <= 65535 &&
+                P.shots[k]->nsrc_rows <= 65535,
+            "data-axis resampling supports at most 65535 samples and trace rows per shot");
         const float tmax = (v[k] - 1) * dd;
         const int nt = (int)std::round(tmax / P.par.dt) + 1;
         if (nt != P.shots[k]->nt)
