@@ -2107,6 +2107,16 @@ int fwi2d_injector_weights(int type, int ntr, const float *locx, const float *lo
     ABI_END
 }
 
+int fwi2d_dipole_weights(int ntr, const float *locx, const float *locz, const float *dip, float gl, int nx, int nz,
+                         float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw)
+{
+    ABI_TRY
+    REQ(ntr >= 0 && nx >= 3 && nz >= 3 && dx > 0 && dz > 0 && gl > 0, "invalid grid or gauge length");
+    REQ(ntr == 0 || (locx && locz && dip && xind && zind && xw && zw), "null array");
+    dipole_weights(ntr, locx, locz, dip, gl, nx, nz, dx, dz, ox, oz, xind, zind, xw, zw);
+    ABI_END
+}
+
 int fwi2d_analyze_model(int npar, float *model, int nx, int nz, float dx, float dz, int data_nt, float data_dt,
                         fwi2d_model_check *check)
 {
@@ -2412,6 +2422,44 @@ int fwi2d_fwi_gradient(fwi2d_ctx *ctx, const float *model, const float *src, con
     ABI_END
 }
 
+}  // extern "C"
+
+// Dipole receivers (dipole_m3) in the drop-in: each dipole becomes two delta
+// receivers, one per end, interleaved (trace t's ends are rows 2t and 2t+1),
+// with the dipole's own index and weight tables.  The forward's dipole trace is
+// end 2 minus end 1 (injector.cpp:359-380, the same per-cell products summed
+// per end); the adjoint injects -q at end 1 and +q at end 2 (:328-357).
+struct DipoleSplit {
+    std::vector<int> xi, zi;
+    std::vector<float> xw, zw;
+    fwi2d_injector inj;
+};
+
+static void split_dipole(const fwi2d_injector &d, DipoleSplit &s)
+{
+    REQ(d.ntr >= 0 && (d.ntr == 0 || (d.xind && d.zind && d.xw && d.zw)), "dipole injector: null table");
+    const int n = d.ntr;
+    s.xi.resize((size_t)6 * n);
+    s.zi.resize((size_t)6 * n);
+    s.xw.resize((size_t)12 * n);
+    s.zw.resize((size_t)12 * n);
+    for (int t = 0; t < n; t++)
+        for (int e = 0; e < 2; e++) {
+            const int row = 2 * t + e;
+            for (int k = 0; k < 3; k++) {
+                s.xi[row * 3 + k] = d.xind[t * 6 + 3 * e + k];
+                s.zi[row * 3 + k] = d.zind[t * 6 + 3 * e + k];
+                for (int p = 0; p < 2; p++) {
+                    s.xw[(row * 2 + p) * 3 + k] = d.xw[(t * 2 + p) * 6 + 3 * e + k];
+                    s.zw[(row * 2 + p) * 3 + k] = d.zw[(t * 2 + p) * 6 + 3 * e + k];
+                }
+            }
+        }
+    s.inj = {FWI2D_INJ_DELTA, 2 * n, s.xi.data(), s.zi.data(), s.xw.data(), s.zw.data()};
+}
+
+extern "C" {
+
 int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, float *allrcv,
                     const fwi2d_injector *inj, const fwi2d_injector *ext, const fwi2d_injector *inja,
                     const fwi2d_injector *exta, float *full_wfld, float *grad, const fwi2d_params *par, int ns, int nr,
@@ -2429,6 +2477,14 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
     if (!ae) REQ(inj && ext, "null argument");
     else if (!adj) REQ(ext && exta && (src_fluid ? inja : inj), "null argument");
     else REQ(inj && inja && (src_fluid || ext), "null argument");
+    // dipole receivers: ext in the forward, inj in the adjoint (elastic and VTI)
+    const fwi2d_injector *rcv_side = adj ? inj : ext;
+    const bool dipole = rcv_side && rcv_side->type == FWI2D_INJ_DIPOLE;
+    if (dipole && kind != FWI2D_ELASTIC && kind != FWI2D_VTI)
+        throw Error(FWI2D_ERR_UNSUPPORTED, "dipole receivers are supported for the elastic and VTI propagators");
+    REQ(!((adj ? ext : inj) && (adj ? ext : inj)->type == FWI2D_INJ_DIPOLE), "a dipole cannot be a source");
+    DipoleSplit dsplit;
+    if (dipole) split_dipole(*rcv_side, dsplit);
     const fwi2d_injector none = {FWI2D_INJ_DELTA, 0, nullptr, nullptr, nullptr, nullptr};
     int dev = 0;
     CK(cudaGetDevice(&dev));
@@ -2447,7 +2503,7 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
     sh.nt = nt;
     if (!ae) {
         sh.src = adj ? *ext : *inj;
-        sh.rcv = adj ? *inj : *ext;
+        sh.rcv = dipole ? dsplit.inj : (adj ? *inj : *ext);
         if (adj) p.mt = sh.src.type == FWI2D_INJ_DDELTA;
     } else if (!adj) {
         sh.src = src_fluid ? none : *inj;
@@ -2473,20 +2529,43 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
     const int in_comp = adj ? out_comp : S.ncomp_src;
     const int stride = adj ? nr : ns;
     std::vector<float> in((size_t)in_comp * in_ntr * nt);
-    for (int c = 0; c < in_comp; c++)
-        for (int t = 0; t < in_ntr; t++)
-            std::memcpy(&in[((size_t)c * in_ntr + t) * nt], allsrc + ((size_t)c * stride + t) * nt, nt * sizeof(float));
+    if (dipole && adj) {
+        // end 1 takes -q, end 2 +q
+        for (int c = 0; c < in_comp; c++)
+            for (int t = 0; t < in_ntr / 2; t++) {
+                const float *q = allsrc + ((size_t)c * stride + t) * nt;
+                float *e1 = &in[((size_t)c * in_ntr + 2 * t) * nt], *e2 = e1 + nt;
+                for (int k = 0; k < nt; k++) {
+                    e1[k] = -q[k];
+                    e2[k] = q[k];
+                }
+            }
+    } else {
+        for (int c = 0; c < in_comp; c++)
+            for (int t = 0; t < in_ntr; t++)
+                std::memcpy(&in[((size_t)c * in_ntr + t) * nt], allsrc + ((size_t)c * stride + t) * nt,
+                            nt * sizeof(float));
+    }
     if (!adj) {
         std::vector<float> out((size_t)out_comp * S.nr * nt);
         upload_traces(ctx, in.data(), false);
         run(ctx, false, store);
         download_rcv(ctx, out.data());
-        for (int c = 0; c < out_comp; c++)
-            for (int t = 0; t < S.nr; t++) {
-                float *dst = allrcv + ((size_t)c * nr + t) * nt;
-                const float *src = &out[((size_t)c * S.nr + t) * nt];
-                for (int k = 0; k < nt; k++) dst[k] += src[k];
-            }
+        if (dipole) {
+            for (int c = 0; c < out_comp; c++)
+                for (int t = 0; t < S.nr / 2; t++) {
+                    float *dst = allrcv + ((size_t)c * nr + t) * nt;
+                    const float *e1 = &out[((size_t)c * S.nr + 2 * t) * nt], *e2 = e1 + nt;
+                    for (int k = 0; k < nt; k++) dst[k] += e2[k] - e1[k];
+                }
+        } else {
+            for (int c = 0; c < out_comp; c++)
+                for (int t = 0; t < S.nr; t++) {
+                    float *dst = allrcv + ((size_t)c * nr + t) * nt;
+                    const float *src = &out[((size_t)c * S.nr + t) * nt];
+                    for (int k = 0; k < nt; k++) dst[k] += src[k];
+                }
+        }
         if (store) store_host_snapshots(ctx, full_wfld);
     } else {
         load_host_snapshots(ctx, full_wfld);

@@ -242,6 +242,52 @@ static float hcoef_at(int n, int i)
     return 1.f;
 }
 
+// dipole_m3::findIndicesWeights (injector.cpp:241-326): the two ends lie at
+// loc -/+ gl/2 (cos dip, sin dip).  The end positions, pivots and alphas are
+// formed in double (the reference's cos / sin of a float resolve to the
+// double functions) and the alphas rounded to single precision; the weights
+// are the delta_m3 formulas in double from the single-precision alphas.
+void dipole_weights(int ntr, const float *locx, const float *locz, const float *dip, float gl, int nx, int nz,
+                    float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw)
+{
+    const float h = gl / 2;
+    auto pivot = [](double g, int n) {
+        int i = (int)std::round(g);
+        if (i == 0) i = 1;
+        if (i == n - 1) i = n - 2;
+        return i;
+    };
+    for (int t = 0; t < ntr; t++) {
+        const double c = std::cos((double)dip[t]), s = std::sin((double)dip[t]);
+        const double gx[2] = {((double)locx[t] - h * c - ox) / dx, ((double)locx[t] + h * c - ox) / dx};
+        const double gz[2] = {((double)locz[t] - h * s - oz) / dz, ((double)locz[t] + h * s - oz) / dz};
+        int *xi = xind + 6 * t, *zi = zind + 6 * t;
+        float *xi0 = xw + 12 * t, *xe = xi0 + 6, *zi0 = zw + 12 * t, *ze = zi0 + 6;
+        for (int e = 0; e < 2; e++) {
+            const int px = pivot(gx[e], nx), pz = pivot(gz[e], nz);
+            for (int k = 0; k < 3; k++) {
+                xi[3 * e + k] = px - 1 + k;
+                zi[3 * e + k] = pz - 1 + k;
+            }
+            const float ax = (float)(gx[e] - px), az = (float)(gz[e] - pz);
+            const double ax2 = (double)ax * (double)ax, az2 = (double)az * (double)az;
+            float *wx = xi0 + 3 * e, *vx = xe + 3 * e, *wz = zi0 + 3 * e, *vz = ze + 3 * e;
+            wx[0] = (float)((ax2 - ax) / (double)(2 * dx * hcoef_at(nx, px - 1)));
+            wx[1] = (float)((-ax2 + 1) / (double)(dx * hcoef_at(nx, px)));
+            wx[2] = (float)((ax2 + ax) / (double)(2 * dx * hcoef_at(nx, px + 1)));
+            wz[0] = (float)((az2 - az) / (double)(2 * dz * hcoef_at(nz, pz - 1)));
+            wz[1] = (float)((-az2 + 1) / (double)(dz * hcoef_at(nz, pz)));
+            wz[2] = (float)((az2 + az) / (double)(2 * dz * hcoef_at(nz, pz + 1)));
+            vx[0] = (float)((ax2 - ax) / 2);
+            vx[1] = (float)(-ax2 + 1);
+            vx[2] = (float)((ax2 + ax) / 2);
+            vz[0] = (float)((az2 - az) / 2);
+            vz[1] = (float)(-az2 + 1);
+            vz[2] = (float)((az2 + az) / 2);
+        }
+    }
+}
+
 void injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz, float dx, float dz,
                       float ox, float oz, int *xind, int *zind, float *xw, float *zw)
 {

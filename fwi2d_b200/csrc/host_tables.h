@@ -46,6 +46,10 @@ void acoustic_scale_divisors(int nx, int nz, float dx, float dz, float dt, const
 void analyze_model(int npar, float *model, int nx, int nz, float dx, float dz, int data_nt, float data_dt,
                    fwi2d_model_check &c);
 
+// dipole_m3::findIndicesWeights (injector.cpp:241-326).
+void dipole_weights(int ntr, const float *locx, const float *locz, const float *dip, float gl, int nx, int nz,
+                    float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw);
+
 void injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz, float dx, float dz,
                       float ox, float oz, int *xind, int *zind, float *xw, float *zw);
 

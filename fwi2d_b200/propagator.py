@@ -51,6 +51,19 @@ def injector_tables(itype, locx, locz, nx, nz, dx, dz, ox, oz):
     return xind, zind, xw, zw
 
 
+def dipole_tables(locx, locz, dip, gl, nx, nz, dx, dz, ox=0.0, oz=0.0):
+    """dipole_m3 tables (distributed acoustic sensing receivers, param.gl > 0)
+    computed by the library: xind, zind [ntr][6], xw, zw [ntr][2][6]."""
+    L = C.load()
+    locx, locz, dip = (np.ascontiguousarray(v, np.float32) for v in (locx, locz, dip))
+    n = len(locx)
+    xind, zind = np.zeros((n, 6), np.int32), np.zeros((n, 6), np.int32)
+    xw, zw = np.zeros((n, 2, 6), np.float32), np.zeros((n, 2, 6), np.float32)
+    C.check(L.fwi2d_dipole_weights(n, C.ptr(locx), C.ptr(locz), C.ptr(dip), float(gl), nx, nz, float(dx), float(dz),
+                                   float(ox), float(oz), C.ptr(xind), C.ptr(zind), C.ptr(xw), C.ptr(zw)))
+    return xind, zind, xw, zw
+
+
 def _injector(itype, tabs):
     if tabs is None:
         return C.Injector(0, 0, None, None, None, None)

@@ -46,6 +46,10 @@ extern "C" {
 /* injector types (src/include/injector.hpp:39, :69) */
 #define FWI2D_INJ_DELTA 0   /* delta_m3: 3x3 discrete delta */
 #define FWI2D_INJ_DDELTA 1  /* ddelta_m3: moment tensor */
+#define FWI2D_INJ_DIPOLE 2  /* dipole_m3 (injector.hpp:99-120): two 3x3 deltas gl apart along the dip, for
+                             * distributed acoustic sensing receivers (param.gl > 0); tables xind/zind
+                             * [ntr][6], xw/zw [ntr][2][6], end 1 in columns 0-2, end 2 in 3-5.
+                             * fwi2d_propagate only (elastic and VTI), as ext (forward) or inj (adjoint). */
 
 /* The fields of the reference's `param` (src/include/param.hpp:8-83) that the
  * propagation reads, plus the storage options of this library. */
@@ -119,6 +123,12 @@ int fwi2d_analyze_model(int npar, float *model, int nx, int nz, float dx, float 
 /* delta_m3 / ddelta_m3::findIndicesWeights (src/cpp/injector.cpp:3-64, 114-187). */
 int fwi2d_injector_weights(int type, int ntr, const float *locx, const float *locz, int nx, int nz,
                            float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw);
+
+/* dipole_m3::findIndicesWeights (src/cpp/injector.cpp:241-326): the tables of
+ * ntr dipoles centred at (locx, locz) with dip angles dip (radians) and gauge
+ * length gl (param.gl; param.rdip gives the angles, param.cpp). */
+int fwi2d_dipole_weights(int ntr, const float *locx, const float *locz, const float *dip, float gl, int nx, int nz,
+                         float dx, float dz, float ox, float oz, int *xind, int *zind, float *xw, float *zw);
 
 /* Context: one device, one stream, one model, one batch plan.  Calls on one
  * context must be serialised by the caller. */

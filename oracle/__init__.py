@@ -288,6 +288,33 @@ class Reference(_Lib):
         shape = [int(x) for x in n[:k]]
         return out[:int(np.prod(shape))].reshape(shape[::-1]).copy(), [(shape[i], o[i], d[i]) for i in range(k)]
 
+    def dipole_weights(self, x, z, dip, gl, nx, nz, dx, dz, ox=0.0, oz=0.0):
+        """dipole_m3 tables: xind, zind [ntr][6], xw, zw [ntr][2][6]."""
+        f = self.lib.ref_dipole_weights
+        vp = ctypes.c_void_p
+        f.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                      ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
+        x, z, dip = self.arr(x), self.arr(z), self.arr(dip)
+        n = len(x)
+        xi, zi = np.zeros((n, 6), np.int32), np.zeros((n, 6), np.int32)
+        xw, zw = np.zeros((n, 2, 6), self.dtype), np.zeros((n, 2, 6), self.dtype)
+        f(n, _ptr(x), _ptr(z), _ptr(dip), gl, nx, nz, dx, dz, ox, oz, _ptr(xi), _ptr(zi), _ptr(xw), _ptr(zw))
+        return xi, zi, xw, zw
+
+    def propagate_dipole(self, kind, adj, model, traces, out, par, nx, nz, d, src_loc, rx, rz, rdip, gl, full=None,
+                         grad=None):
+        """propagate with one delta source and dipole receivers (ref_propagate_dipole)."""
+        f = self.lib.ref_propagate_dipole
+        vp = ctypes.c_void_p
+        f.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, self._real(), self._real(), ctypes.c_int, vp, vp, vp,
+                      ctypes.c_double, vp, vp, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                      ctypes.c_double]
+        rx, rz, rdip = self.arr(rx), self.arr(rz), self.arr(rdip)
+        rc = f(kind, adj, _ptr(self.arr(model)), _ptr(self.arr(traces)), _ptr(out), src_loc[0], src_loc[1], len(rx),
+               _ptr(rx), _ptr(rz), _ptr(rdip), gl, _ptr(full), _ptr(grad), ctypes.byref(par), nx, nz, d, d)
+        if rc != 0:
+            raise RuntimeError("reference dipole propagate failed")
+
     def misfit_grad_rs(self, kind, par, nx, nz, d, nd, dd, prop_dt, method, hl, src_loc, rcv_locs, model_raw, src,
                        obs=None):
         """misfit_grad with sources and data on their own axis (nd samples at

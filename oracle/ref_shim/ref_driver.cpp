@@ -205,6 +205,53 @@ int ref_analyze_model(int npar, data_t *model, int nx, int nz, double dx, double
     return 0;
 }
 
+// dipole_m3 tables (injector.cpp:241-326) for ntr dipoles at (x, z) with dip
+// angles dip and gauge length gl.
+int ref_dipole_weights(int ntr, const data_t *x, const data_t *z, const data_t *dip, double gl, int nx, int nz,
+                       double dx, double dz, double ox, double oz, int *xind, int *zind, data_t *xw, data_t *zw)
+{
+    hypercube<data_t> g = grid(nx, nz, dx, dz, ox, oz);
+    std::vector<std::vector<data_t> > l(ntr);
+    for (int i = 0; i < ntr; i++) l[i] = {x[i], z[i], dip[i]};
+    dipole_m3 J(g, l, (data_t)gl);
+    std::memcpy(xind, J._xind.data(), J._xind.size() * sizeof(int));
+    std::memcpy(zind, J._zind.data(), J._zind.size() * sizeof(int));
+    std::memcpy(xw, J._xw.data(), J._xw.size() * sizeof(data_t));
+    std::memcpy(zw, J._zw.data(), J._zw.size() * sizeof(data_t));
+    return 0;
+}
+
+// nl_we_op_e / nl_we_op_vti::propagate (kind 0 / 1) with one delta source at
+// (sx, sz) and nr dipole receivers (dipole_m3, gauge gl, dip angles rdip) at
+// (rx, rz): the forward extracts into allrcv [2][nr][nt]; the adjoint (adj = 1)
+// injects allsrc [2][nr][nt] through the dipoles (allrcv then is the source's
+// [2][1][nt]) and images into grad.
+int ref_propagate_dipole(int kind, int adj, const data_t *model, const data_t *allsrc, data_t *allrcv,
+                         data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *rdip,
+                         double gl, data_t *full, data_t *grad, const ref_param *rp, int nx, int nz, double dx,
+                         double dz)
+{
+    try {
+        param par = to_param(rp);
+        par.gl = (data_t)gl;
+        hypercube<data_t> g = grid(nx, nz, dx, dz, 0, 0);
+        data_t sl[2] = {sx, sz};
+        injector *src = new delta_m3(g, locs(1, sl, sl + 1));
+        std::vector<std::vector<data_t> > l(nr);
+        for (int i = 0; i < nr; i++) l[i] = {rx[i], rz[i], rdip[i]};
+        injector *rcv = new dipole_m3(g, l, (data_t)gl);
+        injector *inj = adj ? rcv : src, *ext = adj ? src : rcv;
+        if (kind == 0) { nl_we_op_e op; op.propagate(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, 0, 0, 0); }
+        else { nl_we_op_vti op; op.propagate(adj != 0, model, allsrc, allrcv, inj, ext, full, grad, par, nx, nz, (data_t)dx, (data_t)dz, 0, 0, 0); }
+        delete src;
+        delete rcv;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_propagate_dipole: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
 // binWrite (IO.hpp:179-222): vals on ndim axes (axis 1 first: n, o, d) to
 // the header file `header` and its binary <datapath>/<header>@.
 int ref_bin_write(const char *header, const data_t *vals, int ndim, const int *n, const double *o, const double *d,

@@ -234,6 +234,34 @@ def analyze_case():
     return out
 
 
+def dipole_case():
+    """Dipole (DAS) receivers, dipole_m3 (injector.cpp:241-380), on the elastic
+    propagator: the reference's tables, its forward traces [2][nr][nt] with
+    snapshots, and its adjoint imaging condition for injected traces."""
+    lib = O.Reference(32)
+    kind, nx, nz, d, nt, gl = O.KIND_ELASTIC, 64, 56, 0.01, 160, 0.03
+    mc = K.converted(kind, K.model_case(kind, nx, nz, d, seed=13))
+    rng = np.random.default_rng(14)
+    nr = 10
+    rx = np.linspace(0.08, 0.55, nr).astype(np.float32)
+    rz = np.concatenate([np.full(5, 0.013), np.linspace(0.1, 0.45, 5)]).astype(np.float32)
+    rdip = rng.uniform(-np.pi, np.pi, nr).astype(np.float32)
+    rdip[0], rdip[5] = 0.0, np.float32(np.pi / 2)
+    xi, zi, xw, zw = lib.dipole_weights(rx, rz, rdip, gl, nx, nz, d, d)
+    sx, sz = np.float32(0.3), np.float32(0.02)
+    src = K.sources(2, nt, 1e-3)
+    par = O.make_par(**K.par_dict(nt=nt, dt=1e-3), ns=1, nr=nr)
+    rcv = np.zeros((2, nr, nt), np.float32)
+    full = np.zeros((nt + 1, 2, nx, nz), np.float32)
+    lib.propagate_dipole(kind, 0, mc, src, rcv, par, nx, nz, d, (sx, sz), rx, rz, rdip, gl, full=full)
+    adj = np.ascontiguousarray(rng.standard_normal((2, nr, nt)).astype(np.float32) * np.abs(rcv).max())
+    g = np.zeros((3, nx, nz), np.float32)
+    srcb = np.zeros((2, 1, nt), np.float32)
+    lib.propagate_dipole(kind, 1, mc, adj, srcb, par, nx, nz, d, (sx, sz), rx, rz, rdip, gl, full=full, grad=g)
+    return dict(kind=kind, nx=nx, nz=nz, d=d, nt=nt, gl=gl, model=mc, rx=rx, rz=rz, rdip=rdip, sx=sx, sz=sz, src=src,
+                xind=xi, zind=zi, xw=xw, zw=zw, rcv=rcv, adj=adj, grad=g)
+
+
 SEP_AXES = [(0.0, 0.005), (0.5, 0.005), (0.0, 1.0)]   # (o, d): z, x, parameter
 
 
@@ -299,6 +327,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "resample_f32.npz"), **resample_case())
     np.savez_compressed(os.path.join(HERE, "analyze_model_f32.npz"), **analyze_case())
     sep_case()
+    np.savez_compressed(os.path.join(HERE, "dipole_f32.npz"), **dipole_case())
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_elastic_resampled_f32.npz"), **fwi_case_resampled())
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_vti_resampled_f32.npz"),
                         **fwi_case_resampled(O.KIND_VTI, ("sinc",)))

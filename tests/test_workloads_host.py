@@ -78,3 +78,16 @@ def test_analyze_model_matches_reference():
         assert r["nt"] == int(ref["nt"]) and r["sub"] == int(ref["sub"]), name
         k += 1
     assert k == 8
+
+
+def test_dipole_tables_match_reference():
+    """fwi2d_dipole_weights reproduces dipole_m3::findIndicesWeights
+    (injector.cpp:241-326, tables written by the reference build), including
+    dipoles at the free-surface row and at horizontal and vertical dips."""
+    import os
+    from fwi2d_b200.propagator import dipole_tables
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "dipole_f32.npz")))
+    d = float(g["d"])
+    xi, zi, xw, zw = dipole_tables(g["rx"], g["rz"], g["rdip"], float(g["gl"]), int(g["nx"]), int(g["nz"]), d, d)
+    assert np.array_equal(xi, g["xind"]) and np.array_equal(zi, g["zind"])
+    assert np.array_equal(xw, g["xw"]) and np.array_equal(zw, g["zw"])
