@@ -340,15 +340,24 @@ class Reference(_Lib):
             raise RuntimeError("reference misfit/gradient with resampling failed")
         return syn, g
 
-    def misfit_grad_ae(self, par, nx, nz, d, oz, nt, dt, src_loc, rcv_x, rcv_z, rcv_zw, model_raw, src, obs=None):
+    def misfit_grad_ae(self, par, nx, nz, d, oz, nt, dt, src_loc, rcv_x, rcv_z, rcv_zw, model_raw, src, obs=None,
+                       resample=None):
         """Acoustic-elastic forward data [3][nr][nt] (fluid, x, z; seismotype 1)
         and, with obs, the solver's gradient (ref_misfit_grad_ae).  The model
-        grid's first row is at depth oz; the fluid layer lies above it."""
-        f = self.lib.ref_misfit_grad_ae
+        grid's first row is at depth oz; the fluid layer lies above it.
+        resample = (prop_dt, method): nt, dt are then the data axis and the
+        propagation runs at prop_dt (ref_misfit_grad_ae_rs)."""
         vp = ctypes.c_void_p
-        f.argtypes = [ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                      ctypes.c_double, ctypes.c_int, ctypes.c_double, self._real(), self._real(), ctypes.c_int,
-                      vp, vp, vp, vp, vp, vp, vp, vp]
+        args = [ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                ctypes.c_double, ctypes.c_int, ctypes.c_double]
+        if resample is None:
+            f = self.lib.ref_misfit_grad_ae
+            extra = ()
+        else:
+            f = self.lib.ref_misfit_grad_ae_rs
+            args += [ctypes.c_double, ctypes.c_int]
+            extra = (float(resample[0]), 1 if resample[1] == "linear" else 0)
+        f.argtypes = args + [self._real(), self._real(), ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
         rx, rz, rzw = self.arr(rcv_x), self.arr(rcv_z), self.arr(rcv_zw)
         nr = len(rx)
         m = self.arr(model_raw)
@@ -356,7 +365,7 @@ class Reference(_Lib):
         syn = np.zeros((3, nr, nt), self.dtype)
         o = None if obs is None else self.arr(obs)
         g = None if obs is None else np.zeros(m.shape, self.dtype)
-        rc = f(ctypes.byref(par), nx, nz, d, d, oz, nt, dt, src_loc[0], src_loc[1], nr, _ptr(rx), _ptr(rz),
+        rc = f(ctypes.byref(par), nx, nz, d, d, oz, nt, dt, *extra, src_loc[0], src_loc[1], nr, _ptr(rx), _ptr(rz),
                _ptr(rzw), _ptr(m), _ptr(s), _ptr(o), _ptr(syn), _ptr(g))
         if rc != 0:
             raise RuntimeError("reference acoustic-elastic misfit/gradient failed")

@@ -347,21 +347,22 @@ int ref_resample(int linear, int adjoint, int hl, int ntr, int nm, double dm, in
 // (sx, sz) (in the fluid when acoustic_source, its traces [1][nt], else on the
 // elastic grid, [2][nt]); nr receivers at (rx, rz) on the elastic grid and
 // (rx, rzw) in the fluid.  Data [3][nr][nt] (fluid, x, z), seismotype 1.
-int ref_misfit_grad_ae(const ref_param *rp, int nx, int nz, double dx, double dz, double oz, int nt, double dt,
-                       data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *rzw,
-                       const data_t *model, const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
+static int misfit_grad_ae(const ref_param *rp, int nx, int nz, double dx, double dz, double oz, int nt, double dt,
+                          double prop_dt, const char *resampling, data_t sx, data_t sz, int nr, const data_t *rx,
+                          const data_t *rz, const data_t *rzw, const data_t *model, const data_t *src,
+                          const data_t *obs, data_t *syn, data_t *grad)
 {
     try {
         param par = to_param(rp);
         par.nt = nt;
-        par.dt = (data_t)dt;
+        par.dt = (data_t)prop_dt;
         par.sub = obs ? 1 : 0;
         par.ns = 1;
         par.nr = nr;
         par.nmodels = 3;
         par.acoustic_elastic = true;
         par.seismotype = 1;
-        par.resampling = "linear";
+        par.resampling = resampling;
         data_t sl[2] = {sx, sz};
         par.sxz = locs(1, sl, sl + 1);
         par.rxz = {locs(nr, rx, rz)};
@@ -393,6 +394,26 @@ int ref_misfit_grad_ae(const ref_param *rp, int nx, int nz, double dx, double dz
         return -1;
     }
     return 0;
+}
+
+int ref_misfit_grad_ae(const ref_param *rp, int nx, int nz, double dx, double dz, double oz, int nt, double dt,
+                       data_t sx, data_t sz, int nr, const data_t *rx, const data_t *rz, const data_t *rzw,
+                       const data_t *model, const data_t *src, const data_t *obs, data_t *syn, data_t *grad)
+{
+    return misfit_grad_ae(rp, nx, nz, dx, dz, oz, nt, dt, dt, "linear", sx, sz, nr, rx, rz, rzw, model, src, obs, syn,
+                          grad);
+}
+
+// ref_misfit_grad_ae with sources and data on their own axis (nd samples at
+// dd), the propagation at prop_dt, and the sinc (linear = 0, half length 11)
+// or linear resampler, as ref_misfit_grad_rs.
+int ref_misfit_grad_ae_rs(const ref_param *rp, int nx, int nz, double dx, double dz, double oz, int nd, double dd,
+                          double prop_dt, int linear, data_t sx, data_t sz, int nr, const data_t *rx,
+                          const data_t *rz, const data_t *rzw, const data_t *model, const data_t *src,
+                          const data_t *obs, data_t *syn, data_t *grad)
+{
+    return misfit_grad_ae(rp, nx, nz, dx, dz, oz, nd, dd, prop_dt, linear ? "linear" : "sinc", sx, sz, nr, rx, rz, rzw,
+                          model, src, obs, syn, grad);
 }
 
 // kind: 0 elastic, 1 VTI, 2 acoustic, 3 acoustic-elastic.

@@ -313,6 +313,38 @@ def fwi_case_ae():
                 start=start, src=src, obs=obs, grad=g, misfit=0.5 * np.sum(w * r * r))
 
 
+def fwi_case_ae_resampled():
+    """fwi_case_ae with the source and data sampled at 2.5 ms, the propagation
+    at 1 ms and the sinc resampler (ref_misfit_grad_ae_rs)."""
+    lib = O.Reference(32)
+    nx, nz, d, dt, dd, nd = 90, 60, 0.01, 1e-3, 2.5e-3, 121
+    nt = 301
+    nza = 16
+    oz = (nza - 1) * d
+    true = K.model_case(O.KIND_ELASTIC, nx, nz, d, seed=17)
+    true[0] += 0.5
+    true[1] = true[0] / 1.8
+    start = true.copy()
+    from scipy.ndimage import gaussian_filter
+    for c in range(3):
+        start[c] = gaussian_filter(true[c].astype(np.float64), 4, mode="nearest").astype(np.float32)
+    sx, sz = np.float32(0.41 * nx * d), np.float32(0.05)
+    rx = np.linspace(3 * d, (nx - 4) * d, 24).astype(np.float32)
+    rz = np.full(24, oz + 0.02, np.float32)
+    rzw = np.full(24, 0.03, np.float32)
+    src = K.sources(1, nd, dd, f0=15.0).reshape(1, nd)
+    par = O.make_par(**K.par_dict(nt=nt, dt=dt, bc=(2, 2, 2, 2), taper=(4, 10, 10, 10)), ns=1, nr=24, nza=nza,
+                     acoustic_source=1)
+    rs = (dt, "sinc")
+    obs, _ = lib.misfit_grad_ae(par, nx, nz, d, oz, nd, dd, (sx, sz), rx, rz, rzw, true, src, resample=rs)
+    syn0, g = lib.misfit_grad_ae(par, nx, nz, d, oz, nd, dd, (sx, sz), rx, rz, rzw, start, src, obs, resample=rs)
+    w = np.full(nd, dd)
+    w[0] = w[-1] = 0.5 * dd
+    r = syn0.astype(np.float64) - obs
+    return dict(nx=nx, nz=nz, d=d, nt=nt, dt=dt, dd=dd, nd=nd, nza=nza, oz=oz, sx=sx, sz=sz, rx=rx, rz=rz, rzw=rzw,
+                true=true, start=start, src=src, obs_sinc=obs, grad_sinc=g, misfit_sinc=0.5 * np.sum(w * r * r))
+
+
 def main():
     if not O.have_reference(32):
         sys.exit("oracle/_ref is not built (oracle/build_ref.sh needs the reference tree)")
@@ -324,6 +356,7 @@ def main():
     for kind, name in ((O.KIND_ELASTIC, "elastic"), (O.KIND_VTI, "vti"), (O.KIND_ACOUSTIC, "acoustic")):
         np.savez_compressed(os.path.join(HERE, "fwi_gradient_%s_f32.npz" % name), **fwi_case(kind))
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_f32.npz"), **fwi_case_ae())
+    np.savez_compressed(os.path.join(HERE, "fwi_gradient_ae_resampled_f32.npz"), **fwi_case_ae_resampled())
     np.savez_compressed(os.path.join(HERE, "resample_f32.npz"), **resample_case())
     np.savez_compressed(os.path.join(HERE, "analyze_model_f32.npz"), **analyze_case())
     sep_case()

@@ -175,3 +175,31 @@ def test_ae_fwi_gradient_matches_reference_solver():
         err, np.mean(grad == g["grad"]), phi, float(g["misfit"])))
     assert err <= 1e-4
     assert abs(phi - float(g["misfit"])) <= 1e-5 * float(g["misfit"])
+
+
+def test_ae_fwi_gradient_resampled_matches_reference_solver():
+    """As above with the source and the data sampled at 2.5 ms and the
+    propagation at 1 ms (sinc resampler, fwi2d_set_data_axis): the fluid
+    traces' sign and the rate ratio on the data axis,
+    tests/golden/fwi_gradient_ae_resampled_f32.npz."""
+    from fwi2d_b200 import workloads as W
+    g = dict(np.load(os.path.join(GOLD, "fwi_gradient_ae_resampled_f32.npz")))
+    nx, nz, d, nt, dt, nza, oz = (int(g["nx"]), int(g["nz"]), float(g["d"]), int(g["nt"]), float(g["dt"]),
+                                  int(g["nza"]), float(g["oz"]))
+    nd, dd = int(g["nd"]), float(g["dd"])
+    assert F.prop_nt(nd, dd, dt) == nt
+    P = F.Propagator(0)
+    P.set_model(O.KIND_AE, W.convert(O.KIND_ELASTIC, g["start"]), d, d, 0.0, oz)
+    pd = K.par_dict(nt=nt, dt=dt, bc=(2, 2, 2, 2), taper=(4, 10, 10, 10), nza=nza, acoustic_source=1)
+    P.set_shots(F.make_params(**pd, tile_shape=3),
+                [F.ShotSpec(0, nx, nt, [0.0], [oz], g["rx"], g["rz"], water_src_x=[float(g["sx"])],
+                            water_src_z=[float(g["sz"])], water_rcv_x=g["rx"], water_rcv_z=g["rzw"])])
+    P.set_data_axis(dd, [nd], resampling="sinc")
+    grad, phi = P.fwi_gradient(W.convert(O.KIND_ELASTIC, g["start"]), [g["src"]], [g["obs_sinc"]], seismotype=1)
+    P.close()
+    err = K.rel_l2(grad, g["grad_sinc"])
+    mis = float(g["misfit_sinc"])
+    print("AE FWI gradient, resampled data: rel-L2 %.3e (bitwise %.4f), misfit %.9e vs %.9e" % (
+        err, np.mean(grad == g["grad_sinc"]), phi, mis))
+    assert err <= 1e-4
+    assert abs(phi - mis) <= 1e-5 * mis
