@@ -1262,9 +1262,10 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
     return n;
 }
 
-// Time `steps` forward steps of the current plan (fields zeroed, no output),
-// in milliseconds per step.
-static float time_forward_steps(fwi2d_ctx *ctx, int steps)
+// Time `steps` forward steps of the current plan from launch it0 (fields
+// zeroed, no output), in milliseconds per step.  Shots whose records end
+// before a launch return from it, as in a full pass.
+static float time_forward_steps(fwi2d_ctx *ctx, int steps, int it0 = 0)
 {
     Plan &P = *ctx->plan;
     for (auto &S : P.shots) {
@@ -1273,13 +1274,14 @@ static float time_forward_steps(fwi2d_ctx *ctx, int steps)
     }
     const ModelDev md = ctx->M.dev();
     const ShotDev *shots = P.d_shots_f.as<ShotDev>();
-    const int nsteps = std::min(steps, P.nt_max - 1);
-    for (int it = 0; it < std::min(3, nsteps); it++) launch_step(ctx, P, shots, md, it, STEP_EXTRACT, ctx->st);
+    const int nsteps = std::max(0, std::min(steps, P.nt_max - 1 - it0));
+    for (int it = it0; it < it0 + std::min(3, nsteps); it++)
+        launch_step(ctx, P, shots, md, it, STEP_EXTRACT, ctx->st);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     CK(cudaEventRecord(a, ctx->st));
-    for (int it = 0; it < nsteps; it++) launch_step(ctx, P, shots, md, it, STEP_EXTRACT, ctx->st);
+    for (int it = it0; it < it0 + nsteps; it++) launch_step(ctx, P, shots, md, it, STEP_EXTRACT, ctx->st);
     CK(cudaEventRecord(b, ctx->st));
     CK(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -1389,10 +1391,41 @@ static void tune_file_store(const std::string &key, int shape)
 }
 
 // Tile-shape autotuner: for plans that leave the shape open (tile_shape < 0),
-// time a few forward steps of every shape that tiles the grids -- plus as
-// many adjoint steps with the imaging condition for plans that keep
-// snapshots (gradients) -- and keep the fastest.  The choice is cached per
-// (kind, nz, snapshots, shot grid widths).
+// time forward steps of every shape that tiles the grids -- plus adjoint
+// steps with the imaging condition for plans that keep snapshots (gradients)
+// -- and keep the fastest.  The forward is sampled in kTuneWindows windows
+// centred on equal parts of the whole time loop, so that a batch whose
+// shorter records end early is judged on its emptier late steps too (there,
+// units fewer than a wave favour narrower shapes); the adjoint, timed with
+// every shot active, is scaled by the ratio of the sampled loop to the
+// all-active forward steps.  The choice is cached per (kind, nz, snapshots,
+// shot grid widths).
+constexpr int kTuneWindows = 8, kTuneWindowSteps = 8;
+// Gradient plans: the shapes whose sampled score lies within kTuneClose of the
+// best are then timed over one whole forward pass with snapshots and one
+// adjoint pass, through the plan's own CUDA graphs (the sampled steps run as
+// plain stream launches and miss part of the tail's cost).
+constexpr float kTuneClose = 1.04f;
+
+static void run(fwi2d_ctx *ctx, bool adjoint, bool store);
+
+// One whole forward pass with snapshots and one adjoint pass of the current
+// plan on zero traces, in milliseconds (the plan's graphs, CUDA events).
+static float time_full_pass(fwi2d_ctx *ctx)
+{
+    Plan &P = *ctx->plan;
+    for (auto &S : P.shots) {
+        CK(cudaMemsetAsync(S->src_f.p, 0, S->src_f.n, ctx->st));
+        CK(cudaMemsetAsync(S->src_a.p, 0, S->src_a.n, ctx->st));
+    }
+    run(ctx, false, true);
+    run(ctx, true, false);
+    CK(cudaStreamSynchronize(ctx->st));
+    float f = 0.f, a = 0.f;
+    CK(cudaEventElapsedTime(&f, P.ev[0][0], P.ev[0][1]));
+    CK(cudaEventElapsedTime(&a, P.ev[1][0], P.ev[1][1]));
+    return f + a;
+}
 static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
 {
     REQ(par != nullptr && shots != nullptr && nshots > 0, "no shots");
@@ -1418,6 +1451,7 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
         }
         if (chosen < 0 && cells >= 20000000LL) {
             float best = 1e30f;
+            std::vector<std::pair<float, int>> scored;
             for (int s = 0; s < shape_count(); s++) {
                 fwi2d_params q = p;
                 q.tile_shape = s;
@@ -1429,14 +1463,55 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
                     if (e.code == FWI2D_ERR_ARG) continue;   // shape does not tile these grids
                     throw;
                 }
-                float ms = time_forward_steps(ctx, 30);
-                if (grad) ms += time_adjoint_steps(ctx, 30);
+                const int ntm = ctx->plan->nt_max;
+                float ms;
+                if (ntm - 1 >= 2 * kTuneWindows * kTuneWindowSteps) {
+                    // all shots active in the first steps: the reference for the adjoint's scaling
+                    const float first = time_forward_steps(ctx, kTuneWindowSteps, 0);
+                    float all = 0.f;
+                    for (int w = 0; w < kTuneWindows; w++) {
+                        const int it0 = (int)(((long long)(2 * w + 1) * (ntm - 1)) / (2 * kTuneWindows));
+                        all += time_forward_steps(ctx, kTuneWindowSteps, it0) / kTuneWindows;
+                    }
+                    ms = all;
+                    const float adj = grad ? time_adjoint_steps(ctx, 30) : 0.f;
+                    if (grad) ms += adj * (first > 0.f ? all / first : 1.f);
+                    if (std::getenv("FWI2D_TUNE_VERBOSE"))
+                        std::fprintf(stderr, "fwi2d autotune: shape %d forward %.4f ms/step (all active %.4f), "
+                                     "adjoint %.4f ms/step, score %.4f\n", s, all, first, adj, ms);
+                } else {
+                    ms = time_forward_steps(ctx, 30);
+                    if (grad) ms += time_adjoint_steps(ctx, 30);
+                    if (std::getenv("FWI2D_TUNE_VERBOSE"))
+                        std::fprintf(stderr, "fwi2d autotune: shape %d score %.4f ms/step\n", s, ms);
+                }
+                scored.emplace_back(ms, s);
                 if (ms < best) {
                     best = ms;
                     chosen = s;
                 }
             }
             ctx->plan.reset();
+            int close = 0;
+            for (auto &sc : scored) close += sc.first <= kTuneClose * best;
+            if (grad && close > 1) {
+                float bestf = 1e30f;
+                for (auto &sc : scored) {
+                    if (sc.first > kTuneClose * best) continue;
+                    fwi2d_params q = p;
+                    q.tile_shape = sc.second;
+                    set_shots_impl(ctx, &q, nshots, shots);
+                    const float t = time_full_pass(ctx);
+                    ctx->plan.reset();   // before the next plan allocates its snapshots
+                    if (std::getenv("FWI2D_TUNE_VERBOSE"))
+                        std::fprintf(stderr, "fwi2d autotune: shape %d whole forward + adjoint %.1f ms\n", sc.second,
+                                     t);
+                    if (t < bestf) {
+                        bestf = t;
+                        chosen = sc.second;
+                    }
+                }
+            }
             if (chosen >= 0) {
                 cache.emplace_back(key, chosen);
                 tune_file_store(key, chosen);
