@@ -16,7 +16,11 @@ FP16 snapshots, all shots in one plan, timed the same way.  It also carries
 sm_100a into oracle/_ref by oracle/build_ref.sh) timed on a bounded sample of
 the same shot, with "e2e_speedup" = this library's end-to-end value over it.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config single|batch]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config single|batch|large]
+
+--config large: one shot of the large-grid workload (1201 x 4001 at 2.5 m,
+nt = 16001), FP16 snapshots rebuilt by checkpoint-and-recompute every 200
+steps; its adjoint loop time includes the replay of the forward segments.
 
 N > 1 runs one process per GPU (torchrun); each rank computes its own shot
 (weak scaling) and the model gradient is summed over ranks with NCCL.
@@ -46,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="single", choices=["single", "batch"])
+    ap.add_argument("--config", default="single", choices=["single", "batch", "large"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
@@ -134,6 +138,12 @@ def build_workload(name, rank, world):
             sh = dict(wl["shots"][0])
             sh["sx"] = [2.0 + 0.06 * rank]
             wl["shots"] = [sh]
+    elif name == "large":
+        wl = W.elastic_large()
+        if world > 1:   # one shot per rank, sources 100 m apart
+            sh = dict(wl["shots"][0])
+            sh["sx"] = [5.0 + 0.1 * rank]
+            wl["shots"] = [sh]
     else:
         wl = W.vti_batch()
         if world > 1:
@@ -165,6 +175,7 @@ def observed(wl, device, srcs):
     shots = [F.ShotSpec(s["x0"], s["nx"], s["nt"], s["sx"], s["sz"], s["rx"], s["rz"]) for s in wl["shots"]]
     prm = dict(wl["params"])
     prm["sub"] = 0
+    prm["checkpoint_every"] = 0
     P.set_shots(F.make_params(**prm), shots)
     out = P.forward(srcs, store=False)
     P.close()
@@ -288,6 +299,9 @@ def run_reference(args):
 def workload_name(cfg):
     if cfg == "single":
         return "elastic isotropic FWI gradient, 1 shot, 401x801 grid at 5 m, nt=5001, 400 2-C receivers, FP32 snapshots"
+    if cfg == "large":
+        return ("elastic isotropic FWI gradient, 1 shot, 1201x4001 grid at 2.5 m, nt=16001, 798 2-C receivers, "
+                "FP16 snapshots rebuilt by checkpoint-and-recompute every 200 steps")
     return "VTI FWI gradient, 64 shots on cropped grids (1.0-3.5 km apertures, 1.2-2.0 s records), 401x801 at 5 m"
 
 
@@ -400,7 +414,8 @@ def run_ours(args):
     cells_launch = sum(s["nx"] * wl["nz"] for s in wl["shots"])
     adj_launch_s = adj_ms / 1e3 / steps_adj
     fwd_launch_s = fwd_ms / 1e3 / steps_adj
-    achieved = BYTES_ADJ * cells_launch / adj_launch_s / 1e9
+    bytes_adj = BYTES_ADJ - (4 if wl["params"].get("snapshot_precision", 0) else 0)   # 16-bit snapshot read
+    achieved = bytes_adj * cells_launch / adj_launch_s / 1e9
     peak, peak_kind = peaks()
     launches = (info["launches_forward"] + info["launches_adjoint"] + 2 * nshots_rank + 1) * args.steps
     if rank == 0:
@@ -412,7 +427,9 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "shots_per_s": shots_s,
             "config": {"workload": workload_name(args.config), "nx": wl["nx"], "nz": wl["nz"], "nt": wl["nt"],
-                       "shots_per_gpu": nshots_rank, "snapshots": "fp32 every step, in HBM",
+                       "shots_per_gpu": nshots_rank,
+                       "snapshots": ("fp16, checkpoint-and-recompute every 200 steps (the adjoint loop includes the "
+                                     "replay)" if args.config == "large" else "fp32 every step, in HBM"),
                        "cell_updates_per_step": total_cells, "tile_shape": info["tile_shape"],
                        "l2": "inputs larger than L2: %.1f GB of snapshots written and read per step"
                              % (info["snapshot_bytes"] / 1e9),
@@ -421,10 +438,12 @@ def run_ours(args):
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "shots_per_s": total_shots / (e2e_ms / 1e3)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "elastic_step (adjoint + imaging)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": ("elastic_step (adjoint + imaging)" if args.config == "single" else
+                                                    "adjoint loop: marching, band and imaging kernels"),
+                         "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": ADJ_TILE_TRAFFIC_BYTES if args.config == "single" else None,
-                         "algorithmic_bytes_per_launch": BYTES_ADJ * cells_launch,
+                         "algorithmic_bytes_per_launch": bytes_adj * cells_launch,
                          "launch_ms": adj_launch_s * 1e3,
                          "forward_launch_ms": fwd_launch_s * 1e3,
                          "forward_achieved": BYTES_FWD * cells_launch / fwd_launch_s / 1e9},

@@ -35,11 +35,12 @@ def _smooth(rng_field, sigma):
     return gaussian_filter(rng_field, sigma, mode="nearest")
 
 
-def elastic_model(nx=801, nz=401, d=0.005, seed=0):
-    """Raw (vp, vs, rho) of the true model."""
+def elastic_model(nx=801, nz=401, d=0.005, seed=0, sigma_cells=10):
+    """Raw (vp, vs, rho) of the true model: the perturbation is smoothed with a
+    Gaussian of sigma_cells cells (50 m on the 5 m grid)."""
     rng = np.random.default_rng(seed)
     z = np.arange(nz) * d
-    p = _smooth(rng.uniform(-1, 1, (nx, nz)), 10)
+    p = _smooth(rng.uniform(-1, 1, (nx, nz)), sigma_cells)
     p *= 0.05 / np.abs(p).max()
     vp = (2.0 + 0.75 * z)[None, :] * (1 + p)
     vs = vp / 1.73
@@ -98,6 +99,28 @@ def elastic_single(nt=5001):
                   taper_left=60, taper_right=60, taper_strength=0.05)
     return dict(kind=C.ELASTIC, nx=nx, nz=nz, d=d, dt=dt, nt=nt, true=true, start=start, src=src,
                 shots=[dict(x0=0, nx=nx, sx=[2.0], sz=[0.01], rx=rx, rz=rz, nt=nt)], params=params, seismotype=1)
+
+
+def elastic_large(nt=16001, checkpoint_every=200, snapshot_precision=C.SNAP_FP16):
+    """Large-grid elastic gradient workload: 1201 x 4001 cells at 2.5 m, Ricker
+    15 Hz, dt = 0.2 ms, nt = 16001, one shot at x = 5 km with 798 two-component
+    receivers every 12.5 m at 10 m depth.  The perturbation of the true model
+    is smoothed over 50 m (20 cells), the starting model over 125 m (50 cells).
+    Snapshots are 16-bit, rebuilt by checkpoint-and-recompute every 200 steps
+    (the FP32 snapshots of one shot would take 615 GB)."""
+    nx, nz, d, dt = 4001, 1201, 0.0025, 2e-4
+    true = elastic_model(nx, nz, d, sigma_cells=20)
+    start = smoothed(true, 50)
+    w = ricker(nt, dt, 15.0, 0.1)
+    ang = np.float32(1.5708)
+    src = np.stack([w * np.float32(np.cos(ang)), w * np.float32(np.sin(ang))])[:, None, :].astype(np.float32)
+    rx = (0.0125 * (1 + np.arange(798))).astype(np.float32)
+    rz = np.full(798, 0.01, np.float32)
+    params = dict(nt=nt, sub=1, dt=dt, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2, taper_top=0, taper_bottom=60,
+                  taper_left=60, taper_right=60, taper_strength=0.05, checkpoint_every=checkpoint_every,
+                  snapshot_precision=snapshot_precision)
+    return dict(kind=C.ELASTIC, nx=nx, nz=nz, d=d, dt=dt, nt=nt, true=true, start=start, src=src,
+                shots=[dict(x0=0, nx=nx, sx=[5.0], sz=[0.01], rx=rx, rz=rz, nt=nt)], params=params, seismotype=1)
 
 
 def batch_geometry(nshots=64, nt_max=5001, seed=2, nx=801, d=0.005, dt=4e-4):
