@@ -1404,8 +1404,16 @@ constexpr int kTuneWindows = 8, kTuneWindowSteps = 8;
 // Gradient plans: the shapes whose sampled score lies within kTuneClose of the
 // best are then timed over one whole forward pass with snapshots and one
 // adjoint pass, through the plan's own CUDA graphs (the sampled steps run as
-// plain stream launches and miss part of the tail's cost).
+// plain stream launches and miss part of the tail's cost).  The environment
+// variable FWI2D_TUNE_CLOSE overrides the ratio (e.g. 100 to time every shape).
 constexpr float kTuneClose = 1.04f;
+
+static float tune_close()
+{
+    const char *v = std::getenv("FWI2D_TUNE_CLOSE");
+    const float r = v ? (float)std::atof(v) : 0.f;
+    return r >= 1.f ? r : kTuneClose;
+}
 
 static void run(fwi2d_ctx *ctx, bool adjoint, bool store);
 
@@ -1492,12 +1500,13 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
                 }
             }
             ctx->plan.reset();
+            const float ratio = tune_close();
             int close = 0;
-            for (auto &sc : scored) close += sc.first <= kTuneClose * best;
+            for (auto &sc : scored) close += sc.first <= ratio * best;
             if (grad && close > 1) {
                 float bestf = 1e30f;
                 for (auto &sc : scored) {
-                    if (sc.first > kTuneClose * best) continue;
+                    if (sc.first > ratio * best) continue;
                     fwi2d_params q = p;
                     q.tile_shape = sc.second;
                     set_shots_impl(ctx, &q, nshots, shots);
