@@ -10,6 +10,7 @@ ELASTIC, VTI, ACOUSTIC, ACOUSTIC_ELASTIC = 0, 1, 2, 3
 SNAP_FP32, SNAP_BF16, SNAP_FP16 = 0, 1, 2
 INJ_DELTA, INJ_DDELTA, INJ_DIPOLE = 0, 1, 2
 
+ERR_ARG, ERR_CUDA, ERR_OOM, ERR_STATE, ERR_UNSUPPORTED, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "bad state",
           -5: "unsupported", -6: "timeout"}
 

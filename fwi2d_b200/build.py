@@ -19,9 +19,8 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-    "-shared",
 ]
-
+OBJDIR = os.path.join(HERE, "_build")
 
 def nvcc():
     cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
@@ -40,10 +39,24 @@ def stale():
 
 
 def build(force=False, verbose=False):
+    """Compile every translation unit to an object in parallel (they share no
+    device symbols), then link the shared library."""
     if not force and not stale():
         return LIB
-    srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + srcs
+    os.makedirs(OBJDIR, exist_ok=True)
+    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    objs, procs = [], []
+    for s in srcs:
+        o = os.path.join(OBJDIR, os.path.splitext(s)[0] + ".o")
+        cmd = [nvcc()] + NVCC_FLAGS + ["-c", "-o", o, os.path.join(CSRC, s)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((s, subprocess.Popen(cmd, cwd=CSRC)))
+        objs.append(o)
+    failed = [s for s, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc " + " ".join(failed))
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp"] + objs
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=CSRC)

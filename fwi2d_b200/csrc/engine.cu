@@ -290,8 +290,13 @@ struct Plan {
     bool timed[2] = {false, false};
     long long launches[3] = {0, 0, 0};
     long long snap_bytes = 0;
+    // device status word of the bounded waits (launch_take_timeout after each
+    // pass) and its pinned host copy, read after the pass has finished
+    DevBuf d_status;
+    int *h_status = nullptr;
     ~Plan()
     {
+        if (h_status) cudaFreeHost(h_status);
         for (auto &g : graph)
             if (g) cudaGraphExecDestroy(g);
         for (auto &a : ev)
@@ -723,6 +728,13 @@ static StepConst make_const(const fwi2d_params &p, float dx, float dz)
     C.sub = p.sub > 0 ? p.sub : 1;
     C.snap_prec = p.snapshot_precision;
     C.kahan = p.compensated;
+    // poll limit of the marching kernel's bounded waits: FWI2D_SPIN_LIMIT
+    // (read when a plan is built) or 2^20 polls
+    C.spin = 1 << 20;
+    if (const char *e = std::getenv("FWI2D_SPIN_LIMIT")) {
+        const long v = std::strtol(e, nullptr, 10);
+        if (v >= 0 && v <= (1L << 30)) C.spin = (int)v;
+    }
     return C;
 }
 
@@ -1212,8 +1224,38 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     build_init_cells(M, *P);
     upload_init_cells(*P, ctx->st);
     P->d_grad_full.alloc((size_t)P->ncompg * M.nx * M.ldz * sizeof(float));
+    P->d_status.alloc(sizeof(int));
+    CK(cudaMemsetAsync(P->d_status.p, 0, sizeof(int), ctx->st));
+    CK(cudaMallocHost((void **)&P->h_status, sizeof(int)));
+    *P->h_status = 0;
     CK(cudaStreamSynchronize(ctx->st));
     ctx->plan = std::move(P);
+}
+
+// After a pass has finished (its stream synchronised): a bounded device wait
+// that gave up during it makes the pass's results invalid.  Clears the status
+// and reports FWI2D_ERR_TIMEOUT.
+static void check_timeout(fwi2d_ctx *ctx)
+{
+    if (!ctx->plan || !ctx->plan->h_status) return;
+    Plan &P = *ctx->plan;
+    const int v = *P.h_status;
+    if (v == 0) return;
+    *P.h_status = 0;
+    CK(cudaMemsetAsync(P.d_status.p, 0, sizeof(int), ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    P.snapshots_valid = false;
+    throw Error(FWI2D_ERR_TIMEOUT, "a bounded device wait of the marching kernel gave up (row " +
+                                       std::to_string(v - 1) + "); the results of this pass are invalid");
+}
+
+// Queue the move of the device timeout flag into the plan's status word and
+// its copy to the host (read by check_timeout once the stream has finished).
+static void queue_timeout_check(fwi2d_ctx *ctx, Plan &P)
+{
+    launch_take_timeout(P.d_status.as<int>(), ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(P.h_status, P.d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
 }
 
 // One time step of every shot.  Tile-only plans: one launch.  Marching
@@ -1754,6 +1796,7 @@ static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
     CK(cudaGraphLaunch(P.graph[mode], ctx->st));
     CK(cudaEventRecord(P.ev[e][1], ctx->st));
     P.timed[e] = true;
+    queue_timeout_check(ctx, P);
     if (adjoint) {
         CK(cudaMemsetAsync(P.d_grad_full.p, 0, P.d_grad_full.n, ctx->st));
         for (auto &S : P.shots)
@@ -1780,6 +1823,7 @@ static void download_rcv(fwi2d_ctx *ctx, float *rcv)
         CK(cudaStreamSynchronize(ctx->st));
         p += n;
     }
+    check_timeout(ctx);
 }
 
 static void download_grad(fwi2d_ctx *ctx, float *grad)
@@ -1793,6 +1837,7 @@ static void download_grad(fwi2d_ctx *ctx, float *grad)
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, P.d_stage.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    check_timeout(ctx);
 }
 
 
@@ -2089,6 +2134,7 @@ static double read_misfit(fwi2d_ctx *ctx)
     std::vector<double> m(rows_total);
     CK(cudaMemcpyAsync(m.data(), P.d_misfit.p, rows_total * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    check_timeout(ctx);
     double f = 0.0;
     for (double v : m) f += v;
     return 0.5 * (double)(P.dd > 0.f ? P.dd : P.par.dt) * f;
@@ -2308,6 +2354,7 @@ int fwi2d_sync(fwi2d_ctx *ctx)
     REQ(ctx, "null context");
     set_device(ctx);
     CK(cudaStreamSynchronize(ctx->st));
+    check_timeout(ctx);
     ABI_END
 }
 

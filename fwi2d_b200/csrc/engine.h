@@ -102,6 +102,7 @@ struct StepConst {
     int snap_prec;
     int nslot;
     int kahan;                   // compensated gradient accumulation
+    int spin;                    // poll limit of each bounded device wait (marching kernel)
 };
 
 // Work unit of the tile kernel: a TX x TZ window of one shot grid starting

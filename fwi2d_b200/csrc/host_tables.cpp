@@ -50,8 +50,17 @@ void taper_factors(int nx, int nz, int t_top, int t_bottom, int t_left, int t_ri
                    bool use_top, bool use_bottom, bool use_left, bool use_right,
                    std::vector<float> &tz, std::vector<float> &tx)
 {
-    tz.assign(nz, 1.f);
-    tx.assign(nx, 1.f);
+    tz.resize(nz);
+    tx.resize(nx);
+    taper_factors_into(nx, nz, t_top, t_bottom, t_left, t_right, a, use_top, use_bottom, use_left, use_right,
+                       tz.data(), tx.data());
+}
+
+void taper_factors_into(int nx, int nz, int t_top, int t_bottom, int t_left, int t_right, float a,
+                        bool use_top, bool use_bottom, bool use_left, bool use_right, float *tz, float *tx)
+{
+    std::fill(tz, tz + nz, 1.f);
+    std::fill(tx, tx + nx, 1.f);
     const float pi = (float)M_PI, half = 0.5f;
     if (use_top && t_top > 0) {
         const int istart = t_top, iend = 0;
@@ -91,8 +100,16 @@ void elastic_scale_divisors(int nx, int nz, float dx, float dz, float dt, const 
                             const float *rho, const float *eps, long long ld, bool top, bool bottom, bool left,
                             bool right, std::vector<float> &den)
 {
+    den.resize(2 * (2 * nx + 2 * nz));
+    elastic_scale_divisors_into(nx, nz, dx, dz, dt, lam, mu, rho, eps, ld, top, bottom, left, right, den.data());
+}
+
+void elastic_scale_divisors_into(int nx, int nz, float dx, float dz, float dt, const float *lam, const float *mu,
+                                 const float *rho, const float *eps, long long ld, bool top, bool bottom, bool left,
+                                 bool right, float *den)
+{
     const int per = 2 * nx + 2 * nz;
-    den.assign(2 * per, 1.f);
+    std::fill(den, den + 2 * per, 1.f);
     auto T = [&](int ix) -> float * { return &den[ix]; };
     auto B = [&](int ix) -> float * { return &den[nx + ix]; };
     auto L = [&](int iz) -> float * { return &den[2 * nx + iz]; };

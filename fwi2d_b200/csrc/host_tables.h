@@ -29,6 +29,9 @@ const SbpTables &sbp_tables();
 void taper_factors(int nx, int nz, int t_top, int t_bottom, int t_left, int t_right, float strength,
                    bool use_top, bool use_bottom, bool use_left, bool use_right,
                    std::vector<float> &tz, std::vector<float> &tx);
+// The same into caller arrays tz[nz], tx[nx] (no allocation).
+void taper_factors_into(int nx, int nz, int t_top, int t_bottom, int t_left, int t_right, float strength,
+                        bool use_top, bool use_bottom, bool use_left, bool use_right, float *tz, float *tx);
 
 // Divisors of the implicit absorbing scaling at every boundary sample, laid out
 // [ncomp][top nx | bottom nx | left nz | right nz]; 1 where nothing divides.
@@ -37,6 +40,10 @@ void taper_factors(int nx, int nz, int t_top, int t_bottom, int t_left, int t_ri
 void elastic_scale_divisors(int nx, int nz, float dx, float dz, float dt, const float *lam, const float *mu,
                             const float *rho, const float *eps, long long ld, bool top, bool bottom, bool left,
                             bool right, std::vector<float> &den);
+// The same into a caller array den[2 * (2*nx + 2*nz)] (no allocation).
+void elastic_scale_divisors_into(int nx, int nz, float dx, float dz, float dt, const float *lam, const float *mu,
+                                 const float *rho, const float *eps, long long ld, bool top, bool bottom, bool left,
+                                 bool right, float *den);
 void acoustic_scale_divisors(int nx, int nz, float dx, float dz, float dt, const float *K, const float *irho,
                              long long ld, bool top, bool bottom, bool left, bool right, std::vector<float> &den);
 

@@ -1157,4 +1157,17 @@ void launch_vti_grad_coefs(int n, const float *lam, const float *mu, const float
     vti_grad_coefs<<<296, 256, 0, st>>>(n, lam, mu, c13, v2, v3);
 }
 
+// Moves the marching kernel's timeout flag into *status (keeping the first
+// row recorded) and clears the flag, in stream order.
+__global__ void take_timeout(int *status)
+{
+    const int v = g_march_timeout;
+    if (v != 0) {
+        if (*status == 0) *status = v;
+        g_march_timeout = 0;
+    }
+}
+
+void launch_take_timeout(int *status, cudaStream_t st) { take_timeout<<<1, 1, 0, st>>>(status); }
+
 }  // namespace fwi2d

@@ -43,6 +43,9 @@ void launch_ae_couple(const ShotDev *elastic, const ShotDev *fluid, int nshots, 
                       const StepConst &C, int it, int flags, float dtg, float Kw, float val0, int sign, cudaStream_t st);
 void launch_acoustic_final_grad(const ShotDev *shots, int nshots, const ModelDev &M, const StepConst &C, float dtg,
                                 cudaStream_t st);
+// Move the marching kernel's timeout flag (the row + 1 where a bounded wait
+// gave up, 0 if none) into *status unless it already holds one, and clear it.
+void launch_take_timeout(int *status, cudaStream_t st);
 
 // layout helpers (engine.cu)
 void launch_to_time_major(const float *in, float *out, int rows, int nt, cudaStream_t st);

@@ -47,8 +47,14 @@
 namespace fwi2d {
 
 // Set (to the row where it happened + 1) when a bounded wait of the marching
-// kernel gives up; read and cleared by the host after each run.
+// kernel gives up.  After every forward or adjoint pass the engine moves it
+// into the plan's status word and clears it (launch_take_timeout); the host
+// then returns FWI2D_ERR_TIMEOUT for that pass.
 __device__ int g_march_timeout;
+
+// Iterations of the bounded wait for the copies in flight when a CTA leaves
+// after a timeout (independent of the step-wait limit StepConst::spin).
+#define MARCH_DRAIN_LIMIT (1 << 22)
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -82,10 +88,11 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
     return ok != 0;
 }
 
-// Bounded wait for a phase of an mbarrier; false when the limit was reached.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+// Bounded wait for a phase of an mbarrier; false when `limit` polls found it
+// still incomplete.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int limit)
 {
-    for (int k = 0; k < (1 << 20); k++)
+    for (int k = 0; k < limit; k++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -130,6 +137,9 @@ struct MarchCtx {
     long long slot_elems;
     float *grad;
     unsigned ph[2];           // mbarrier phase parity per stage
+    int spin;                 // poll limit of the per-step wait
+    int tmo_bar;              // after a timeout: the stage whose copies may be in flight, and its parity
+    unsigned tmo_par;
 };
 
 // Register queues along x.  UNR = 8: ring of 8 slots, row j+d of phase PH at
@@ -311,7 +321,9 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD, UNR> &Q, MarchCtx &X, fl
     // ---- wait for the copies issued at the previous step, then the step barrier
     bool tmo = false;
     if (j > j0) {
-        tmo = !mbar_wait(bars + (P & 1), X.ph[P & 1]);
+        tmo = !mbar_wait(bars + (P & 1), X.ph[P & 1], X.spin);
+        X.tmo_bar = P & 1;
+        X.tmo_par = X.ph[P & 1];
         X.ph[P & 1] ^= 1u;
     }
     if (__syncthreads_or(tmo)) {
@@ -588,6 +600,9 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
     X.slot_elems = S.snap_slot;
     X.grad = S.grad;
     X.ph[0] = X.ph[1] = 0u;
+    X.spin = C.spin;
+    X.tmo_bar = 0;
+    X.tmo_par = 0u;
 
     constexpr int UNR = GRAD ? MARCH_GRAD_UNROLL : MARCH_FWD_UNROLL;
     MarchQ<GRAD, UNR> Q;
@@ -611,9 +626,10 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
 #undef MARCH_PHASE
     }
     if (!ok) {
-        // a copy stage may still be in flight: give it a bounded wait before the
-        // shared memory is released
-        for (int s = 0; s < 2; s++) mbar_wait(bars + s, X.ph[s]);
+        // the copies of the stage that timed out may still be in flight: give
+        // them a bounded wait before the shared memory is released (no copy
+        // was issued after that wait)
+        mbar_wait(bars + X.tmo_bar, X.tmo_par, MARCH_DRAIN_LIMIT);
         return;
     }
 

@@ -9,8 +9,8 @@
 // propagation -- the pitched model, the two wavefield buffers, the time-major
 // traces and the injection / extraction / boundary tables -- in one
 // file-scope static __device__ array of FWI2D_NOALLOC_SCRATCH_BYTES (64 MiB),
-// and its host-side tables in fixed-size static host arrays.  Every GPU that
-// loads the library holds the 64 MiB until the process exits.
+// and its host-side tables in fixed-size static host arrays.  A GPU holds
+// the 64 MiB from the first call on it until the process exits.
 //
 // Contract:
 // * inputs and outputs are host buffers with the reference's propagate
@@ -19,14 +19,23 @@
 // * the problem must fit the scratch array and the static tables (at most
 //   FWI2D_NOALLOC_MAX_* of each); larger ones are rejected with
 //   FWI2D_ERR_ARG and a message naming the limit;
-// * all calls share the scratch array, which keeps the last call's contents;
-//   everything that must start at zero is cleared at the start of each call;
-// * calls are serialised on the host by a mutex; calls that overlap on the
-//   GPU (from other processes sharing the module, or work this call does not
-//   order against) race on the scratch array;
-// * the first call on a device looks up the device address of the scratch
-//   array (cudaGetSymbolAddress) with that device current.  Make that first
-//   call before any stream capture on the device.
+// * all calls in a process share the scratch array of the current device,
+//   which keeps the last call's contents; everything that must start at zero
+//   is cleared at the start of each call;
+// * every call runs on the legacy default stream (stream 0), not on a stream
+//   given to fwi2d_set_stream, so it waits for, and holds up, the work of
+//   every blocking stream on the device; it returns only after its GPU work
+//   has finished;
+// * calls that overlapped on the GPU would race on the shared array; a host
+//   mutex serialises the calls of a process and each call finishes its GPU
+//   work before it returns, so they never overlap.  Each process (each CUDA
+//   context) has its own copy of the array: other processes do not share it;
+// * the CUDA runtime loads the module that holds the array lazily (the
+//   default since CUDA 12), so the 64 MiB are reserved on a device by the
+//   first call on it, which also looks up the array's device address
+//   (cudaGetSymbolAddress) with that device current and may synchronise the
+//   device.  Make that first call at start-up, before any real-time loop or
+//   stream capture; later calls allocate nothing.
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdio>
@@ -79,118 +88,6 @@ static int owner(int g, int n, int T)
 {
     if (g >= n - T) return (n + T - 1) / T - 1;
     return g / T;
-}
-
-static double DS(float x) { return std::sqrt((double)x); }
-
-// esat_scale_boundaries (spatial_operators.cpp:307-413) divisors, written into
-// a fixed array laid out [comp][top nx | bottom nx | left nz | right nz].
-static void scale_divisors(int nx, int nz, float dx, float dz, float dt, const float *lam, const float *mu,
-                           const float *rho, bool top, bool bottom, bool left, bool right)
-{
-    const int per = 2 * nx + 2 * nz;
-    for (int i = 0; i < 2 * per; i++) h_den[i] = 1.f;
-    auto set = [&](int k, float s0, float s1) {
-        h_den[k] = 1 + s0;
-        h_den[per + k] = 1 + s1;
-    };
-    auto at = [&](int ix, int iz) { return (long long)ix * nz + iz; };
-    auto cxx = [&](long long i) -> float { return lam[i] + 2 * mu[i]; };
-    const float h0 = sbp_tables().h0;
-    const double ddt = (double)dt, vz = (double)(2 * dz * h0), vx = (double)(2 * dx * h0);
-    const int T0 = 0, B0 = nx, L0 = 2 * nx, R0 = 2 * nx + nz;
-    float sc1x = 0, sc1z = 0, sc2x = 0, sc2z = 0;
-    if (top) {
-        long long c0 = at(0, 0), c1 = at(nx - 1, 0);
-        sc1x = (float)(DS(mu[c0] / rho[c0]) * ddt / vz);
-        sc1z = (float)(sc1x * DS((lam[c0] + 2 * mu[c0]) / mu[c0]));
-        sc2x = (float)(DS(mu[c1] / rho[c1]) * ddt / vz);
-        sc2z = (float)(sc1x * DS((lam[c1] + 2 * mu[c1]) / mu[c1]));
-        for (int ix = 1; ix < nx - 1; ix++) {
-            long long i = at(ix, 0);
-            float sx = (float)(DS(mu[i] / rho[i]) * ddt / vz);
-            float sz = (float)(sx * DS((lam[i] + 2 * mu[i]) / mu[i]));
-            set(T0 + ix, sx, sz);
-        }
-    }
-    if (left) {
-        long long c0 = at(0, 0), b = at(0, nz - 1);
-        sc1x = (float)(sc1x + DS(cxx(c0) / rho[c0]) * ddt / vx);
-        sc1z = (float)(sc1z + DS(mu[c0] / rho[c0]) * ddt / vx);
-        set(T0, sc1x, sc1z);
-        sc1x = (float)(DS(cxx(b) / rho[b]) * ddt / vx);
-        sc1z = (float)(sc1x * DS(mu[b] / cxx(b)));
-        for (int iz = 1; iz < nz - 1; iz++) {
-            long long i = at(0, iz);
-            float sx = (float)(DS(cxx(i) / rho[i]) * ddt / vx);
-            float sz = (float)(sx * DS(mu[i] / cxx(i)));
-            set(L0 + iz, sx, sz);
-        }
-    } else {
-        set(T0, sc1x, sc1z);
-        sc1x = 0;
-        sc1z = 0;
-    }
-    if (bottom) {
-        long long b = at(0, nz - 1), c = at(nx - 1, nz - 1);
-        sc1x = (float)(sc1x + DS(mu[b] / rho[b]) * ddt / vz);
-        sc1z = (float)(sc1z + DS((lam[b] + 2 * mu[b]) / rho[b]) * ddt / vz);
-        set(B0, sc1x, sc1z);
-        sc1x = (float)(DS(mu[c] / rho[c]) * ddt / vz);
-        sc1z = (float)(sc1x * DS((lam[c] + 2 * mu[c]) / mu[c]));
-        for (int ix = 1; ix < nx - 1; ix++) {
-            long long i = at(ix, nz - 1);
-            float sx = (float)(DS(mu[i] / rho[i]) * ddt / vz);
-            float sz = (float)(sx * DS((lam[i] + 2 * mu[i]) / mu[i]));
-            set(B0 + ix, sx, sz);
-        }
-    } else {
-        set(B0, sc1x, sc1z);
-        sc1x = 0;
-        sc1z = 0;
-    }
-    if (right) {
-        long long c = at(nx - 1, nz - 1), t = at(nx - 1, 0);
-        sc1x = (float)(sc1x + DS(cxx(c) / rho[c]) * ddt / vx);
-        sc1z = (float)(sc1z + DS(mu[c] / rho[c]) * ddt / vx);
-        set(B0 + nx - 1, sc1x, sc1z);
-        for (int iz = 1; iz < nz - 1; iz++) {
-            long long i = at(nx - 1, iz);
-            float sx = (float)(DS(cxx(i) / rho[i]) * ddt / vx);
-            float sz = (float)(sx * DS(mu[i] / cxx(i)));
-            set(R0 + iz, sx, sz);
-        }
-        sc2x = (float)(sc2x + DS(cxx(t) / rho[t]) * ddt / vx);
-        sc2z = (float)(sc2z + DS(mu[t] / rho[t]) * ddt / vx);
-        set(T0 + nx - 1, sc2x, sc2z);
-    } else {
-        set(B0 + nx - 1, sc1x, sc1z);
-        set(T0 + nx - 1, sc2x, sc2z);
-    }
-}
-
-// cos^2 taper factors (spatial_operators.cpp:523-549, ISPC loops in float).
-static void tapers(int nx, int nz, const fwi2d_params &p)
-{
-    for (int i = 0; i < nz; i++) h_tz[i] = 1.f;
-    for (int i = 0; i < nx; i++) h_tx[i] = 1.f;
-    const float a = p.taper_strength, pi = (float)M_PI, half = 0.5f;
-    for (int i = 0; i < p.taper_top; i++) {
-        float v = std::cos(a * half * pi * (float)(i + 1 - p.taper_top) / (float)(0 - p.taper_top));
-        h_tz[i] = h_tz[i] * (v * v);
-    }
-    for (int i = nz - p.taper_bottom; i < nz && p.taper_bottom > 0; i++) {
-        float v = std::cos(a * half * pi * (float)(i - (nz - p.taper_bottom)) / (float)p.taper_bottom);
-        h_tz[i] = h_tz[i] * (v * v);
-    }
-    for (int i = 0; i < p.taper_left; i++) {
-        float v = (float)std::cos(a * 0.5 * M_PI * (i + 1 - p.taper_left) / (0 - p.taper_left));
-        h_tx[i] = h_tx[i] * (v * v);
-    }
-    for (int i = nx - p.taper_right; i < nx && p.taper_right > 0; i++) {
-        float v = (float)std::cos(a * 0.5 * M_PI * (i - (nx - p.taper_right)) / p.taper_right);
-        h_tx[i] = h_tx[i] * (v * v);
-    }
 }
 
 // stable grouping of entries by tile (counting sort into fixed arrays)
@@ -254,6 +151,8 @@ extern "C" int fwi2d_propagate_noalloc(const float *model, const float *allsrc, 
     if (p.taper_top < 0 || p.taper_bottom < 0 || p.taper_left < 0 || p.taper_right < 0 ||
         p.taper_top + p.taper_bottom > nz || p.taper_left + p.taper_right > nx)
         return fail(FWI2D_ERR_ARG, "invalid or overlapping tapers");
+    for (const fwi2d_injector *J : {inj, ext})
+        if (!J->xind || !J->zind || !J->xw || !J->zw) return fail(FWI2D_ERR_ARG, "incomplete injector tables");
     for (const fwi2d_injector *J : {inj, ext})
         for (int t = 0; t < J->ntr; t++)
             for (int k = 0; k < 3; k++)
@@ -392,9 +291,11 @@ extern "C" int fwi2d_propagate_noalloc(const float *model, const float *allsrc, 
     }
     const int ioff[2] = {0, ncell};
 
-    scale_divisors(nx, nz, dx, dz, p.dt, lam, mu, rho, p.bc_top == 2, p.bc_bottom == 2, p.bc_left == 2,
-                   p.bc_right == 2);
-    tapers(nx, nz, p);
+    // the regular path's table helpers, writing into the static host arrays
+    elastic_scale_divisors_into(nx, nz, dx, dz, p.dt, lam, mu, rho, nullptr, nz, p.bc_top == 2, p.bc_bottom == 2,
+                                p.bc_left == 2, p.bc_right == 2, h_den);
+    taper_factors_into(nx, nz, p.taper_top, p.taper_bottom, p.taper_left, p.taper_right, p.taper_strength, true,
+                       true, true, true, h_tz, h_tx);
     for (int tzi = 0, k = 0; tzi < tiles_z; tzi++)
         for (int txi = 0; txi < tiles_x; txi++, k++) {
             TileRef &r = h_tiles[k];
@@ -476,6 +377,7 @@ extern "C" int fwi2d_propagate_noalloc(const float *model, const float *allsrc, 
     C.bc[3] = p.bc_right;
     C.sub = 1;
     C.snap_prec = FWI2D_SNAP_FP32;
+    C.spin = 1 << 20;
 
     const ShotDev *shots = (const ShotDev *)(S + o_shot);
     launch_init_state(shots, 1, (const InitCell *)(S + o_cells), (const int *)(S + o_ioff), (const int *)(S + o_idx),

@@ -256,13 +256,19 @@ int fwi2d_propagate(int kind, int adj, const float *model, const float *allsrc, 
  * fwi2d_propagate with adj = 0 and no snapshots, for the elastic isotropic
  * propagator with point-force sources: host inputs, receivers accumulated into
  * allrcv.  All device-side buffers live in one static array of
- * FWI2D_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
- * exit; problems that do not fit it (or exceed the FWI2D_NOALLOC_MAX_* table
- * limits) are rejected with FWI2D_ERR_ARG.  The array keeps the last call's
- * contents (each call clears what must start at zero); calls serialise on the
- * host, and calls that overlap on the GPU race on the array.  The first call
- * on a device looks up the array's device address with that device current:
- * make it before any stream capture.  Errors: fwi2d_noalloc_last_error(). */
+ * FWI2D_NOALLOC_SCRATCH_BYTES; problems that do not fit it (or exceed the
+ * FWI2D_NOALLOC_MAX_* table limits) are rejected with FWI2D_ERR_ARG.
+ * The CUDA runtime loads that array lazily: the first call on a device
+ * reserves it (a GPU then holds it until the process exits), looks up its
+ * device address with that device current and may synchronise the device.
+ * Make that first call at start-up, before any real-time loop or stream
+ * capture; later calls allocate nothing.  The array keeps the last call's
+ * contents (each call clears what must start at zero).  Calls that overlapped
+ * on the GPU would race on it: a host mutex serialises the calls of a process
+ * and each returns only after its GPU work is done, so they never overlap;
+ * every process has its own copy.  Each call runs on the legacy default
+ * stream (not the stream of fwi2d_set_stream), so it synchronises with every
+ * blocking stream on the device.  Errors: fwi2d_noalloc_last_error(). */
 #define FWI2D_NOALLOC_SCRATCH_BYTES (64u << 20)
 #define FWI2D_NOALLOC_MAX_AXIS 16384
 #define FWI2D_NOALLOC_MAX_SOURCES 16
