@@ -1245,8 +1245,8 @@ static void check_timeout(fwi2d_ctx *ctx)
     CK(cudaMemsetAsync(P.d_status.p, 0, sizeof(int), ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     P.snapshots_valid = false;
-    throw Error(FWI2D_ERR_TIMEOUT, "a bounded device wait of the marching kernel gave up (row " +
-                                       std::to_string(v - 1) + "); the results of this pass are invalid");
+    throw Error(FWI2D_ERR_TIMEOUT, "a bounded device wait of the marching kernel reached its limit (row " +
+                                       std::to_string(v - 1) + "); the results of this pass are not trusted");
 }
 
 // Queue the move of the device timeout flag into the plan's status word and

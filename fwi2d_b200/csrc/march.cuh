@@ -46,15 +46,18 @@
 
 namespace fwi2d {
 
-// Set (to the row where it happened + 1) when a bounded wait of the marching
-// kernel gives up.  After every forward or adjoint pass the engine moves it
+// Set (to the row where it happened + 1) when a wait of the marching kernel
+// reaches its limit.  After every forward or adjoint pass the engine moves it
 // into the plan's status word and clears it (launch_take_timeout); the host
 // then returns FWI2D_ERR_TIMEOUT for that pass.
 __device__ int g_march_timeout;
 
-// Iterations of the bounded wait for the copies in flight when a CTA leaves
-// after a timeout (independent of the step-wait limit StepConst::spin).
-#define MARCH_DRAIN_LIMIT (1 << 22)
+// Each per-row wait has two bounds.  Past the first (StepConst::spin polls,
+// FWI2D_SPIN_LIMIT) the row is recorded in g_march_timeout and the CTA keeps
+// waiting for the same phase, so that no copy is left in flight in its shared
+// memory; past the second (MARCH_HARD_LIMIT more polls) the copies are taken
+// to be lost and the CTA leaves.
+#define MARCH_HARD_LIMIT (1 << 22)
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -137,9 +140,7 @@ struct MarchCtx {
     long long slot_elems;
     float *grad;
     unsigned ph[2];           // mbarrier phase parity per stage
-    int spin;                 // poll limit of the per-step wait
-    int tmo_bar;              // after a timeout: the stage whose copies may be in flight, and its parity
-    unsigned tmo_par;
+    int spin;                 // poll limit of the per-step wait before the row is reported
 };
 
 // Register queues along x.  UNR = 8: ring of 8 slots, row j+d of phase PH at
@@ -274,7 +275,7 @@ __device__ __forceinline__ void march_issue(const MarchCtx &X, float *sm, const 
     }
 }
 
-// Returns false when the CTA must stop (a bounded wait gave up).
+// Returns false when the CTA must stop (a wait reached its second bound).
 // Register queues of 8 rows.  Unrolled (PH >= 0): row j+d sits at index
 // (PH + d) & 7.  Rolled (PH < 0): row j+d sits at index d + 2 and the queues
 // shift by one row at the end of each step.
@@ -319,14 +320,17 @@ __device__ __forceinline__ bool march_step(MarchQ<GRAD, UNR> &Q, MarchCtx &X, fl
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(sm + L::MBAR);
 
     // ---- wait for the copies issued at the previous step, then the step barrier
-    bool tmo = false;
+    bool lost = false;
     if (j > j0) {
-        tmo = !mbar_wait(bars + (P & 1), X.ph[P & 1], X.spin);
-        X.tmo_bar = P & 1;
-        X.tmo_par = X.ph[P & 1];
+        const unsigned par = X.ph[P & 1];
+        if (!mbar_wait(bars + (P & 1), par, X.spin)) {
+            // first bound reached: report the row, keep waiting for the phase
+            if (g_march_timeout == 0) atomicCAS(&g_march_timeout, 0, j + 1);
+            lost = !mbar_wait(bars + (P & 1), par, MARCH_HARD_LIMIT);
+        }
         X.ph[P & 1] ^= 1u;
     }
-    if (__syncthreads_or(tmo)) {
+    if (__syncthreads_or(lost)) {
         if (threadIdx.x == 0) atomicCAS(&g_march_timeout, 0, j + 1);
         return false;
     }
@@ -601,8 +605,6 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
     X.grad = S.grad;
     X.ph[0] = X.ph[1] = 0u;
     X.spin = C.spin;
-    X.tmo_bar = 0;
-    X.tmo_par = 0u;
 
     constexpr int UNR = GRAD ? MARCH_GRAD_UNROLL : MARCH_FWD_UNROLL;
     MarchQ<GRAD, UNR> Q;
@@ -625,13 +627,7 @@ elastic_march(const ShotDev *__restrict__ shots, const MarchRef *__restrict__ un
         MARCH_PHASE(4) MARCH_PHASE(5) MARCH_PHASE(6) MARCH_PHASE(7)
 #undef MARCH_PHASE
     }
-    if (!ok) {
-        // the copies of the stage that timed out may still be in flight: give
-        // them a bounded wait before the shared memory is released (no copy
-        // was issued after that wait)
-        mbar_wait(bars + X.tmo_bar, X.tmo_par, MARCH_DRAIN_LIMIT);
-        return;
-    }
+    if (!ok) return;   // a wait reached its second bound: the copies did not arrive
 
     if ((flags & F_AMAX) && ((it + 1) % C.sub == 0)) {
         float *red = smem + L::RED;

@@ -2,15 +2,17 @@
 
 The marching kernel waits on an mbarrier for the bulk copies of each row.
 Every such wait is bounded by a poll limit (FWI2D_SPIN_LIMIT, read when a plan
-is built); a wait that reaches it makes the CTA wait (again bounded) for the
-copies still in flight, set a device flag and leave.  After the pass the
-engine moves the flag into the plan's status word and the call returns
-FWI2D_ERR_TIMEOUT instead of a silently wrong result.
+is built).  A wait that reaches it records the row in a device flag and keeps
+waiting, again bounded, for the same copies, so that none is left in flight
+in the CTA's shared memory (past that second bound the CTA leaves).  After
+the pass the engine moves the flag into the plan's status word and the call
+returns FWI2D_ERR_TIMEOUT instead of results nobody checked.
 
-The test sets the limit to 0 polls, so every wait gives up at once (nothing
-is left spinning, nothing can hang), checks the error code, and then shows
-that the context still works: a plan built with the default limit on the same
-context gives the oracle's traces.
+The test sets the limit to 0 polls, so every wait reaches it at once (the
+second bound is the ordinary one, nothing is left spinning), checks the error
+code and that the pass's snapshots are refused, and then shows that the
+context still works: a plan built with the default limit on the same context
+gives the oracle's traces.
 """
 import numpy as np
 import pytest
@@ -44,7 +46,7 @@ def test_march_wait_limit_returns_timeout(monkeypatch):
     with pytest.raises(C.Fwi2dError) as err:
         P.forward([src], store=True)
     assert err.value.code == C.ERR_TIMEOUT, str(err.value)
-    assert "bounded device wait" in str(err.value)
+    assert "reached its limit" in str(err.value)
     # the adjoint refuses the snapshots of the failed pass
     with pytest.raises(C.Fwi2dError):
         P.adjoint([np.zeros((2, len(rl[0]), nt), np.float32)])
