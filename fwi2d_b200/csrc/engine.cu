@@ -231,6 +231,8 @@ struct Plan {
     int shape = 0;                 // index into the shape list (tile shapes, then marching shapes)
     int tshape = 0, TZ = 32, TX = 16;   // tile shape of the tile kernel's units
     bool march = false;            // interior rows on the marching kernel
+    bool framed = false;           // interior on the tile kernel's interior path, frame on the band kernels
+    int ishape = 0;                // framed: tile shape of the interior tiles
     int nth = 0, lx = 0;           // marching: threads (z window) per unit, rows per unit
     int nt_max = 0;
     int ncompg = 3;
@@ -238,7 +240,8 @@ struct Plan {
     std::vector<TileRef> tiles;
     std::vector<MarchRef> marches;
     std::vector<BandRef> bands;
-    DevBuf d_tiles, d_march, d_bands, d_shots_f, d_shots_a;
+    std::vector<TileRef> itiles;   // framed: interior tiles
+    DevBuf d_tiles, d_march, d_bands, d_itiles, d_shots_f, d_shots_a;
     // checkpoint-and-recompute: every `ckpt` steps; cuts[k] is the first
     // imaging time of segment k (cuts.back() = nt - 1); per-segment shot
     // tables of the replay (forward with snapshot store) and of the adjoint
@@ -427,34 +430,53 @@ static const MarchShape kMarchShapes[] = {{224, 64}, {256, 64}, {192, 64}, {128,
 static const int kNumMarch = sizeof(kMarchShapes) / sizeof(kMarchShapes[0]);
 static const int kBandTile = 3;    // (TZ, TX) = (32, 8): band windows of 8 columns own 6
 static const int kBand = 6;
+// Framed tile plans: the tile kernel's interior path on windows of one of
+// these tile shapes over the cells clear of all four boundary bands, and the
+// band kernels of the marching plans on the frame.  Shape indices follow the
+// marching shapes.
+static const int kFramedShapes[] = {3, 2};
+static const int kNumFramed = sizeof(kFramedShapes) / sizeof(kFramedShapes[0]);
 
-static int shape_count() { return elastic_tile_count() + kNumMarch; }
+static int shape_count() { return elastic_tile_count() + kNumMarch + kNumFramed; }
+static bool is_march_shape(int s) { return s >= elastic_tile_count() && s < elastic_tile_count() + kNumMarch; }
+static bool is_framed_shape(int s) { return s >= elastic_tile_count() + kNumMarch && s < shape_count(); }
+static int framed_tile_shape(int s) { return kFramedShapes[s - elastic_tile_count() - kNumMarch]; }
 
 // Work units of one shot.  Units are numbered per shot: tiles first, then
 // marching units (segment-major, then z window).
 struct ShotUnits {
-    bool march = false;
+    bool march = false;            // marching plan: x-band tiles, bands, marching units
+    bool framed = false;           // framed tile plan: x-band tiles, bands, interior tiles
     int nx = 0, nz = 0;
     int TX = 0, TZ = 0, tiles_x = 0, tiles_z = 0;
     int lx = 0, nseg = 0, nwin = 0;
+    int ITX = 0, ITZ = 0, itiles_x = 0;   // framed: interior tile shape and tiles along x
     std::vector<int> zo;           // marching: owned z starts of the core windows, plus nz - 6
-    std::vector<TileRef> tiles;    // marching plans: the x-band tiles
+    std::vector<TileRef> tiles;    // marching and framed plans: the x-band tiles
     std::vector<BandRef> bands;    // top / bottom band units (two per run of rows)
     std::vector<MarchRef> marches;
-    int nunits() const { return (int)(tiles.size() + bands.size() + marches.size()); }
+    std::vector<TileRef> itiles;   // framed: tiles of the interior [6, nx-6) x [6, nz-6)
+    int nunits() const { return (int)(tiles.size() + bands.size() + marches.size() + itiles.size()); }
     int unit_of(int x, int z) const
     {
-        if (!march) return owner_tile(z, nz, TZ) * tiles_x + owner_tile(x, nx, TX);
+        if (!march && !framed) return owner_tile(z, nz, TZ) * tiles_x + owner_tile(x, nx, TX);
         if (x < kBand) return owner_tile(z, nz, TZ);
         if (x >= nx - kBand) return tiles_z + owner_tile(z, nz, TZ);
         const int nt = (int)tiles.size();
         if (z < kBand || z >= nz - kBand) return nt + 2 * ((x - kBand) / zband_rows()) + (z < kBand ? 0 : 1);
+        if (framed)
+            return nt + (int)bands.size() + owner_tile(z - kBand, nz - 2 * kBand, ITZ) * itiles_x +
+                   owner_tile(x - kBand, nx - 2 * kBand, ITX);
         const int seg = (x - kBand) / lx;
         const int k = (int)(std::upper_bound(zo.begin(), zo.end(), z) - zo.begin()) - 1;
         return nt + (int)bands.size() + seg * nwin + k;
     }
     // units whose entries are sorted by row and indexed by per-row records
-    bool row_sorted(int u) const { return u >= (int)tiles.size(); }
+    // (band and marching units)
+    bool row_sorted(int u) const
+    {
+        return u >= (int)tiles.size() && u < (int)(tiles.size() + bands.size() + marches.size());
+    }
     struct RowUnit {
         int unit, xb, xe, roff;
     };
@@ -496,8 +518,13 @@ static bool shape_fits(int shape, int nx, int nz)
         return axis_fits(tz, nz) && axis_fits(tx, nx);
     }
     elastic_tile_shape(kBandTile, &tz, &tx);
-    return axis_fits(tz, nz) && nx >= 2 * tx && nx > 2 * kBand && nz >= 40 &&
-           march_threads_ok(kMarchShapes[shape - elastic_tile_count()].nth);
+    const bool frame = axis_fits(tz, nz) && nx >= 2 * tx && nx > 2 * kBand && nz >= 40;
+    if (is_framed_shape(shape)) {
+        int itz, itx;
+        elastic_tile_shape(framed_tile_shape(shape), &itz, &itx);
+        return frame && axis_fits(itz, nz - 2 * kBand) && axis_fits(itx, nx - 2 * kBand);
+    }
+    return frame && march_threads_ok(kMarchShapes[shape - elastic_tile_count()].nth);
 }
 
 static ShotUnits make_units(int shape, int shot, int nx, int nz)
@@ -505,11 +532,13 @@ static ShotUnits make_units(int shape, int shot, int nx, int nz)
     ShotUnits U;
     U.nx = nx;
     U.nz = nz;
-    const bool march = shape >= elastic_tile_count();
+    const bool framed = is_framed_shape(shape);
+    const bool march = is_march_shape(shape);
     U.march = march;
-    elastic_tile_shape(march ? kBandTile : shape, &U.TZ, &U.TX);
+    U.framed = framed;
+    elastic_tile_shape(march || framed ? kBandTile : shape, &U.TZ, &U.TX);
     U.tiles_z = (nz + U.TZ - 1) / U.TZ;
-    if (!march) {
+    if (!march && !framed) {
         U.tiles_x = (nx + U.TX - 1) / U.TX;
         for (int tzi = 0; tzi < U.tiles_z; tzi++)
             for (int txi = 0; txi < U.tiles_x; txi++) {
@@ -546,6 +575,29 @@ static ShotUnits make_units(int shape, int shot, int nx, int nz)
             roff += b.xe - b.xb + 1;
             U.bands.push_back(b);
         }
+    if (framed) {
+        // interior windows, tiled as the tile plans tile a whole grid, offset by the band
+        elastic_tile_shape(framed_tile_shape(shape), &U.ITZ, &U.ITX);
+        const int ni_x = nx - 2 * kBand, ni_z = nz - 2 * kBand;
+        U.itiles_x = (ni_x + U.ITX - 1) / U.ITX;
+        const int itiles_z = (ni_z + U.ITZ - 1) / U.ITZ;
+        for (int tzi = 0; tzi < itiles_z; tzi++)
+            for (int txi = 0; txi < U.itiles_x; txi++) {
+                TileRef r;
+                r.shot = shot;
+                r.unit = (int)(U.tiles.size() + U.bands.size() + U.itiles.size());
+                tile_window_host(txi, U.itiles_x, ni_x, U.ITX, r.wx0, r.ox0, r.ox1);
+                tile_window_host(tzi, itiles_z, ni_z, U.ITZ, r.wz0, r.oz0, r.oz1);
+                r.wx0 += kBand;
+                r.ox0 += kBand;
+                r.ox1 += kBand;
+                r.wz0 += kBand;
+                r.oz0 += kBand;
+                r.oz1 += kBand;
+                U.itiles.push_back(r);
+            }
+        return U;
+    }
     const MarchShape ms = kMarchShapes[shape - elastic_tile_count()];
     std::vector<int> za;
     march_windows(nz, ms.nth, U.zo, za);
@@ -991,8 +1043,10 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     }
     REQ(shape_ok(shape), "the requested tile shape does not fit a shot grid");
     P->shape = shape;
-    P->march = shape >= elastic_tile_count();
-    P->tshape = P->march ? kBandTile : shape;
+    P->march = is_march_shape(shape);
+    P->framed = is_framed_shape(shape);
+    P->tshape = P->march || P->framed ? kBandTile : shape;
+    if (P->framed) P->ishape = framed_tile_shape(shape);
     elastic_tile_shape(P->tshape, &P->TZ, &P->TX);
     if (P->march) {
         P->nth = kMarchShapes[shape - elastic_tile_count()].nth;
@@ -1165,12 +1219,14 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         P->tiles.insert(P->tiles.end(), U.tiles.begin(), U.tiles.end());
         P->marches.insert(P->marches.end(), U.marches.begin(), U.marches.end());
         P->bands.insert(P->bands.end(), U.bands.begin(), U.bands.end());
+        P->itiles.insert(P->itiles.end(), U.itiles.begin(), U.itiles.end());
         P->shots.push_back(std::move(S));
     }
     P->have_snapshots = p.sub > 0;
     P->d_tiles.upload(P->tiles, ctx->st);
     P->d_march.upload(P->marches, ctx->st);
     P->d_bands.upload(P->bands, ctx->st);
+    P->d_itiles.upload(P->itiles, ctx->st);
     std::vector<ShotDev> sf(nshots), sa(nshots);
     for (int s = 0; s < nshots; s++) {
         shot_dev(*P, *P->shots[s], M, false, sf[s]);
@@ -1284,7 +1340,7 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
                              st);
         return 1;
     }
-    if (P.marches.empty()) {
+    if (!P.march && !P.framed) {
         launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md,
                             P.C, it, flags, P.dtg, st);
         return 1;
@@ -1297,8 +1353,12 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
                          P.dtg, ctx->side);
     n += 2;
     CK(cudaEventRecord(ctx->join, ctx->side));
-    launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>(), (int)P.marches.size(), P.nth, md, P.C,
-                         it, flags, P.dtg, st);
+    if (P.framed)
+        launch_elastic_step(P.ishape, P.kind == KIND_VTI, shots, P.d_itiles.as<TileRef>(), (int)P.itiles.size(), md,
+                            P.C, it, flags, P.dtg, st);
+    else
+        launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>(), (int)P.marches.size(), P.nth, md,
+                             P.C, it, flags, P.dtg, st);
     n++;
     CK(cudaStreamWaitEvent(st, ctx->join, 0));
     return n;
@@ -2419,7 +2479,7 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     REQ(ctx, "null context");
     Plan &P = need_plan(ctx);
     const long long steps = P.nt_max - 1;
-    const long long per = P.marches.empty() && !P.ae ? 1 : 3;
+    const long long per = (P.march || P.framed || P.ae) ? 3 : 1;
     const long long nseg = P.ckpt > 0 ? (long long)P.cuts.size() - 1 : 0;
     const long long acf = P.kind == KIND_ACOUSTIC ? 1 : 0;
     // forward: init, steps, last sample (+ checkpoint copies); adjoint: init, steps,
@@ -2478,6 +2538,7 @@ int fwi2d_tile_shape(int index, int *tz, int *tx)
     ABI_TRY
     REQ(index >= 0 && index < shape_count() && tz && tx, "no such tile shape");
     if (index < elastic_tile_count()) elastic_tile_shape(index, tz, tx);
+    else if (is_framed_shape(index)) elastic_tile_shape(framed_tile_shape(index), tz, tx);
     else {
         *tz = kMarchShapes[index - elastic_tile_count()].nth;
         *tx = kMarchShapes[index - elastic_tile_count()].lx;

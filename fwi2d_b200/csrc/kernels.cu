@@ -151,8 +151,9 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     const bool full = tr.ox0 == wx0 && tr.ox1 == wx0 + TX && tr.oz0 == wz0 && tr.oz1 == wz0 + TZ;
     const bool lean = !AE && RZ == 2 && interior && full && (wz0 & 3) == 0;
     // one cell per thread: tiles clear of the boundary bands take the scalar
-    // interior forms (no closure code, which keeps the hot loop small)
-    const bool lean1 = !AE && RZ == 1 && interior && full;
+    // interior forms (no closure code, which keeps the hot loop small); a
+    // thread whose cell the tile does not own computes nothing in phase 3
+    const bool lean1 = !AE && RZ == 1 && interior;
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
@@ -183,6 +184,33 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             const float4 b = *reinterpret_cast<const float4 *>(curr + nxz + o);
             *reinterpret_cast<float4 *>(U0 + r * UZ + 4 * q) = a;
             *reinterpret_cast<float4 *>(U1 + r * UZ + 4 * q) = b;
+        }
+        constexpr int Q2 = WZ / 2;
+        for (int f = threadIdx.x; f < WX * Q2; f += NT) {
+            const int r = f / Q2, q = f - r * Q2;
+            const int o = (wx0 - 2 + r) * mld + wz0 - 2 + 2 * q;
+            *reinterpret_cast<float2 *>(MU + r * WZ + 2 * q) = *reinterpret_cast<const float2 *>(mp1 + o);
+            *reinterpret_cast<float2 *>(Q + r * WZ + 2 * q) = *reinterpret_cast<const float2 *>(qsrc + o);
+            if (GRAD) {
+                float2 f0 = make_float2(0.f, 0.f), f1 = f0;
+                if (do_grad) {
+                    const long long so = (long long)itf * slot_elems + (wx0 - 2 + r) * ldz + wz0 - 2 + 2 * q;
+                    f0 = snap_load2(snap, so, prec, finv);
+                    f1 = snap_load2(snap, so + nxz, prec, finv);
+                }
+                *reinterpret_cast<float2 *>(F0 + r * WZ + 2 * q) = f0;
+                *reinterpret_cast<float2 *>(F1 + r * WZ + 2 * q) = f1;
+            }
+        }
+    } else if (lean1 && (wz0 & 1) == 0) {
+        // interior window on an even row: pairs of samples, no bounds checks
+        // (the window and its 4-cell halo lie inside the grid)
+        constexpr int Q2U = UZ / 2;
+        for (int f = threadIdx.x; f < UX * Q2U; f += NT) {
+            const int r = f / Q2U, q = f - r * Q2U;
+            const int o = (wx0 - 4 + r) * ldz + wz0 - 4 + 2 * q;
+            *reinterpret_cast<float2 *>(U0 + r * UZ + 2 * q) = *reinterpret_cast<const float2 *>(curr + o);
+            *reinterpret_cast<float2 *>(U1 + r * UZ + 2 * q) = *reinterpret_cast<const float2 *>(curr + nxz + o);
         }
         constexpr int Q2 = WZ / 2;
         for (int f = threadIdx.x; f < WX * Q2; f += NT) {
@@ -534,6 +562,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
         // the general path's arithmetic in its interior forms (sbp.cuh d1i,
         // md1i, d2i): no SAT and no boundary divisor can reach these cells
         const int gx = wx0 + warp, gz = wz0 + lane;
+        if (gx >= tr.ox0 && gx < tr.ox1 && gz >= tr.oz0 && gz < tr.oz1) {
         const int ui = (warp + 4) * UZ + (lane + 4);
         const int wi = (warp + 2) * WZ + (lane + 2);
         const int cell = gx * ldz + gz;
@@ -640,6 +669,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 *g1 = *g1 + gw * dtg * dm;
                 *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
             }
+        }
         }
     } else {
 #pragma unroll

@@ -227,7 +227,12 @@ int fwi2d_copy_gradient(fwi2d_ctx *ctx, float *dst_device);
  * adjoint time loops, in milliseconds (-1 if none ran). */
 int fwi2d_last_timing(fwi2d_ctx *ctx, float *forward_ms, float *adjoint_ms);
 
-/* Tile shapes offered to the autotuner. */
+/* Work shapes offered to the autotuner: tile shapes of the tile kernel over
+ * whole shot grids (tz x tx cells), then marching shapes (tz threads, one z
+ * cell each, marching runs of tx rows) for the cells clear of the boundary
+ * bands, then framed tile shapes (tz x tx tiles of the tile kernel's interior
+ * path over those cells); marching and framed plans run the boundary bands on
+ * the band kernels. */
 int fwi2d_tile_shape_count(void);
 int fwi2d_tile_shape(int index, int *tz, int *tx);
 

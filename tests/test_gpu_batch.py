@@ -9,8 +9,8 @@ same nt:
 * the model-grid gradient (the sum of the shots' imaging conditions scattered
   onto their columns) to 1e-5 rel-L2.
 
-Both the tile kernel and the marching kernel (with its band kernels) are
-covered, for the elastic and VTI propagators.  The grid spacing is 2^-7 km and
+The tile kernel, the marching kernel and the framed tile plan (the last two
+with their band kernels) are covered, for the elastic and VTI propagators.  The grid spacing is 2^-7 km and
 every location sits on a binary fraction of a cell, so that the injector
 weights computed from model coordinates (the batch) and from the cropped
 grid's own coordinates (the oracle) are the same numbers.
@@ -34,7 +34,7 @@ SHOTS = [  # x0, nx, nt, source x offset (cells), receivers
 
 
 @pytest.mark.parametrize("kind", [O.KIND_ELASTIC, O.KIND_VTI])
-@pytest.mark.parametrize("shape", [3, 4])
+@pytest.mark.parametrize("shape", [3, 4, 14])
 def test_uneven_batch_matches_per_shot_oracle(kind, shape):
     nxm, nz, d, dt = 160, 72, 2.0 ** -7, 1e-3
     raw = K.model_case(kind, nxm, nz, d, seed=21)

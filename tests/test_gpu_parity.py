@@ -44,7 +44,8 @@ def run_gpu(kind, mc, src, pd, nx, nz, d, src_locs, rcv_locs, adj_src=None, mt=0
 @pytest.mark.parametrize("shape,grid", [(0, (72, 80)), (1, (72, 80)), (2, (72, 80)), (3, (72, 80)),
                                         (0, (120, 200)), (1, (120, 200)),
                                         (4, (72, 80)), (6, (120, 200)), (7, (120, 200)), (11, (120, 200)),
-                                        (11, (60, 251))])
+                                        (11, (60, 251)), (14, (72, 80)), (15, (72, 80)), (14, (120, 200)),
+                                        (15, (60, 251))])
 def test_forward_adjoint_vs_oracle(kind, mt, bc, shape, grid):
     """Shapes 0-3 run the tile kernel over the whole grid: small grids exercise
     the boundary path only; the 120 x 200 grid has interior tiles, which take
@@ -52,7 +53,10 @@ def test_forward_adjoint_vs_oracle(kind, mt, bc, shape, grid):
     marching kernel on the rows clear of the x boundary bands (one z window
     on 80 rows, two on 200; on 251 rows with 128-cell windows the last
     window is shifted up so that it owns the whole bottom band) and runs of
-    64 or 32 rows."""
+    64 or 32 rows.  Shapes 14 and 15 are framed plans: 32 x 8 and 32 x 16
+    tiles on the tile kernel's interior path over the cells clear of the
+    bands (the last window of each axis flush with the band, owning part of
+    its cells), the bands on the band kernels."""
     nx, nz = grid
     d, nt = 0.01, 220 if nz < 100 else 160
     m = K.model_case(kind, nx, nz, d, seed=3)
