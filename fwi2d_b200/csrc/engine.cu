@@ -145,6 +145,35 @@ __global__ void k_unpitch(const float *__restrict__ in, float *__restrict__ out,
     }
 }
 
+// Compensated (two-level) gradient accumulation.  The step kernels add each
+// time sample's imaging term into the FP32 accumulator `grad` in the
+// reference's order, so that `grad` holds the sum over the last few adjoint
+// steps only; every kCompWindow steps this kernel adds it into a running sum
+// held as an unevaluated pair (hi, lo) with Neumaier's compensated summation
+// (hi + lo carries the sum to about twice the FP32 precision) and clears it.
+// final: the last partial window is added and `grad` receives hi + lo.
+static const int kCompWindow = 8;
+__global__ void k_grad_flush(const ShotDev *__restrict__ shots, int ncompg, int final)
+{
+    const ShotDev &S = shots[blockIdx.y];
+    const long long n = (long long)ncompg * S.nx * S.ldz;
+    float *__restrict__ g = S.grad;
+    float *__restrict__ hi = S.gcomp;
+    float *__restrict__ lo = S.gcomp + n;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float w = g[i], h = hi[i];
+        const float t = h + w;
+        const float c = lo[i] + (fabsf(h) >= fabsf(w) ? (h - t) + w : (w - t) + h);
+        if (final) {
+            g[i] = t + c;
+        } else {
+            hi[i] = t;
+            lo[i] = c;
+            g[i] = 0.f;
+        }
+    }
+}
+
 void launch_to_time_major(const float *in, float *out, int rows, int nt, cudaStream_t st)
 {
     dim3 g((nt + 31) / 32, (rows + 31) / 32), b(32, 8);
@@ -211,6 +240,9 @@ struct ShotPlan {
     int nsrc_rows = 0, nrcv_rows = 0;
     int nslot = 0;                 // snapshot time slots of the shot (1 + nt/sub)
     int nbuf = 0;                  // slots held on the device (nslot, or the replay window)
+    size_t snap_need = 0;          // bytes of its snapshot store
+    int u_t0 = 0, u_m0 = 0, u_b0 = 0, u_i0 = 0;   // first tile / marching / band / interior unit in the plan
+    void *snap_base = nullptr;     // its snapshot store: `snap`, or its place in the plan's wave pool
     std::vector<InjEntry> inj_f, inj_a;
     std::vector<int> inj_f_off, inj_a_off, inj_f_roff, inj_a_roff;
     std::vector<ExtEntry> ext_f;
@@ -220,6 +252,7 @@ struct ShotPlan {
     DevBuf d_inj_f, d_inj_f_off, d_inj_a, d_inj_a_off, d_ext_f, d_ext_f_off, d_ext_none_off;
     DevBuf d_mrow_f, d_mrow_a;
     DevBuf den, tz, tx, snap, amax, grad, gwt;
+    DevBuf gcomp;                  // compensated accumulation: running sum pair (hi, lo) of the gradient
     DevBuf r0, r1, ckpt;           // checkpoint-and-recompute: replay fields and checkpoints
     DevBuf halo;                   // acoustic-elastic: prev of the interface row [nx]
     std::unique_ptr<ShotPlan> fluid;   // acoustic-elastic: the fluid layer's grid (nx x nza)
@@ -242,6 +275,23 @@ struct Plan {
     std::vector<BandRef> bands;
     std::vector<TileRef> itiles;   // framed: interior tiles
     DevBuf d_tiles, d_march, d_bands, d_itiles, d_shots_f, d_shots_a;
+    // Waves: contiguous runs of shots whose snapshots fit the device together.
+    // A plan whose snapshots all fit has one wave.  Each wave has its own
+    // forward-with-snapshots and adjoint graphs over its shots' units; the
+    // waves share one snapshot pool (snap_pool), so a gradient runs wave by
+    // wave.  `all` spans every shot and unit (forward without snapshots,
+    // autotuning).
+    struct Wave {
+        int s0 = 0, s1 = 0, nt_max = 0;
+        int t0 = 0, t1 = 0, m0 = 0, m1 = 0, b0 = 0, b1 = 0, i0 = 0, i1 = 0;   // unit ranges
+        cudaGraphExec_t graph[2] = {nullptr, nullptr};                        // forward + snapshots, adjoint
+        cudaEvent_t ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+        long long launches[2] = {0, 0};
+    };
+    std::vector<Wave> waves;
+    Wave all;
+    DevBuf snap_pool;
+    bool fwd_waves = false;        // the last forward timing is the sum over the waves' events
     // checkpoint-and-recompute: every `ckpt` steps; cuts[k] is the first
     // imaging time of segment k (cuts.back() = nt - 1); per-segment shot
     // tables of the replay (forward with snapshot store) and of the adjoint
@@ -300,6 +350,13 @@ struct Plan {
     ~Plan()
     {
         if (h_status) cudaFreeHost(h_status);
+        for (auto &w : waves) {
+            for (auto &g : w.graph)
+                if (g) cudaGraphExecDestroy(g);
+            for (auto &a : w.ev)
+                for (auto &e : a)
+                    if (e) cudaEventDestroy(e);
+        }
         for (auto &g : graph)
             if (g) cudaGraphExecDestroy(g);
         for (auto &a : ev)
@@ -779,7 +836,6 @@ static StepConst make_const(const fwi2d_params &p, float dx, float dz)
     C.bc[3] = p.bc_right;
     C.sub = p.sub > 0 ? p.sub : 1;
     C.snap_prec = p.snapshot_precision;
-    C.kahan = p.compensated;
     // poll limit of the marching kernel's bounded waits: FWI2D_SPIN_LIMIT
     // (read when a plan is built) or 2^20 polls
     C.spin = 1 << 20;
@@ -826,10 +882,11 @@ static void shot_dev(const Plan &P, const ShotPlan &s, const ModelState &M, bool
     d.den = s.den.as<float>();
     d.tz = s.tz.as<float>();
     d.tx = s.tx.as<float>();
-    d.snap = s.snap.p;
+    d.snap = s.snap_base;
     d.snap_slot = (long long)s.ncomp * s.nx * M.ldz;
     d.snap_amax = s.amax.as<unsigned>();
     d.grad = s.grad.as<float>();
+    d.gcomp = s.gcomp.as<float>();
     d.gwt = s.gwt.as<float>();
     d.halo_save = s.halo.as<float>();
     (void)P;
@@ -952,6 +1009,92 @@ static void upload_init_cells(Plan &P, cudaStream_t st)
         P.d_icells[mode].upload(P.icells[mode], st);
         P.d_ioff[mode].upload(P.ioff[mode], st);
         P.d_iidx[mode].upload(P.iidx[mode], st);
+    }
+}
+
+// Snapshot stores and waves.  All shots in one wave when their snapshots fit
+// the device (less a reserve for the rest of the work), each shot with its
+// own store.  Otherwise contiguous runs of shots, each as large as the
+// budget takes, that share one pool as large as the largest run.
+// FWI2D_SNAPSHOT_BUDGET (bytes) replaces the budget.  Elastic and VTI plans
+// only: checkpointed plans (their replay windows are small), acoustic and
+// acoustic-elastic plans keep one wave.
+static void plan_waves(Plan &P, bool one_wave)
+{
+    const int n = (int)P.shots.size();
+    size_t total = 0, largest = 0;
+    for (auto &S : P.shots) {
+        total += S->snap_need;
+        largest = std::max(largest, S->snap_need);
+    }
+    size_t budget = 0;
+    if (const char *e = std::getenv("FWI2D_SNAPSHOT_BUDGET")) {
+        budget = (size_t)std::strtoull(e, nullptr, 10);
+    } else {
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t reserve = (size_t)2 << 30;
+        budget = free_b > reserve ? free_b - reserve : 0;
+        budget -= budget / 20;
+    }
+    auto range = [&](Plan::Wave &w, int s0, int s1) {
+        w.s0 = s0;
+        w.s1 = s1;
+        w.nt_max = 0;
+        for (int s = s0; s < s1; s++) w.nt_max = std::max(w.nt_max, P.shots[s]->nt);
+        const ShotPlan &a = *P.shots[s0];
+        w.t0 = a.u_t0;
+        w.m0 = a.u_m0;
+        w.b0 = a.u_b0;
+        w.i0 = a.u_i0;
+        if (s1 < n) {
+            const ShotPlan &b = *P.shots[s1];
+            w.t1 = b.u_t0;
+            w.m1 = b.u_m0;
+            w.b1 = b.u_b0;
+            w.i1 = b.u_i0;
+        } else {
+            w.t1 = (int)P.tiles.size();
+            w.m1 = (int)P.marches.size();
+            w.b1 = (int)P.bands.size();
+            w.i1 = (int)P.itiles.size();
+        }
+    };
+    P.waves.clear();
+    range(P.all, 0, n);
+    if (one_wave || total <= budget || total == 0) {
+        P.waves.push_back(P.all);
+        for (auto &S : P.shots) {
+            S->snap.alloc(S->snap_need);
+            S->snap_base = S->snap.p;
+        }
+        return;
+    }
+    if (largest > budget)
+        throw Error(FWI2D_ERR_OOM, "the snapshots of one shot exceed the device memory: use checkpoint_every");
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t pool = 0;
+    for (int s0 = 0; s0 < n;) {
+        size_t bytes = 0;
+        int s1 = s0;
+        while (s1 < n && (s1 == s0 || bytes + al(P.shots[s1]->snap_need) <= budget))
+            bytes += al(P.shots[s1++]->snap_need);
+        Plan::Wave w;
+        range(w, s0, s1);
+        P.waves.push_back(w);
+        pool = std::max(pool, bytes);
+        s0 = s1;
+    }
+    P.snap_pool.alloc(pool);
+    P.snap_bytes = P.snap_bytes - total + pool;
+    for (const auto &w : P.waves) {
+        size_t off = 0;
+        for (int s = w.s0; s < w.s1; s++) {
+            ShotPlan &S = *P.shots[s];
+            S.snap.release();
+            S.snap_base = (char *)P.snap_pool.p + off;
+            off += (S.snap_need + 255) & ~(size_t)255;
+        }
     }
 }
 
@@ -1197,13 +1340,15 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->tx.upload(tx, ctx->st);
         S->gwt.upload(gw, ctx->st);
         S->grad.alloc((size_t)P->ncompg * sh.nx * M.ldz * sizeof(float));
+        if (p.compensated && p.sub > 0) S->gcomp.alloc(2 * S->grad.n);
+        else S->gcomp.release();
         if (S->nslot > 0) {
             const size_t esz = p.snapshot_precision == FWI2D_SNAP_FP32 ? 4 : 2;
             const int K = p.checkpoint_every;
             // checkpointing: a replay window of K + 2 slots (times cuts[k]-1 .. cuts[k+1])
             S->nbuf = K > 0 ? std::min(S->nslot, K + 2) : S->nslot;
             size_t bytes = (size_t)S->nbuf * field * esz;
-            S->snap.alloc(bytes);
+            S->snap_need = bytes;   // allocated below, once the waves are known
             S->amax.alloc((size_t)S->nslot * sizeof(unsigned));
             if (K > 0) {
                 const int nseg = (sh.nt - 1 + K - 1) / K;
@@ -1216,6 +1361,10 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             total_bytes += bytes;
         }
         P->nt_max = std::max(P->nt_max, sh.nt);
+        S->u_t0 = (int)P->tiles.size();
+        S->u_m0 = (int)P->marches.size();
+        S->u_b0 = (int)P->bands.size();
+        S->u_i0 = (int)P->itiles.size();
         P->tiles.insert(P->tiles.end(), U.tiles.begin(), U.tiles.end());
         P->marches.insert(P->marches.end(), U.marches.begin(), U.marches.end());
         P->bands.insert(P->bands.end(), U.bands.begin(), U.bands.end());
@@ -1223,6 +1372,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         P->shots.push_back(std::move(S));
     }
     P->have_snapshots = p.sub > 0;
+    plan_waves(*P, p.checkpoint_every > 0 || ae || acoustic);
     P->d_tiles.upload(P->tiles, ctx->st);
     P->d_march.upload(P->marches, ctx->st);
     P->d_bands.upload(P->bands, ctx->st);
@@ -1261,7 +1411,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             const long long base = k == 0 ? -1 : P->cuts[k] - 1;
             for (int s = 0; s < nshots; s++) {
                 ShotPlan &S = *P->shots[s];
-                char *win = (char *)S.snap.p - base * (long long)sf[s].snap_slot * (long long)esz;
+                char *win = (char *)S.snap_base - base * (long long)sf[s].snap_slot * (long long)esz;
                 ShotDev r = sf[s];
                 r.u[0] = S.r0.as<float>();
                 r.u[1] = S.r1.as<float>();
@@ -1320,8 +1470,13 @@ static void queue_timeout_check(fwi2d_ctx *ctx, Plan &P)
 // disjoint cells and join before the next step.  Returns the number of
 // launches.
 static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, const ModelDev &md, int it, int flags,
-                       cudaStream_t st)
+                       cudaStream_t st, const Plan::Wave *wave = nullptr)
 {
+    // the units of the wave's shots (the kernels index the shot tables by the
+    // units' own shot numbers)
+    const Plan::Wave &R = wave ? *wave : P.all;
+    const TileRef *tiles = P.d_tiles.as<TileRef>() + R.t0;
+    const int ntiles = R.t1 - R.t0;
     int n = 0;
     if (P.ae) {
         // fluid layer, elastic grid, then the implicit interface coupling
@@ -1341,24 +1496,22 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
         return 1;
     }
     if (!P.march && !P.framed) {
-        launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md,
-                            P.C, it, flags, P.dtg, st);
+        launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, st);
         return 1;
     }
     CK(cudaEventRecord(ctx->fork, st));
     CK(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
-    launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C,
-                        it, flags, P.dtg, ctx->side);
-    launch_elastic_zband(P.kind == KIND_VTI, P.d_bands.as<BandRef>(), (int)P.bands.size(), shots, md, P.C, it, flags,
+    launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
+    launch_elastic_zband(P.kind == KIND_VTI, P.d_bands.as<BandRef>() + R.b0, R.b1 - R.b0, shots, md, P.C, it, flags,
                          P.dtg, ctx->side);
     n += 2;
     CK(cudaEventRecord(ctx->join, ctx->side));
     if (P.framed)
-        launch_elastic_step(P.ishape, P.kind == KIND_VTI, shots, P.d_itiles.as<TileRef>(), (int)P.itiles.size(), md,
+        launch_elastic_step(P.ishape, P.kind == KIND_VTI, shots, P.d_itiles.as<TileRef>() + R.i0, R.i1 - R.i0, md,
                             P.C, it, flags, P.dtg, st);
     else
-        launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>(), (int)P.marches.size(), P.nth, md,
-                             P.C, it, flags, P.dtg, st);
+        launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>() + R.m0, R.m1 - R.m0, P.nth, md, P.C,
+                             it, flags, P.dtg, st);
     n++;
     CK(cudaStreamWaitEvent(st, ctx->join, 0));
     return n;
@@ -1518,6 +1671,8 @@ static float tune_close()
 }
 
 static void run(fwi2d_ctx *ctx, bool adjoint, bool store);
+static void run_wave(fwi2d_ctx *ctx, Plan &P, int w, bool adjoint);
+static float pass_ms(Plan &P, int e);
 
 // One whole forward pass with snapshots and one adjoint pass of the current
 // plan on zero traces, in milliseconds (the plan's graphs, CUDA events).
@@ -1528,13 +1683,12 @@ static float time_full_pass(fwi2d_ctx *ctx)
         CK(cudaMemsetAsync(S->src_f.p, 0, S->src_f.n, ctx->st));
         CK(cudaMemsetAsync(S->src_a.p, 0, S->src_a.n, ctx->st));
     }
-    run(ctx, false, true);
-    run(ctx, true, false);
+    for (int w = 0; w < (int)P.waves.size(); w++) {
+        run_wave(ctx, P, w, false);
+        run_wave(ctx, P, w, true);
+    }
     CK(cudaStreamSynchronize(ctx->st));
-    float f = 0.f, a = 0.f;
-    CK(cudaEventElapsedTime(&f, P.ev[0][0], P.ev[0][1]));
-    CK(cudaEventElapsedTime(&a, P.ev[1][0], P.ev[1][1]));
-    return f + a;
+    return pass_ms(P, 0) + pass_ms(P, 1);
 }
 static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const fwi2d_shot *shots)
 {
@@ -1633,6 +1787,20 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
     set_shots_impl(ctx, &p, nshots, shots);
 }
 
+// Compensated accumulation (params.compensated): after adjoint launch
+// `count` (1-based), close a window every kCompWindow launches; `final` adds
+// the last window and leaves the sum in the gradient accumulators.  Returns
+// the number of launches.
+static int grad_flush(const Plan &P, const Plan::Wave &R, int count, bool final, cudaStream_t st)
+{
+    if (!P.par.compensated || P.shots.empty() || !P.shots[0]->gcomp.p) return 0;
+    if (!final && count % kCompWindow != 0) return 0;
+    k_grad_flush<<<dim3(148, (unsigned)(R.s1 - R.s0)), 256, 0, st>>>(P.d_shots_a.as<ShotDev>() + R.s0, P.ncompg,
+                                                                        final ? 1 : 0);
+    CK(cudaGetLastError());
+    return 1;
+}
+
 // Checkpoint-and-recompute time loops (all shots share nt, sub = 1).
 // Forward: receivers and 16-bit snapshot scales as usual, no snapshot store;
 // before launch cuts[k] - 1 (k >= 1) both field buffers of every shot are
@@ -1668,6 +1836,7 @@ static long long capture_checkpointed(fwi2d_ctx *ctx, Plan &P, bool adj, cudaStr
     // acoustic imaging at launch it uses time nt-1-it, the elastic one nt-2-it
     const int a = P.kind == KIND_ACOUSTIC ? 1 : 0;
     const ShotDev *last_adj = nullptr;
+    int nadj = 0;   // adjoint launches so far (compensated accumulation windows)
     for (int k = nseg - 1; k >= 0; k--) {
         const ShotDev *rs = P.d_shots_r.as<ShotDev>() + (size_t)k * nshots;
         const ShotDev *as = P.d_shots_c.as<ShotDev>() + (size_t)k * nshots;
@@ -1688,7 +1857,10 @@ static long long capture_checkpointed(fwi2d_ctx *ctx, Plan &P, bool adj, cudaStr
         n++;
         const int lo = k == nseg - 1 ? 0 : nt - 1 - P.cuts[k + 1] + a;
         const int hi = k == 0 ? nt - 2 : nt - 2 - P.cuts[k] + a;
-        for (int it = lo; it <= hi; it++) n += launch_step(ctx, P, as, md, it, STEP_GRAD, cst);
+        for (int it = lo; it <= hi; it++) {
+            n += launch_step(ctx, P, as, md, it, STEP_GRAD, cst);
+            n += grad_flush(P, P.all, ++nadj, false, cst);
+        }
         last_adj = as;
     }
     if (P.kind == KIND_ACOUSTIC) {
@@ -1698,30 +1870,38 @@ static long long capture_checkpointed(fwi2d_ctx *ctx, Plan &P, bool adj, cudaStr
     return n;
 }
 
-static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
+// Capture one pass as a CUDA graph: mode 0 the forward of every shot without
+// snapshots; mode 1 the forward with snapshots and mode 2 the adjoint of the
+// shots of wave `w`.
+static void capture(fwi2d_ctx *ctx, Plan &P, int mode, int w = 0)
 {
     const ModelState &M = ctx->M;
     const bool adj = mode == 2;
     const bool store = mode == 1;
+    const Plan::Wave &R = mode == 0 ? P.all : P.waves[w];
     cudaGraph_t g;
     // graphs are captured on the context's own stream and may be launched on any stream
     cudaStream_t cst = ctx->own;
     CK(cudaStreamSynchronize(ctx->st));
     CK(cudaStreamBeginCapture(cst, cudaStreamCaptureModeThreadLocal));
     long long n = 0;
-    for (auto &S : P.shots) {
+    for (int s = R.s0; s < R.s1; s++) {
+        ShotPlan *S = P.shots[s].get();
         CK(cudaMemsetAsync(S->u0.p, 0, S->u0.n, cst));
         CK(cudaMemsetAsync(S->u1.p, 0, S->u1.n, cst));
         if (adj) CK(cudaMemsetAsync(S->grad.p, 0, S->grad.n, cst));
+        if (adj && S->gcomp.p) CK(cudaMemsetAsync(S->gcomp.p, 0, S->gcomp.n, cst));
         if (store && S->amax.p) CK(cudaMemsetAsync(S->amax.p, 0, S->amax.n, cst));
         if (P.ae) {
             CK(cudaMemsetAsync(S->fluid->u0.p, 0, S->fluid->u0.n, cst));
             CK(cudaMemsetAsync(S->fluid->u1.p, 0, S->fluid->u1.n, cst));
         }
     }
+    // per-shot kernels take the wave's run of the shot tables; the step
+    // kernels take the whole tables (their units carry the shot numbers)
     const ShotDev *shots = (adj ? P.d_shots_a : P.d_shots_f).as<ShotDev>();
     const ShotDev *wshots = P.ae ? (adj ? P.d_wshots_a : P.d_wshots_f).as<ShotDev>() : nullptr;
-    const int nshots = (int)P.shots.size();
+    const int nshots = R.s1 - R.s0;
     const int im = adj ? 1 : 0;
     // acoustic-elastic: the initial injection goes to the fluid layer when the
     // source is in the water, else to the elastic grid, in both directions
@@ -1730,7 +1910,7 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
         launch_init_state(wshots, nshots, P.d_wicells[im].as<InitCell>(), P.d_wioff[im].as<int>(),
                           P.d_wiidx[im].as<int>(), cst);
     else
-        launch_init_state(shots, nshots, P.d_icells[im].as<InitCell>(), P.d_ioff[im].as<int>(),
+        launch_init_state(shots + R.s0, nshots, P.d_icells[im].as<InitCell>(), P.d_ioff[im].as<int>() + R.s0,
                           P.d_iidx[im].as<int>(), cst);
     n++;
     int flags = 0;
@@ -1747,27 +1927,37 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode)
     if (P.ckpt > 0 && (store || adj)) {
         n += capture_checkpointed(ctx, P, adj, cst);
     } else {
-        for (int it = 0; it < P.nt_max - 1; it++) n += launch_step(ctx, P, shots, md, it, flags, cst);
+        for (int it = 0; it < R.nt_max - 1; it++) {
+            n += launch_step(ctx, P, shots, md, it, flags, cst, &R);
+            if (adj) n += grad_flush(P, R, it + 1, false, cst);
+        }
         if (!adj) {
-            launch_finalize(shots, nshots, P.C, ncomp, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
+            launch_finalize(shots + R.s0, nshots, P.C, ncomp, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
             n++;
             if (P.ae) {
                 launch_finalize(wshots, nshots, P.Cw, 1, STEP_EXTRACT, cst);
                 n++;
             }
         } else if (P.kind == KIND_ACOUSTIC) {
-            launch_acoustic_final_grad(shots, nshots, md, P.C, P.dtg, cst);   // snapshot 0 with the last adjoint field
+            // snapshot 0 with the last adjoint field
+            launch_acoustic_final_grad(shots + R.s0, nshots, md, P.C, P.dtg, cst);
             n++;
         }
     }
+    if (adj) n += grad_flush(P, R, 0, true, cst);
     CK(cudaGetLastError());
     CK(cudaStreamEndCapture(cst, &g));
     cudaGraphExec_t ge;
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    P.graph[mode] = ge;
-    P.launches[mode] = n;
+    if (mode == 0) {
+        P.graph[0] = ge;
+        P.launches[0] = n;
+    } else {
+        P.waves[w].graph[mode - 1] = ge;
+        P.waves[w].launches[mode - 1] = n;
+    }
 }
 
 static Plan &need_plan(fwi2d_ctx *ctx)
@@ -1836,6 +2026,35 @@ static void upload_sources_axis(fwi2d_ctx *ctx, const float *traces)
     CK(cudaStreamSynchronize(ctx->st));   // the caller's traces may be reused on return
 }
 
+// One pass of wave w: the forward with snapshots, or the adjoint, which adds
+// the wave's shot gradients onto the model grid (wave 0 clears it first).
+static void run_wave(fwi2d_ctx *ctx, Plan &P, int w, bool adjoint)
+{
+    Plan::Wave &W = P.waves[w];
+    const int mode = adjoint ? 2 : 1;
+    if (!W.graph[mode - 1]) capture(ctx, P, mode, w);
+    const int e = adjoint ? 1 : 0;
+    if (!W.ev[e][0]) {
+        CK(cudaEventCreate(&W.ev[e][0]));
+        CK(cudaEventCreate(&W.ev[e][1]));
+    }
+    CK(cudaEventRecord(W.ev[e][0], ctx->st));
+    CK(cudaGraphLaunch(W.graph[mode - 1], ctx->st));
+    CK(cudaEventRecord(W.ev[e][1], ctx->st));
+    P.timed[e] = true;
+    if (!adjoint) P.fwd_waves = true;
+    queue_timeout_check(ctx, P);
+    if (adjoint) {
+        if (w == 0) CK(cudaMemsetAsync(P.d_grad_full.p, 0, P.d_grad_full.n, ctx->st));
+        for (int s = W.s0; s < W.s1; s++) {
+            const ShotPlan &S = *P.shots[s];
+            launch_add_subgrid(P.d_grad_full.as<float>(), S.grad.as<float>(), P.ncompg, S.x0, S.nx, ctx->M.ldz,
+                               (long long)ctx->M.nx * ctx->M.ldz, ctx->st);
+        }
+        CK(cudaGetLastError());
+    }
+}
+
 static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
 {
     Plan &P = need_plan(ctx);
@@ -1845,27 +2064,48 @@ static void run(fwi2d_ctx *ctx, bool adjoint, bool store)
             throw Error(FWI2D_ERR_STATE, "the adjoint needs a forward pass that stored snapshots (sub > 0)");
     }
     if (store && !P.have_snapshots) throw Error(FWI2D_ERR_ARG, "snapshots requested with sub = 0");
-    const int mode = adjoint ? 2 : (store ? 1 : 0);
-    if (!P.graph[mode]) capture(ctx, P, mode);
-    const int e = adjoint ? 1 : 0;
-    if (!P.ev[e][0]) {
-        CK(cudaEventCreate(&P.ev[e][0]));
-        CK(cudaEventCreate(&P.ev[e][1]));
+    if (adjoint || store) {
+        if (P.waves.size() != 1)
+            throw Error(FWI2D_ERR_UNSUPPORTED,
+                        "the snapshots of this plan's shots do not fit the device together: the plan runs in " +
+                            std::to_string(P.waves.size()) +
+                            " waves, which fwi2d_fwi_gradient drives (forward and adjoint of each wave in turn)");
+        run_wave(ctx, P, 0, adjoint);
+        if (store) P.snapshots_valid = true;
+        return;
     }
-    CK(cudaEventRecord(P.ev[e][0], ctx->st));
-    CK(cudaGraphLaunch(P.graph[mode], ctx->st));
-    CK(cudaEventRecord(P.ev[e][1], ctx->st));
-    P.timed[e] = true;
+    if (!P.graph[0]) capture(ctx, P, 0);
+    if (!P.ev[0][0]) {
+        CK(cudaEventCreate(&P.ev[0][0]));
+        CK(cudaEventCreate(&P.ev[0][1]));
+    }
+    CK(cudaEventRecord(P.ev[0][0], ctx->st));
+    CK(cudaGraphLaunch(P.graph[0], ctx->st));
+    CK(cudaEventRecord(P.ev[0][1], ctx->st));
+    P.timed[0] = true;
+    P.fwd_waves = false;
     queue_timeout_check(ctx, P);
-    if (adjoint) {
-        CK(cudaMemsetAsync(P.d_grad_full.p, 0, P.d_grad_full.n, ctx->st));
-        for (auto &S : P.shots)
-            launch_add_subgrid(P.d_grad_full.as<float>(), S->grad.as<float>(), P.ncompg, S->x0, S->nx, ctx->M.ldz,
-                               (long long)ctx->M.nx * ctx->M.ldz, ctx->st);
-        CK(cudaGetLastError());
-    } else if (store) {
-        P.snapshots_valid = true;
+}
+
+// Device time of the last forward (e = 0) or adjoint (e = 1) pass, summed
+// over the waves; -1 if none ran.
+static float pass_ms(Plan &P, int e)
+{
+    if (!P.timed[e]) return -1.f;
+    float total = 0.f;
+    if (e == 0 && !P.fwd_waves) {
+        CK(cudaEventSynchronize(P.ev[0][1]));
+        CK(cudaEventElapsedTime(&total, P.ev[0][0], P.ev[0][1]));
+        return total;
     }
+    for (auto &W : P.waves) {
+        if (!W.ev[e][0]) continue;
+        float ms = 0.f;
+        CK(cudaEventSynchronize(W.ev[e][1]));
+        CK(cudaEventElapsedTime(&ms, W.ev[e][0], W.ev[e][1]));
+        total += ms;
+    }
+    return total;
 }
 
 static void download_rcv(fwi2d_ctx *ctx, float *rcv)
@@ -2047,7 +2287,9 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
 {
     Plan &P = need_plan(ctx);
     REQ(P.d_obs.p != nullptr, "no observed data (fwi2d_set_observed)");
-    run(ctx, false, true);
+    set_device(ctx);
+    REQ(P.have_snapshots, "the FWI gradient needs snapshots (sub > 0)");
+    const int nsh = (int)P.shots.size();
     size_t rows_total = 0;
     for (auto &S : P.shots) rows_total += S->nrcv_rows;
     P.d_misfit.ensure(std::max<size_t>(rows_total, 1) * sizeof(double));
@@ -2057,12 +2299,14 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
     // the shots share one partial buffer: their kernels run in stream order and
     // each shot reduces its partials before the next shot writes them
     P.d_part.ensure(part_max * sizeof(float2));
-    size_t obs_off = 0, row_off = 0;
+    // observed-data and misfit-row offsets of every shot
+    std::vector<size_t> obs_off(nsh + 1, 0), row_off(nsh + 1, 0);
+    for (int k = 0; k < nsh; k++) {
+        const ShotPlan &S = *P.shots[k];
+        obs_off[k + 1] = obs_off[k] + (size_t)(P.dd > 0.f ? P.nd[k] : S.nt) * S.nrcv_rows;
+        row_off[k + 1] = row_off[k] + S.nrcv_rows;
+    }
     if (P.dd > 0.f) {
-        // data on their own axis: receivers -> alpha Dt -> adjoint resampling to
-        // the data axis; residual, misfit, Ht weighting there; resampling back,
-        // Ht^-1, reversal, -alpha, Dt^T (we_op.cpp:1030-1054, 1100-1124)
-        const float alpha = P.par.dt / P.dd;
         size_t mx = 1, pm = 1;
         for (size_t k = 0; k < P.shots.size(); k++) {
             mx = std::max(mx, (size_t)P.shots[k]->nrcv_rows * std::max(P.shots[k]->nt, P.nd[k]));
@@ -2071,8 +2315,15 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
         P.d_rs0.ensure(std::max(P.d_rs0.n, mx * sizeof(float)));
         P.d_rs1.ensure(std::max(P.d_rs1.n, mx * sizeof(float)));
         P.d_part.ensure(std::max(P.d_part.n, pm * sizeof(float2)));
-        for (size_t k = 0; k < P.shots.size(); k++) {
-            ShotPlan &S = *P.shots[k];
+    }
+    // residual, misfit rows and adjoint sources of shot k (after its forward)
+    auto residual = [&](int k) {
+        ShotPlan &S = *P.shots[k];
+        if (P.dd > 0.f) {
+            // data on their own axis: receivers -> alpha Dt -> adjoint resampling to
+            // the data axis; residual, misfit, Ht weighting there; resampling back,
+            // Ht^-1, reversal, -alpha, Dt^T (we_op.cpp:1030-1054, 1100-1124)
+            const float alpha = P.par.dt / P.dd;
             const int rows = S.nrcv_rows, nt = S.nt, nd = P.nd[k];
             const int neg = P.ae ? S.nr : 0;
             const int nchunk = (nd + kRsChunk - 1) / kRsChunk;
@@ -2082,32 +2333,32 @@ static void fwi_gradient(fwi2d_ctx *ctx, int seismotype, bool chain)
             k_resample_adj<<<dim3((nd + 127) / 128, rows), 128, 0, ctx->st>>>(r0, r1, nd, P.dd, nt, P.par.dt,
                                                                              P.rs_hl, P.rs_linear);
             k_residual_axis<<<dim3((rows + 127) / 128, nchunk), 128, 0, ctx->st>>>(
-                r1, P.d_obs.as<float>() + obs_off, r0, P.d_part.as<float2>(), rows, nd, P.dd);
+                r1, P.d_obs.as<float>() + obs_off[k], r0, P.d_part.as<float2>(), rows, nd, P.dd);
             k_misfit_rows<<<(rows + 127) / 128, 128, 0, ctx->st>>>(P.d_part.as<float2>(),
-                                                                  P.d_misfit.as<double>() + row_off, rows, nchunk);
+                                                                  P.d_misfit.as<double>() + row_off[k], rows, nchunk);
             k_resample_fwd<<<dim3((nt + 127) / 128, rows), 128, 0, ctx->st>>>(r0, r1, nd, P.dd, nt, P.par.dt,
                                                                              P.rs_hl, P.rs_linear);
             k_adjoint_source_axis<<<dim3((rows + 127) / 128, nt), 128, 0, ctx->st>>>(
                 r1, S.src_a.as<float>(), rows, nt, P.par.dt, alpha, seismotype, neg);
-            CK(cudaGetLastError());
-            obs_off += (size_t)nd * rows;
-            row_off += rows;
+        } else {
+            const int nchunk = (S.nt + kResChunk - 1) / kResChunk;
+            dim3 grid((S.nrcv_rows + 127) / 128, nchunk);
+            k_residual<<<grid, 128, 0, ctx->st>>>(S.rcv_f.as<float>(), P.d_obs.as<float>() + obs_off[k],
+                                                  S.src_a.as<float>(), nullptr, P.d_part.as<float2>(), S.nt,
+                                                  S.nrcv_rows, P.par.dt, seismotype, P.ae ? S.nr : 0);
+            k_misfit_rows<<<(S.nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
+                P.d_part.as<float2>(), P.d_misfit.as<double>() + row_off[k], S.nrcv_rows, nchunk);
         }
-    } else {
-        for (auto &S : P.shots) {
-            const int nchunk = (S->nt + kResChunk - 1) / kResChunk;
-            dim3 grid((S->nrcv_rows + 127) / 128, nchunk);
-            k_residual<<<grid, 128, 0, ctx->st>>>(S->rcv_f.as<float>(), P.d_obs.as<float>() + obs_off,
-                                                  S->src_a.as<float>(), nullptr, P.d_part.as<float2>(), S->nt,
-                                                  S->nrcv_rows, P.par.dt, seismotype, P.ae ? S->nr : 0);
-            k_misfit_rows<<<(S->nrcv_rows + 127) / 128, 128, 0, ctx->st>>>(
-                P.d_part.as<float2>(), P.d_misfit.as<double>() + row_off, S->nrcv_rows, nchunk);
-            CK(cudaGetLastError());
-            obs_off += (size_t)S->nt * S->nrcv_rows;
-            row_off += S->nrcv_rows;
-        }
+        CK(cudaGetLastError());
+    };
+    // wave by wave: forward with snapshots, residuals, adjoint (the waves
+    // share the snapshot store; one wave when every shot fits)
+    for (int w = 0; w < (int)P.waves.size(); w++) {
+        run_wave(ctx, P, w, false);
+        for (int k = P.waves[w].s0; k < P.waves[w].s1; k++) residual(k);
+        run_wave(ctx, P, w, true);
     }
-    run(ctx, true, false);
+    P.snapshots_valid = P.waves.size() == 1;
     if (chain) {
         const ModelState &M = ctx->M;
         const SbpTables &t = sbp_tables();
@@ -2213,7 +2464,7 @@ static void load_host_snapshots(fwi2d_ctx *ctx, const float *full)
     for (int k = 0; k < S.nslot; k++) {
         CK(cudaMemcpyAsync(P.d_stage.p, full + (size_t)k * slot_in, slot_in * sizeof(float), cudaMemcpyHostToDevice,
                            ctx->st));
-        k_pitch<<<592, 256, 0, ctx->st>>>(P.d_stage.as<float>(), S.snap.as<float>() + (size_t)k * slot_out,
+        k_pitch<<<592, 256, 0, ctx->st>>>(P.d_stage.as<float>(), (float *)S.snap_base + (size_t)k * slot_out,
                                           (long long)rows, M.nz, M.ldz);
         CK(cudaGetLastError());
     }
@@ -2232,7 +2483,7 @@ static void store_host_snapshots(fwi2d_ctx *ctx, float *full)
     // the reference writes slots it/sub for it in [0, nt-1]; later slots stay untouched
     const int written = (S.nt - 1) / P.C.sub + 1;
     for (int k = 0; k < std::min(written, S.nslot); k++) {
-        k_unpitch<<<592, 256, 0, ctx->st>>>(S.snap.as<float>() + (size_t)k * slot_in, P.d_stage.as<float>(),
+        k_unpitch<<<592, 256, 0, ctx->st>>>((const float *)S.snap_base + (size_t)k * slot_in, P.d_stage.as<float>(),
                                             (long long)rows, M.nz, M.ldz);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(full + (size_t)k * slot_out, P.d_stage.p, slot_out * sizeof(float), cudaMemcpyDeviceToHost,
@@ -2427,13 +2678,14 @@ int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out)
     ShotPlan &S = *P.shots[shot];
     REQ(P.have_snapshots && slot >= 0 && slot < S.nslot, "no such snapshot");
     REQ(P.ckpt == 0, "snapshots are recomputed segment by segment under checkpointing and are not kept");
+    REQ(P.waves.size() == 1, "the plan runs its shots in waves that share one snapshot store");
     set_device(ctx);
     const ModelState &M = ctx->M;
     const size_t field = (size_t)S.ncomp * S.nx * M.ldz;
     const int prec = P.par.snapshot_precision;
     const size_t esz = prec == FWI2D_SNAP_FP32 ? 4 : 2;
     std::vector<unsigned char> raw(field * esz);
-    CK(cudaMemcpyAsync(raw.data(), (const char *)S.snap.p + (size_t)slot * field * esz, field * esz,
+    CK(cudaMemcpyAsync(raw.data(), (const char *)S.snap_base + (size_t)slot * field * esz, field * esz,
                        cudaMemcpyDeviceToHost, ctx->st));
     unsigned amax = 0;
     if (prec != FWI2D_SNAP_FP32)
@@ -2478,14 +2730,22 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     ABI_TRY
     REQ(ctx, "null context");
     Plan &P = need_plan(ctx);
-    const long long steps = P.nt_max - 1;
     const long long per = (P.march || P.framed || P.ae) ? 3 : 1;
     const long long nseg = P.ckpt > 0 ? (long long)P.cuts.size() - 1 : 0;
     const long long acf = P.kind == KIND_ACOUSTIC ? 1 : 0;
-    // forward: init, steps, last sample (+ checkpoint copies); adjoint: init, steps,
-    // acoustic final imaging, per-shot scatter (+ replays: restore, steps, last snapshot)
-    if (lf) *lf = steps * per + 2 + (P.ae ? 1 : 0) + (nseg > 0 ? nseg - 1 : 0);
-    if (la) *la = steps * per + 1 + acf + (long long)P.shots.size() + (nseg > 0 ? (steps + nseg - 1) * per + 2 * nseg : 0);
+    // per wave -- forward: init, steps, last sample (+ checkpoint copies);
+    // adjoint: init, steps, acoustic final imaging, per-shot scatter (+ replays:
+    // restore, steps, last snapshot) and, with compensated accumulation, one
+    // window flush per kCompWindow adjoint launches plus the final one
+    long long f = 0, a = 0;
+    for (const auto &W : P.waves) {
+        const long long steps = W.nt_max - 1;
+        f += steps * per + 2 + (P.ae ? 1 : 0) + (nseg > 0 ? nseg - 1 : 0);
+        const long long flushes = P.par.compensated && P.par.sub > 0 ? steps / kCompWindow + 1 : 0;
+        a += steps * per + 1 + acf + (W.s1 - W.s0) + (nseg > 0 ? (steps + nseg - 1) * per + 2 * nseg : 0) + flushes;
+    }
+    if (lf) *lf = f;
+    if (la) *la = a;
     if (shape) *shape = P.shape;
     if (snap_bytes) *snap_bytes = P.snap_bytes;
     ABI_END
@@ -2520,14 +2780,8 @@ int fwi2d_last_timing(fwi2d_ctx *ctx, float *forward_ms, float *adjoint_ms)
     Plan &P = need_plan(ctx);
     set_device(ctx);
     float *out[2] = {forward_ms, adjoint_ms};
-    for (int e = 0; e < 2; e++) {
-        if (!out[e]) continue;
-        *out[e] = -1.f;
-        if (P.timed[e]) {
-            CK(cudaEventSynchronize(P.ev[e][1]));
-            CK(cudaEventElapsedTime(out[e], P.ev[e][0], P.ev[e][1]));
-        }
-    }
+    for (int e = 0; e < 2; e++)
+        if (out[e]) *out[e] = pass_ms(P, e);
     ABI_END
 }
 

@@ -69,7 +69,7 @@ struct ShotDev {
     float *snap_inv;      // per-slot dequantisation factor (16-bit snapshots)
     unsigned *snap_amax;  // per-slot max |u| bits (16-bit snapshots)
     float *grad;          // [3 or 2][nx][ldz] gradient accumulator of this shot
-    float *gcomp;         // compensation terms (compensated accumulation) or nullptr
+    float *gcomp;         // compensated accumulation: running sum pair hi [3 or 2][nx][ldz], then lo; or nullptr
     float *halo_save;     // interface scratch (acoustic-elastic) or nullptr
     const float *gwt;     // gradient time-damping weight per snapshot index
     float *ckpt;          // checkpoints [k][2][ncomp][nx][ldz] (checkpoint-and-recompute) or nullptr
@@ -101,7 +101,6 @@ struct StepConst {
     int sub;
     int snap_prec;
     int nslot;
-    int kahan;                   // compensated gradient accumulation
     int spin;                    // poll limit of each bounded device wait (marching kernel)
 };
 

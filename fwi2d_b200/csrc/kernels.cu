@@ -1041,6 +1041,7 @@ void elastic_tile_shape(int i, int *tz, int *tx)
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
+    if (ntiles <= 0) return;
     switch (shape) {
     case 0: vti ? launch_elastic_t<true, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
                 : launch_elastic_t<false, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;

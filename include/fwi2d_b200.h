@@ -67,7 +67,11 @@ typedef struct fwi2d_params {
     /* library options */
     int snapshot_precision;                                /* FWI2D_SNAP_* */
     int checkpoint_every;                                  /* 0: keep snapshots; k>0: recompute from checkpoints every k steps */
-    int compensated;                                       /* compensated (two-level) gradient accumulation */
+    int compensated;                                       /* 1: compensated (two-level) gradient accumulation: the
+                                                            * imaging terms of 8 adjoint steps are summed in FP32,
+                                                            * each such partial sum joins a running (hi, lo) pair by
+                                                            * Neumaier's compensated summation; 0: the reference's
+                                                            * plain FP32 accumulation (bitwise) */
     int tile_shape;                                        /* -1: autotuned; else fwi2d_tile_shape index */
 } fwi2d_params;
 

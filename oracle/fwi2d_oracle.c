@@ -820,6 +820,30 @@ static real gdamp_weight(const orc_param *par, int it, real dtg)
     return w;
 }
 
+/* Test switch, not the reference's behaviour: with g_exact_sum set, the
+ * elastic / VTI imaging condition adds each time sample's terms (computed
+ * exactly as below) into a double array, rounded to real once at the end of
+ * the propagation: the exact sum of the same single-precision terms, against
+ * which the tests measure the summation error of the device's plain and
+ * compensated gradient accumulations.  Off by default. */
+static int g_exact_sum = 0;
+static double *g_xsum = NULL;   /* [3][nxz] while an exact-sum adjoint runs */
+
+void ORC(set_exact_gradient_sum)(int on) { g_exact_sum = on != 0; }
+
+/* g[i] += term in real arithmetic, or the term into the exact sum */
+static inline void acc_r(real *g, double *x, long i, real term)
+{
+    if (x) x[i] += (double)term;
+    else g[i] += term;
+}
+/* g[i] = (real)((double)g[i] + term), or the term into the exact sum */
+static inline void acc_d(real *g, double *x, long i, double term)
+{
+    if (x) x[i] += term;
+    else g[i] = (real)((double)g[i] + term);
+}
+
 /* nl_we_op_e::compute_gradients (we_op.cpp:505-562) and the VTI variant
  * (we_op.cpp:1478-1557).  m: converted model; ufull [nsnap][2][nxz]. */
 static void grad_elastic(int vti, const real *m, const real *ufull, const real *adj, const real *ax, const real *az,
@@ -840,6 +864,7 @@ static void grad_elastic(int vti, const real *m, const real *ufull, const real *
     const real *fp0 = it + 1 <= last ? f0 + 2 * nxz : NULL, *fp1 = fp0 ? fp0 + nxz : NULL;
     const real *fm0 = it > 0 ? f0 - 2 * nxz : NULL, *fm1 = fm0 ? fm0 + nxz : NULL;
     real *g0 = g, *g1 = g + nxz, *g2 = g + 2 * nxz;
+    double *x0 = g_xsum, *x1 = g_xsum ? g_xsum + nxz : NULL, *x2 = g_xsum ? g_xsum + 2 * nxz : NULL;
     OMP_FOR
     for (long i = 0; i < nxz; i++) {
         real dl, dm;
@@ -856,21 +881,21 @@ static void grad_elastic(int vti, const real *m, const real *ufull, const real *
                + v3 * (ax0[i] * t1[i] + az1[i] * t0[i]);
         }
         if (it > 0 && it < last) {
-            if (!vti) { g0[i] += w * dtg * (ax0[i] + az1[i]) * (t0[i] + t1[i]); }
-            else g0[i] += w * dtg * dl;
-            g1[i] += w * dtg * dm;
-            g2[i] = (real)((double)g2[i] + (double)w * 1.0 / (double)dtg
+            if (!vti) acc_r(g0, x0, i, w * dtg * (ax0[i] + az1[i]) * (t0[i] + t1[i]));
+            else acc_r(g0, x0, i, w * dtg * dl);
+            acc_r(g1, x1, i, w * dtg * dm);
+            acc_d(g2, x2, i, (double)w * 1.0 / (double)dtg
                   * (double)(a0[i] * (fp0[i] - 2 * f0[i] + fm0[i]) + a1[i] * (fp1[i] - 2 * f1[i] + fm1[i])));
         } else if (it == 0) {
-            g0[i] = (real)((double)g0[i] + (double)w * 0.5 * (double)dtg * (double)(vti ? dl : (ax0[i] + az1[i])) * (double)(vti ? 1 : (t0[i] + t1[i])));
-            g1[i] = (real)((double)g1[i] + (double)w * 0.5 * (double)dtg * (double)dm);
-            g2[i] = (real)((double)g2[i] + (double)w * 1.0 / (double)dtg
+            acc_d(g0, x0, i, (double)w * 0.5 * (double)dtg * (double)(vti ? dl : (ax0[i] + az1[i])) * (double)(vti ? 1 : (t0[i] + t1[i])));
+            acc_d(g1, x1, i, (double)w * 0.5 * (double)dtg * (double)dm);
+            acc_d(g2, x2, i, (double)w * 1.0 / (double)dtg
                   * (double)(a0[i] * (fp0[i] - f0[i]) + a1[i] * (fp1[i] - f1[i])));
         } else {
-            if (!vti) { g0[i] += w * dtg * (ax0[i] + az1[i]) * (t0[i] + t1[i]); }
-            else g0[i] += w * dtg * dl;
-            g1[i] += w * dtg * dm;
-            g2[i] = (real)((double)g2[i] + (double)w * 1.0 / (double)dtg
+            if (!vti) acc_r(g0, x0, i, w * dtg * (ax0[i] + az1[i]) * (t0[i] + t1[i]));
+            else acc_r(g0, x0, i, w * dtg * dl);
+            acc_r(g1, x1, i, w * dtg * dm);
+            acc_d(g2, x2, i, (double)w * 1.0 / (double)dtg
                   * (double)(a0[i] * (-f0[i] + fm0[i]) + a1[i] * (-f1[i] + fm1[i])));
         }
     }
@@ -928,6 +953,7 @@ static void propagate_elastic(int vti, int adj, const real *model, const real *a
     real *prev = u, *curr = u + 2 * nxz, *next = u + 4 * nxz;
     const real *lam = model, *mu = model + nxz, *rho = model + 2 * nxz;
     const real *c13 = vti ? model + 3 * nxz : NULL, *eps = vti ? model + 4 * nxz : NULL;
+    g_xsum = grad && g_exact_sum ? (double *)calloc(3 * nxz, sizeof(double)) : NULL;
 
     /* coefficient fields of the variable-coefficient operators */
     real *f2mu = (real *)malloc(nxz * sizeof(real));
@@ -1038,6 +1064,11 @@ static void propagate_elastic(int vti, int adj, const real *model, const real *a
         extract(ext, curr + nxz, rcvz, nz, nt, nt - 1);
     }
     if (grad) grad_elastic(vti, model, full, curr, dux, duz, tmp, grad, par, nx, nz, 0, dx, dz, sub * dt);
+    if (g_xsum) {
+        for (long i = 0; i < 3 * nxz; i++) grad[i] = (real)((double)grad[i] + g_xsum[i]);
+        free(g_xsum);
+        g_xsum = NULL;
+    }
 
     free(u); free(dux); free(duz); free(tmp); free(tmp1);
     free(f2mu); free(fxx); free(fimp_s); free(fimp_p);
