@@ -8,13 +8,22 @@ snapshot storage, residual against observed data, adjoint sources, adjoint
 propagation with the zero-lag imaging condition, H quadrature and chain rule.
 Cell-updates per step: (nt-1) * nx * nz forward + the same adjoint.
 
-At N = 1 the line also carries "batched": the same evaluation for a batch of
-32 shots of the batch geometry (every other shot of the 64-shot line, cropped
-grids of 1.0-3.5 km apertures, 1.2-2.0 s records) on the elastic model with
-FP16 snapshots, all shots in one plan, timed the same way.  It also carries
-"reference_gpu": the reference's own GPU implementation (src/cuda, built for
-sm_100a into oracle/_ref by oracle/build_ref.sh) timed on a bounded sample of
-the same shot, with "e2e_speedup" = this library's end-to-end value over it.
+At N = 1 the line also carries:
+* "batched": the batched VTI configuration as written -- 64 shots 60 m apart
+  on cropped grids (1.0-3.5 km apertures, 1.2-2.0 s records), VTI model,
+  FP32 snapshots -- in one plan on one GPU.  Its snapshots (about 430 GB) do
+  not fit the device, so the plan runs its shots in HBM-sized waves, each
+  wave a CUDA graph, the gradient summed over all shots;
+* "large": 4 shots of the large-grid configuration (1201 x 4001 at 2.5 m,
+  nt = 16001), FP16 snapshots rebuilt by checkpoint-and-recompute every 200
+  steps, with the 32-shot time projected from it;
+* "fp64_error" on each of them: trace and gradient error against the
+  reference's FP64 build (oracle/_ref) on a bounded sample of the same
+  geometry (FP32, and for the large grid also BF16 and FP16 snapshots);
+* "reference_gpu": the reference's own GPU implementation (src/cuda, built
+  for sm_100a into oracle/_ref by oracle/build_ref.sh) timed on a bounded
+  sample of the same shot, with "e2e_speedup" = this library's end-to-end
+  value over it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config single|batch|large]
 
@@ -42,6 +51,7 @@ sys.path.insert(0, ROOT)
 METRIC = "elastic FWI gradient shots/s + Gcell-updates/s, batched vs plain, 1 B200"
 BYTES_FWD = 36 + 8      # algorithmic bytes per forward cell-update (fields, model, fp32 snapshot store)
 BYTES_ADJ = 68          # adjoint + imaging: fields, model, snapshot read, gradient read-modify-write
+VTI_EXTRA = 8           # VTI reads c13 and eps as well
 
 
 def parse():
@@ -53,6 +63,7 @@ def parse():
     ap.add_argument("--config", default="single", choices=["single", "batch", "large"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     return ap.parse_args()
 
 
@@ -193,6 +204,63 @@ def observed(wl, device, srcs):
 def cells_per_step(wl):
     nz = wl["nz"]
     return sum(2 * (s["nt"] - 1) * s["nx"] * nz for s in wl["shots"])
+
+
+def fp64_error(kind, mc, nz, d, shot, params, src, nt, device, precs=(0,), checkpoint_every=0, tile_shape=3):
+    """Error of this library against the reference's FP64 build (oracle/_ref,
+    the reference's sources with DOUBLE_PRECISION) on a bounded sample of one
+    shot: its cropped grid, nt time samples.  Forward traces, then the adjoint
+    imaging condition with the FP64 traces reversed in time as adjoint
+    sources, for each snapshot precision in precs.  Returns a dict of relative
+    L2 errors."""
+    import oracle as O
+    import fwi2d_b200 as F
+    if not O.have_reference(64):
+        return {"unavailable": "the reference FP64 build (oracle/_ref) is absent"}
+    ref = O.Reference(64)
+    x0, nx = shot["x0"], shot["nx"]
+    mcs = np.ascontiguousarray(mc[:, x0:x0 + nx])
+    ox = np.float32(x0 * d)
+    sx, sz = np.array(shot["sx"], np.float32) - ox, np.array(shot["sz"], np.float32)
+    rx, rz = np.asarray(shot["rx"], np.float32) - ox, np.asarray(shot["rz"], np.float32)
+    nr = len(rx)
+    src_s = np.ascontiguousarray(src[:, :, :nt])
+    keys = ("sub", "dt", "bc_top", "bc_bottom", "bc_left", "bc_right", "taper_top", "taper_bottom", "taper_left",
+            "taper_right", "taper_strength")
+    par = O.make_par(**{k: params[k] for k in keys}, nt=nt, ns=1, nr=nr)
+    m64 = mcs.astype(np.float64)
+    rcv64 = np.zeros((2, nr, nt), np.float64)
+    full64 = np.zeros((nt + 1, 2, nx, nz), np.float64)
+    ref.propagate(kind, 0, m64, src_s.astype(np.float64), rcv64, par, nx, nz, d, d, 0.0, 0.0, (sx, sz), (rx, rz),
+                  full=full64)
+    adj = np.ascontiguousarray(rcv64[:, :, ::-1] / max(np.abs(rcv64).max(), 1e-30)).astype(np.float32)
+    g64 = np.zeros((5 if kind == 1 else 3, nx, nz), np.float64)
+    ref.propagate(kind, 1, m64, adj.astype(np.float64), np.zeros((2, 1, nt)), par, nx, nz, d, d, 0.0, 0.0,
+                  (rx, rz), (sx, sz), full=full64, grad=g64)
+    del full64
+
+    def rel(a, b):
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm((np.asarray(a, np.float64) - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+    out = {"sample": "shot grid %d x %d, %d time samples; adjoint sources: the FP64 traces reversed in time"
+                     % (nz, nx, nt)}
+    names = {0: "fp32", 1: "bf16", 2: "fp16"}
+    for prec in precs:
+        P = F.Propagator(device)
+        P.set_model(kind, mcs, d, d)
+        prm = {k: params[k] for k in keys}
+        prm.update(nt=nt, snapshot_precision=prec, checkpoint_every=checkpoint_every if nt > checkpoint_every else 0,
+                   tile_shape=tile_shape)
+        P.set_shots(F.make_params(**prm), [F.ShotSpec(0, nx, nt, sx, sz, rx, rz)])
+        rcv = P.forward([src_s], store=True)[0]
+        g = P.adjoint([adj])
+        P.close()
+        e = {"gradient": [rel(g[c], g64[c]) for c in range(3)]}
+        if prec == precs[0]:
+            out["traces"] = rel(rcv, rcv64)
+        out[names[prec]] = e
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -449,6 +517,12 @@ def run_ours(args):
                          "forward_achieved": BYTES_FWD * cells_launch / fwd_launch_s / 1e9},
             "clocks": clocks,
         }
+        if world == 1 and args.config == "single":
+            try:
+                line["fp64_error"] = fp64_error(wl["kind"], start, wl["nz"], wl["d"], wl["shots"][0], wl["params"],
+                                                wl["src"], 500, local, tile_shape=info["tile_shape"])
+            except Exception as e:   # never blocks the main line
+                line["fp64_error"] = {"unavailable": "failed: %s" % e}
         if world == 1 and args.config == "single" and not args.no_batched:
             try:
                 b = run_batched(local, 2, 1)
@@ -457,6 +531,11 @@ def run_ours(args):
                 line["batched"] = b
             except Exception as e:   # the batched leg never blocks the main line
                 line["batched"] = {"error": str(e)}
+        if world == 1 and args.config == "single" and not args.no_large:
+            try:
+                line["large"] = run_large(local)
+            except Exception as e:   # the large-grid leg never blocks the main line
+                line["large"] = {"error": str(e)}
         if world == 1 and args.config == "single":
             try:
                 rg = reference_gpu_sample(wl)
@@ -483,13 +562,15 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
-def run_batched(local, steps, warmup):
-    """Batched elastic gradients (FP16 snapshots) on one GPU; returns a dict."""
+def timed_gradients(wl, local, steps, warmup, tile_shape=None):
+    """FWI gradients of a workload on one GPU, device-resident inputs; returns
+    (ms per gradient, forward ms, adjoint ms, plan info, waves, snapshot bytes
+    of all shots)."""
     import torch
     import fwi2d_b200 as F
-    from fwi2d_b200 import workloads as W
     from fwi2d_b200 import _capi as C
-    wl = W.elastic_batch(every=2)
+    if tile_shape is not None:
+        wl = dict(wl, params=dict(wl["params"], tile_shape=tile_shape))
     P, start, srcs = make_prop(wl, local)
     obs = observed(wl, local, srcs)
     stream = torch.cuda.Stream()
@@ -515,25 +596,75 @@ def run_batched(local, steps, warmup):
     ms = ev0.elapsed_time(ev1) / steps
     fwd_ms, adj_ms = P.last_timing()
     info = P.plan_info()
+    nwaves, snap_all = P.plan_waves()
     P.close()
+    return ms, fwd_ms, adj_ms, info, nwaves, snap_all
+
+
+def run_batched(local, steps, warmup):
+    """The batched VTI configuration (64 shots, cropped grids, uneven records,
+    FP32 snapshots) on one GPU; returns a dict."""
+    from fwi2d_b200 import workloads as W
+    wl = W.vti_batch()
+    ms, fwd_ms, adj_ms, info, nwaves, snap_all = timed_gradients(wl, local, steps, warmup)
     cells = cells_per_step(wl)
-    # average algorithmic HBM bandwidth of each time loop: FP16 snapshots,
-    # 36 + 4 B per forward cell-update, 68 - 4 B per adjoint one
+    # average algorithmic HBM bandwidth of each time loop (VTI, FP32 snapshots)
     peak, peak_kind = peaks()
     half = cells / 2
-    fwd_gbs = 40 * half / (fwd_ms / 1e3) / 1e9
-    adj_gbs = 64 * half / (adj_ms / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel": "elastic_march + band kernels (adjoint + imaging)", "achieved": adj_gbs,
+    fwd_gbs = (BYTES_FWD + VTI_EXTRA) * half / (fwd_ms / 1e3) / 1e9
+    adj_gbs = (BYTES_ADJ + VTI_EXTRA) * half / (adj_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": "elastic_march<VTI> + band kernels (adjoint + imaging)", "achieved": adj_gbs,
             "peak": peak, "unit": "GB/s", "frac": adj_gbs / peak, "peak_source": peak_kind,
+            "bytes_per_cell_update": {"forward": BYTES_FWD + VTI_EXTRA, "adjoint": BYTES_ADJ + VTI_EXTRA},
             "forward_achieved": fwd_gbs, "forward_frac": fwd_gbs / peak}
-    return {"workload": "elastic FWI gradient, %d shots of the batch geometry on cropped grids (mean %d x %d cells, "
-                        "mean nt %d), FP16 snapshots" % (len(wl["shots"]),
-                                                          np.mean([s["nx"] for s in wl["shots"]]), wl["nz"],
-                                                          np.mean([s["nt"] for s in wl["shots"]])),
-            "shots": len(wl["shots"]), "ms_per_step": ms, "shots_per_s": len(wl["shots"]) / (ms / 1e3),
-            "value": cells / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "cell_updates_per_step": cells,
-            "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "tile_shape": info["tile_shape"], "roofline": roof,
-            "snapshot_bytes": info["snapshot_bytes"], "steps": steps, "warmup": warmup}
+    out = {"workload": "VTI FWI gradient, %d shots of the batch geometry on cropped grids (mean %d x %d cells, "
+                       "mean nt %d), FP32 snapshots" % (len(wl["shots"]), np.mean([s["nx"] for s in wl["shots"]]),
+                                                         wl["nz"], np.mean([s["nt"] for s in wl["shots"]])),
+           "shots": len(wl["shots"]), "ms_per_step": ms, "shots_per_s": len(wl["shots"]) / (ms / 1e3),
+           "value": cells / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "cell_updates_per_step": cells,
+           "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "tile_shape": info["tile_shape"], "roofline": roof,
+           "waves": nwaves, "snapshot_bytes_all_shots": snap_all, "snapshot_bytes_held": info["snapshot_bytes"],
+           "steps": steps, "warmup": warmup}
+    try:
+        from fwi2d_b200 import workloads as W2
+        sh = wl["shots"][0]
+        out["fp64_error"] = fp64_error(wl["kind"], W2.convert(wl["kind"], wl["start"]), wl["nz"], wl["d"], sh,
+                                       wl["params"], wl["src"], 500, local)
+    except Exception as e:
+        out["fp64_error"] = {"unavailable": "failed: %s" % e}
+    return out
+
+
+# autotuner's choice for the large-grid workload (marching units of 224 z
+# cells x 32 rows), pinned so that the bench does not rerun the tuner's
+# whole-pass stage, whose passes take tens of seconds on this grid
+LARGE_TILE_SHAPE = 8
+
+
+def run_large(local, nshots=4):
+    """4 shots of the large-grid configuration (FP16 snapshots rebuilt by
+    checkpoint-and-recompute every 200 steps) on one GPU; returns a dict."""
+    from fwi2d_b200 import workloads as W
+    wl = W.elastic_large(nshots=nshots)
+    ms, fwd_ms, adj_ms, info, nwaves, _ = timed_gradients(wl, local, 1, 1, tile_shape=LARGE_TILE_SHAPE)
+    cells = cells_per_step(wl)
+    out = {"workload": "elastic FWI gradient, %d shots of the 1201 x 4001 grid at 2.5 m, nt = 16001, FP16 "
+                       "snapshots rebuilt by checkpoint-and-recompute every 200 steps" % nshots,
+           "shots": nshots, "ms_per_step": ms, "shots_per_s": nshots / (ms / 1e3),
+           "value": cells / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s", "cell_updates_per_step": cells,
+           "recompute": "the adjoint loop replays each 200-step segment; replayed steps are not counted",
+           "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "tile_shape": info["tile_shape"],
+           "projected_32_shots_s": 32 * ms / nshots / 1e3, "steps": 1, "warmup": 1}
+    try:
+        # a crop of the large grid: 201 x 601 cells at 2.5 m, Ricker 15 Hz, dt 0.2 ms, 1201 samples
+        crop = dict(wl["shots"][0], x0=0, nx=601, sx=[0.75], rx=(0.0125 * (1 + np.arange(46))).astype(np.float32),
+                    rz=np.full(46, 0.01, np.float32))
+        mc = W.convert(wl["kind"], wl["start"])[:, :601, :201]
+        out["fp64_error"] = fp64_error(wl["kind"], mc, 201, wl["d"], crop, wl["params"], wl["src"], 1201, local,
+                                       precs=(0, 1, 2), checkpoint_every=200)
+    except Exception as e:
+        out["fp64_error"] = {"unavailable": "failed: %s" % e}
+    return out
 
 
 def main():

@@ -21,7 +21,7 @@ SYMBOLS = [
     "fwi2d_sync", "fwi2d_snapshot", "fwi2d_plan_info", "fwi2d_tile_shape_count", "fwi2d_tile_shape",
     "fwi2d_propagate", "fwi2d_update_model", "fwi2d_set_observed", "fwi2d_fwi_gradient", "fwi2d_last_timing",
     "fwi2d_set_stream", "fwi2d_copy_gradient", "fwi2d_set_data_axis", "fwi2d_resample", "fwi2d_propagate_noalloc",
-    "fwi2d_noalloc_last_error", "fwi2d_analyze_model", "fwi2d_dipole_weights",
+    "fwi2d_noalloc_last_error", "fwi2d_analyze_model", "fwi2d_dipole_weights", "fwi2d_plan_waves",
 ]
 
 RESAMPLE_SINC, RESAMPLE_LINEAR = 0, 1
@@ -114,6 +114,7 @@ def load(build_if_missing=False):
     L.fwi2d_resample.argtypes = [i, i, i, i, i, f, i, f, vp, vp]
     L.fwi2d_dipole_weights.argtypes = [i, vp, vp, vp, f, i, i, f, f, f, f, vp, vp, vp, vp]
     L.fwi2d_analyze_model.argtypes = [i, vp, i, i, f, f, i, f, ctypes.POINTER(ModelCheck)]
+    L.fwi2d_plan_waves.argtypes = [vp, vp, vp]
     _lib = L
     return L
 

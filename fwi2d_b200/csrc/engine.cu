@@ -2751,6 +2751,20 @@ int fwi2d_plan_info(fwi2d_ctx *ctx, long long *lf, long long *la, int *shape, lo
     ABI_END
 }
 
+int fwi2d_plan_waves(fwi2d_ctx *ctx, int *nwaves, long long *snapshot_bytes_all)
+{
+    ABI_TRY
+    REQ(ctx, "null context");
+    Plan &P = need_plan(ctx);
+    if (nwaves) *nwaves = (int)P.waves.size();
+    if (snapshot_bytes_all) {
+        long long b = 0;
+        for (auto &S : P.shots) b += (long long)S->snap_need;
+        *snapshot_bytes_all = b;
+    }
+    ABI_END
+}
+
 int fwi2d_set_stream(fwi2d_ctx *ctx, void *stream)
 {
     ABI_TRY

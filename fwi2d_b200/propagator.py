@@ -316,6 +316,12 @@ class Propagator:
         C.check(self.L.fwi2d_last_timing(self.h, ctypes.byref(f), ctypes.byref(a)))
         return f.value, a.value
 
+    def plan_waves(self):
+        """(number of waves, snapshot bytes of all shots together)."""
+        n, b = ctypes.c_int(), ctypes.c_longlong()
+        C.check(self.L.fwi2d_plan_waves(self.h, ctypes.byref(n), ctypes.byref(b)))
+        return n.value, b.value
+
     def plan_info(self):
         lf, la, sh, sb = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int(), ctypes.c_longlong()
         C.check(self.L.fwi2d_plan_info(self.h, ctypes.byref(lf), ctypes.byref(la), ctypes.byref(sh), ctypes.byref(sb)))

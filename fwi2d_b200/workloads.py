@@ -101,13 +101,14 @@ def elastic_single(nt=5001):
                 shots=[dict(x0=0, nx=nx, sx=[2.0], sz=[0.01], rx=rx, rz=rz, nt=nt)], params=params, seismotype=1)
 
 
-def elastic_large(nt=16001, checkpoint_every=200, snapshot_precision=C.SNAP_FP16):
+def elastic_large(nt=16001, checkpoint_every=200, snapshot_precision=C.SNAP_FP16, nshots=1):
     """Large-grid elastic gradient workload: 1201 x 4001 cells at 2.5 m, Ricker
-    15 Hz, dt = 0.2 ms, nt = 16001, one shot at x = 5 km with 798 two-component
-    receivers every 12.5 m at 10 m depth.  The perturbation of the true model
-    is smoothed over 50 m (20 cells), the starting model over 125 m (50 cells).
-    Snapshots are 16-bit, rebuilt by checkpoint-and-recompute every 200 steps
-    (the FP32 snapshots of one shot would take 615 GB)."""
+    15 Hz, dt = 0.2 ms, nt = 16001, shots at x = 5 km (one shot) or spread
+    over 1-9 km (nshots > 1), each with 798 two-component receivers every
+    12.5 m at 10 m depth on the whole grid.  The perturbation of the true
+    model is smoothed over 50 m (20 cells), the starting model over 125 m
+    (50 cells).  Snapshots are 16-bit, rebuilt by checkpoint-and-recompute
+    every 200 steps (the FP32 snapshots of one shot would take 615 GB)."""
     nx, nz, d, dt = 4001, 1201, 0.0025, 2e-4
     true = elastic_model(nx, nz, d, sigma_cells=20)
     start = smoothed(true, 50)
@@ -119,8 +120,10 @@ def elastic_large(nt=16001, checkpoint_every=200, snapshot_precision=C.SNAP_FP16
     params = dict(nt=nt, sub=1, dt=dt, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2, taper_top=0, taper_bottom=60,
                   taper_left=60, taper_right=60, taper_strength=0.05, checkpoint_every=checkpoint_every,
                   snapshot_precision=snapshot_precision)
+    sxs = [5.0] if nshots == 1 else [1.0 + 8.0 * k / (nshots - 1) for k in range(nshots)]
     return dict(kind=C.ELASTIC, nx=nx, nz=nz, d=d, dt=dt, nt=nt, true=true, start=start, src=src,
-                shots=[dict(x0=0, nx=nx, sx=[5.0], sz=[0.01], rx=rx, rz=rz, nt=nt)], params=params, seismotype=1)
+                shots=[dict(x0=0, nx=nx, sx=[sx], sz=[0.01], rx=rx, rz=rz, nt=nt) for sx in sxs], params=params,
+                seismotype=1)
 
 
 def batch_geometry(nshots=64, nt_max=5001, seed=2, nx=801, d=0.005, dt=4e-4):

@@ -219,6 +219,16 @@ int fwi2d_snapshot(fwi2d_ctx *ctx, int shot, int slot, float *out);
 int fwi2d_plan_info(fwi2d_ctx *ctx, long long *launches_fwd, long long *launches_adj, int *tile_shape,
                     long long *snapshot_bytes);
 
+/* Waves of the plan.  When the snapshots of all its shots do not fit the
+ * device together (less a reserve), an elastic or VTI plan runs its shots in
+ * waves: contiguous runs of shots whose snapshots fit, sharing one snapshot
+ * store.  fwi2d_fwi_gradient then runs forward, residual and adjoint wave by
+ * wave; fwi2d_forward with snapshots, fwi2d_adjoint and fwi2d_snapshot return
+ * FWI2D_ERR_UNSUPPORTED.  The environment variable FWI2D_SNAPSHOT_BUDGET
+ * (bytes), read by fwi2d_set_shots, replaces the budget.  No counterpart in
+ * the reference, which runs one shot at a time (we_op.cpp:970, 1146). */
+int fwi2d_plan_waves(fwi2d_ctx *ctx, int *nwaves, long long *snapshot_bytes_all);
+
 /* Order all later work of the context on a caller's CUDA stream (a
  * cudaStream_t; NULL returns to the context's own stream). */
 int fwi2d_set_stream(fwi2d_ctx *ctx, void *stream);
