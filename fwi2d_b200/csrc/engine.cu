@@ -371,8 +371,9 @@ struct fwi2d_ctx {
     int device = 0;
     cudaStream_t st = nullptr;      // stream all work is ordered on
     cudaStream_t own = nullptr;     // the context's own stream
-    cudaStream_t side = nullptr;    // boundary-band kernels run here, overlapping the core kernel
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side = nullptr;    // boundary-band kernels run here and on side2, overlapping the core kernel
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     fwi2d::ModelState M;
     std::unique_ptr<fwi2d::Plan> plan;
 };
@@ -491,7 +492,7 @@ static const int kBand = 6;
 // these tile shapes over the cells clear of all four boundary bands, and the
 // band kernels of the marching plans on the frame.  Shape indices follow the
 // marching shapes.
-static const int kFramedShapes[] = {3, 2};
+static const int kFramedShapes[] = {3, 2, 1, 0};
 static const int kNumFramed = sizeof(kFramedShapes) / sizeof(kFramedShapes[0]);
 
 static int shape_count() { return elastic_tile_count() + kNumMarch + kNumFramed; }
@@ -508,6 +509,7 @@ struct ShotUnits {
     int TX = 0, TZ = 0, tiles_x = 0, tiles_z = 0;
     int lx = 0, nseg = 0, nwin = 0;
     int ITX = 0, ITZ = 0, itiles_x = 0;   // framed: interior tile shape and tiles along x
+    int itiles_z = 0, izlast = 0;          // framed: tiles along z, first row of the last (interior coordinates)
     std::vector<int> zo;           // marching: owned z starts of the core windows, plus nz - 6
     std::vector<TileRef> tiles;    // marching and framed plans: the x-band tiles
     std::vector<BandRef> bands;    // top / bottom band units (two per run of rows)
@@ -521,9 +523,11 @@ struct ShotUnits {
         if (x >= nx - kBand) return tiles_z + owner_tile(z, nz, TZ);
         const int nt = (int)tiles.size();
         if (z < kBand || z >= nz - kBand) return nt + 2 * ((x - kBand) / zband_rows()) + (z < kBand ? 0 : 1);
-        if (framed)
-            return nt + (int)bands.size() + owner_tile(z - kBand, nz - 2 * kBand, ITZ) * itiles_x +
-                   owner_tile(x - kBand, nx - 2 * kBand, ITX);
+        if (framed) {
+            const int zi = z - kBand;
+            const int kz = zi >= izlast ? itiles_z - 1 : zi / ITZ;
+            return nt + (int)bands.size() + kz * itiles_x + owner_tile(x - kBand, nx - 2 * kBand, ITX);
+        }
         const int seg = (x - kBand) / lx;
         const int k = (int)(std::upper_bound(zo.begin(), zo.end(), z) - zo.begin()) - 1;
         return nt + (int)bands.size() + seg * nwin + k;
@@ -633,18 +637,31 @@ static ShotUnits make_units(int shape, int shot, int nx, int nz)
             U.bands.push_back(b);
         }
     if (framed) {
-        // interior windows, tiled as the tile plans tile a whole grid, offset by the band
+        // interior windows, tiled as the tile plans tile a whole grid, offset by
+        // the band; along z every window starts on an even row (the kernel's
+        // z-pairs), so the last one may reach one row into the bottom band,
+        // which it does not own: its owned cells' stencils stay interior and
+        // its halo inside the grid
         elastic_tile_shape(framed_tile_shape(shape), &U.ITZ, &U.ITX);
         const int ni_x = nx - 2 * kBand, ni_z = nz - 2 * kBand;
         U.itiles_x = (ni_x + U.ITX - 1) / U.ITX;
         const int itiles_z = (ni_z + U.ITZ - 1) / U.ITZ;
+        const int T = U.ITZ;
+        auto zw = [&](int i) {
+            const int v = i * T < ni_z - T ? i * T : ni_z - T;
+            return v + (v & 1);
+        };
+        U.itiles_z = itiles_z;
+        U.izlast = zw(itiles_z - 1);
         for (int tzi = 0; tzi < itiles_z; tzi++)
             for (int txi = 0; txi < U.itiles_x; txi++) {
                 TileRef r;
                 r.shot = shot;
                 r.unit = (int)(U.tiles.size() + U.bands.size() + U.itiles.size());
                 tile_window_host(txi, U.itiles_x, ni_x, U.ITX, r.wx0, r.ox0, r.ox1);
-                tile_window_host(tzi, itiles_z, ni_z, U.ITZ, r.wz0, r.oz0, r.oz1);
+                r.wz0 = zw(tzi);
+                r.oz0 = tzi == 0 ? 0 : zw(tzi);
+                r.oz1 = tzi == itiles_z - 1 ? ni_z : zw(tzi + 1);
                 r.wx0 += kBand;
                 r.ox0 += kBand;
                 r.ox1 += kBand;
@@ -1499,21 +1516,25 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
         launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, st);
         return 1;
     }
+    // the x-band tiles and the top / bottom bands on two side streams, beside the core
     CK(cudaEventRecord(ctx->fork, st));
     CK(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+    CK(cudaStreamWaitEvent(ctx->side2, ctx->fork, 0));
     launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
     launch_elastic_zband(P.kind == KIND_VTI, P.d_bands.as<BandRef>() + R.b0, R.b1 - R.b0, shots, md, P.C, it, flags,
-                         P.dtg, ctx->side);
+                         P.dtg, ctx->side2);
     n += 2;
     CK(cudaEventRecord(ctx->join, ctx->side));
+    CK(cudaEventRecord(ctx->join2, ctx->side2));
     if (P.framed)
         launch_elastic_step(P.ishape, P.kind == KIND_VTI, shots, P.d_itiles.as<TileRef>() + R.i0, R.i1 - R.i0, md,
-                            P.C, it, flags, P.dtg, st);
+                            P.C, it, flags, P.dtg, st, true);
     else
         launch_elastic_march(P.kind == KIND_VTI, shots, P.d_march.as<MarchRef>() + R.m0, R.m1 - R.m0, P.nth, md, P.C,
                              it, flags, P.dtg, st);
     n++;
     CK(cudaStreamWaitEvent(st, ctx->join, 0));
+    CK(cudaStreamWaitEvent(st, ctx->join2, 0));
     return n;
 }
 
@@ -2581,8 +2602,10 @@ int fwi2d_ctx_create(int device, fwi2d_ctx **out)
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->join2, cudaEventDisableTiming));
     c->st = c->own;
     const SbpTables &t = sbp_tables();
     upload_sbp_tables(&t.b1[0][0], &t.b2[0][0][0], t.c2, t.c1, t.sc, t.hc);
@@ -2601,8 +2624,10 @@ int fwi2d_ctx_destroy(fwi2d_ctx *ctx)
     ctx->plan.reset();
     cudaStreamDestroy(ctx->own);
     cudaStreamDestroy(ctx->side);
+    cudaStreamDestroy(ctx->side2);
     cudaEventDestroy(ctx->fork);
     cudaEventDestroy(ctx->join);
+    cudaEventDestroy(ctx->join2);
     delete ctx;
     ABI_END
 }

@@ -98,9 +98,12 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 // Elastic isotropic / VTI step.  Tiles are TZ = 32*RZ (z) by TX (x) cells on
 // 32*TX threads.  Tiles whose every evaluated point is clear of the SBP
 // boundary bands take the lean path (RZ == 2): each thread owns a z-pair of
-// one column, loads are vectorised and all offsets are compile-time.  Other
-// tiles take the general path, which carries the boundary closures, the SAT
-// terms and the absorbing scaling.  Both paths perform the same arithmetic.
+// one column, loads are vectorised, all offsets are compile-time and the
+// pair is evaluated with packed FP32x2 arithmetic (sbp.cuh add2 / mul2:
+// FADD2 / FMUL2, each lane rounded as the scalar operation); a lane whose
+// cell the tile does not own is computed but not stored.  Other tiles take
+// the general path, which carries the boundary closures, the SAT terms and
+// the absorbing scaling.  All paths perform the same arithmetic.
 // ---------------------------------------------------------------------------
 // AE: the elastic part of the acoustic-elastic propagator
 // (nl_we_op_ae::propagate, we_op.cpp:2137-2577): isotropic, version-1 split of
@@ -115,8 +118,17 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 #ifndef TILE_MIN_BLOCKS
 #define TILE_MIN_BLOCKS 5
 #endif
-template <bool VTI, int RZ, int TX, bool GRAD, bool AE>
-__global__ void __launch_bounds__(32 * TX, RZ == 1 && TX == 8 ? TILE_MIN_BLOCKS : 1)
+// CORE: the interior-only instantiation for the interior windows of framed
+// plans, which the engine places clear of the boundary bands (owned cells at
+// least 6 cells from every edge, window and halo inside the grid, even first
+// row); it compiles the lean paths only, without the general path's
+// registers.
+#ifndef CORE_MIN_BLOCKS
+#define CORE_MIN_BLOCKS 2
+#endif
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE, bool CORE = false>
+__global__ void __launch_bounds__(32 * TX, TX == 8 ? (RZ == 1 ? TILE_MIN_BLOCKS : (CORE ? CORE_MIN_BLOCKS : 1))
+                                                   : (CORE && RZ == 1 ? 2 : 1))
 elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C,
              int it, int flags, float dtg)
 {
@@ -147,13 +159,11 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     const int wx0 = tr.wx0, wz0 = tr.wz0;
     // every point this tile evaluates is clear of the SBP boundary bands
     const bool interior = wx0 >= 6 && wx0 + TX + 6 <= nx && wz0 >= 6 && wz0 + TZ + 6 <= nz;
-    // the lean path writes every cell of its window: only for tiles that own all of it
-    const bool full = tr.ox0 == wx0 && tr.ox1 == wx0 + TX && tr.oz0 == wz0 && tr.oz1 == wz0 + TZ;
-    const bool lean = !AE && RZ == 2 && interior && full && (wz0 & 3) == 0;
+    const bool lean = CORE ? RZ == 2 : (!AE && RZ == 2 && interior && (wz0 & 1) == 0);
     // one cell per thread: tiles clear of the boundary bands take the scalar
     // interior forms (no closure code, which keeps the hot loop small); a
     // thread whose cell the tile does not own computes nothing in phase 3
-    const bool lean1 = !AE && RZ == 1 && interior;
+    const bool lean1 = CORE ? RZ == 1 : (!AE && RZ == 1 && interior);
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
@@ -175,7 +185,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
 
     // ---- phase 1: curr with a 4-cell halo, coefficients (and snapshot) with a 2-cell halo
     // (vector loads for interior tiles that start on a multiple of 4 cells)
-    if (lean || (lean1 && (wz0 & 3) == 0)) {
+    if ((lean || lean1) && (wz0 & 3) == 0) {
         constexpr int Q4 = UZ / 4;   // float4 per window row
         for (int f = threadIdx.x; f < UX * Q4; f += NT) {
             const int r = f / Q4, q = f - r * Q4;
@@ -202,7 +212,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 *reinterpret_cast<float2 *>(F1 + r * WZ + 2 * q) = f1;
             }
         }
-    } else if (lean1 && (wz0 & 1) == 0) {
+    } else if ((lean || lean1) && (wz0 & 1) == 0) {
         // interior window on an even row: pairs of samples, no bounds checks
         // (the window and its 4-cell halo lie inside the grid)
         constexpr int Q2U = UZ / 2;
@@ -278,30 +288,21 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             const float2 bm2 = ld2(U1, ui - 2 * UZ), bm1 = ld2(U1, ui - UZ), bp1 = ld2(U1, ui + UZ), bp2 = ld2(U1, ui + 2 * UZ);
             const float2 alo = ld2(U0, ui - 2), amid = ld2(U0, ui), ahi = ld2(U0, ui + 2);
             const float2 blo = ld2(U1, ui - 2), bmid = ld2(U1, ui), bhi = ld2(U1, ui + 2);
-            float2 t0, t1, bx, cz;
-            float vlb[2], vc13[2], vlam[2];
-            if (VTI) {
+            // the pair's z-neighbours: (m2, m1, p1, p2) = (lo, lo|mid, mid|hi, hi)
+            const float2 ux_x = d1s2(am2, am1, ap1, ap2, C.sdx);
+            const float2 uz_z = d1s2(blo, zsh(blo, bmid), zsh(bmid, bhi), bhi, C.sdz);
+            const float2 bx = d1s2(bm2, bm1, bp1, bp2, C.sdx);
+            const float2 cz = d1s2(alo, zsh(alo, amid), zsh(amid, ahi), ahi, C.sdz);
+            float2 t0, t1 = make_float2(0.f, 0.f);
+            if (!VTI) {
+                t0 = add2(ux_x, uz_z);
+            } else {
                 const long long o = mofs + (long long)(wx0 - 2 + sx) * mld + wz0 - 2 + pz;
                 const float2 lb = *reinterpret_cast<const float2 *>(M.lbis + o);
                 const float2 cc = *reinterpret_cast<const float2 *>(M.c13 + o);
                 const float2 ll = *reinterpret_cast<const float2 *>(M.p0 + o);
-                vlb[0] = lb.x; vlb[1] = lb.y; vc13[0] = cc.x; vc13[1] = cc.y; vlam[0] = ll.x; vlam[1] = ll.y;
-            }
-#pragma unroll
-            for (int c = 0; c < 2; c++) {
-                const Z5 az = zsel(alo, amid, ahi, c), bz = zsel(blo, bmid, bhi, c);
-                const float ux_x = d1s(pick(am2, c), pick(am1, c), pick(ap1, c), pick(ap2, c), C.sdx);
-                const float uz_z = d1s(bz.m2, bz.m1, bz.p1, bz.p2, C.sdz);
-                const float vbx = d1s(pick(bm2, c), pick(bm1, c), pick(bp1, c), pick(bp2, c), C.sdx);
-                const float vcz = d1s(az.m2, az.m1, az.p1, az.p2, C.sdz);
-                float vt0, vt1 = 0.f;
-                if (!VTI) vt0 = ux_x + uz_z;
-                else {
-                    vt0 = vlb[c] * ux_x + vc13[c] * uz_z;
-                    vt1 = vlam[c] * uz_z + vc13[c] * ux_x;
-                }
-                if (c == 0) { t0.x = vt0; t1.x = vt1; bx.x = vbx; cz.x = vcz; }
-                else { t0.y = vt0; t1.y = vt1; bx.y = vbx; cz.y = vcz; }
+                t0 = add2(mul2(lb, ux_x), mul2(cc, uz_z));
+                t1 = add2(mul2(ll, uz_z), mul2(cc, ux_x));
             }
             const int wo = sx * WZ + pz;
             *reinterpret_cast<float2 *>(T0 + wo) = t0;
@@ -412,77 +413,91 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
         float2 pv0 = *reinterpret_cast<const float2 *>(pn + cell0);
         float2 pv1 = *reinterpret_cast<const float2 *>(pn + nxz + cell0);
         const float2 rho2 = *reinterpret_cast<const float2 *>(mp2 + gx * mld + gz0);
+        // cells of the pair this tile owns (windows next to a flush window own part of theirs)
+        const bool ownx = gx >= tr.ox0 && gx < tr.ox1;
+        const bool own0 = ownx && gz0 >= tr.oz0 && gz0 < tr.oz1;
+        const bool own1 = ownx && gz0 + 1 >= tr.oz0 && gz0 + 1 < tr.oz1;
         if (store) {
             const int slot = it / C.sub;
             const float sc = prec == SNAP_FP32 ? 1.f : snap_scale(Sp->snap_amax, slot);
             const long long o = (long long)slot * slot_elems + cell0;
-            snap_store(Sp->snap, o, prec, a00.x, sc);
-            snap_store(Sp->snap, o + 1, prec, a00.y, sc);
-            snap_store(Sp->snap, o + nxz, prec, b00.x, sc);
-            snap_store(Sp->snap, o + nxz + 1, prec, b00.y, sc);
+            if (own0) {
+                snap_store(Sp->snap, o, prec, a00.x, sc);
+                snap_store(Sp->snap, o + nxz, prec, b00.x, sc);
+            }
+            if (own1) {
+                snap_store(Sp->snap, o + 1, prec, a00.y, sc);
+                snap_store(Sp->snap, o + nxz + 1, prec, b00.y, sc);
+            }
         }
-        float2 out0, out1;
-        float vax0[2], vaz1[2];
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-            const int gz = gz0 + c;
-            const Z5 az = zsel(alo, a00, ahi, c), bz = zsel(blo, b00, bhi, c), mz = zsel(mlo, m00, mhi, c);
-            const Brk bkx = brk5(pick(mm2, c), pick(mm1, c), pick(m00, c), pick(mp1v, c), pick(mp2v, c));
-            const Brk bkz = brk5(mz.m2, mz.m1, mz.c, mz.p1, mz.p2);
-            float n0, n1;
-            if (!VTI) n0 = d2s(0.f, twice(bkx), pick(am2, c), pick(am1, c), pick(a00, c), pick(ap1, c), pick(ap2, c), C.inv_d2x);
-            else {
-                const float2 q00 = ld2(Q, wi);
-                n0 = d2s(0.f, brk5(pick(qm2, c), pick(qm1, c), pick(q00, c), pick(qp1, c), pick(qp2, c)), pick(am2, c),
-                         pick(am1, c), pick(a00, c), pick(ap1, c), pick(ap2, c), C.inv_d2x);
-            }
-            n1 = d2s(0.f, twice(bkz), bz.m2, bz.m1, bz.c, bz.p1, bz.p2, C.inv_d2z);
-            n1 = d2s(n1, bkx, pick(bm2, c), pick(bm1, c), pick(b00, c), pick(bp1, c), pick(bp2, c), C.inv_d2x);
-            n0 = d2s(n0, bkz, az.m2, az.m1, az.c, az.p1, az.p2, C.inv_d2z);
-            const Z5 tz5 = zsel(tlo, tmid, thi, c);
-            if (!VTI) {
-                const float2 qlo = ld2(Q, wi - 2), qmid = ld2(Q, wi), qhi = ld2(Q, wi + 2);
-                const Z5 qz = zsel(qlo, qmid, qhi, c);
-                n0 += md1s(pick(tm2, c), pick(qm2, c), pick(tm1, c), pick(qm1, c), pick(tp1, c), pick(qp1, c),
-                           pick(tp2, c), pick(qp2, c), C.adx);
-                n1 += md1s(tz5.m2, qz.m2, tz5.m1, qz.m1, tz5.p1, qz.p1, tz5.p2, qz.p2, C.adz);
-            } else {
-                n0 += d1s(pick(tm2, c), pick(tm1, c), pick(tp1, c), pick(tp2, c), C.sdx);
-                n1 += d1s(tz5.m2, tz5.m1, tz5.p1, tz5.p2, C.sdz);
-            }
-            n1 += md1s(pick(cm2, c), pick(mm2, c), pick(cm1, c), pick(mm1, c), pick(cp1, c), pick(mp1v, c),
-                       pick(cp2, c), pick(mp2v, c), C.adx);
-            const Z5 xz = zsel(xlo, xmid, xhi, c);
-            n0 += md1s(xz.m2, mz.m2, xz.m1, mz.m1, xz.p1, mz.p1, xz.p2, mz.p2, C.adz);
-            // sources
-            for (int e = e0; e < e1; e++) {
-                const InjEntry &E = Sp->inj[e];
-                if (E.gx == gx && E.gz == gz) {
-                    const float v = E.mt ? (E.wa * srcrow[E.ia] - E.wb * srcrow[E.ib]) : E.wa * srcrow[E.ia];
-                    if (E.comp == 0) n0 += v;
-                    else n1 += v;
+        // the pair's z-neighbours of a field with pairs (lo, 00, hi): (lo, lo|00, 00|hi, hi)
+        const float2 mz1 = zsh(mlo, m00), mzp = zsh(m00, mhi);
+        const Brk2 bkx = brk52(mm2, mm1, m00, mp1v, mp2v);
+        const Brk2 bkz = brk52(mlo, mz1, m00, mzp, mhi);
+        const float2 zero2 = make_float2(0.f, 0.f);
+        float2 n0, n1;
+        if (!VTI) n0 = d2s2(zero2, twice2(bkx), am2, am1, a00, ap1, ap2, C.inv_d2x);
+        else n0 = d2s2(zero2, brk52(qm2, qm1, ld2(Q, wi), qp1, qp2), am2, am1, a00, ap1, ap2, C.inv_d2x);
+        n1 = d2s2(zero2, twice2(bkz), blo, zsh(blo, b00), b00, zsh(b00, bhi), bhi, C.inv_d2z);
+        n1 = d2s2(n1, bkx, bm2, bm1, b00, bp1, bp2, C.inv_d2x);
+        n0 = d2s2(n0, bkz, alo, zsh(alo, a00), a00, zsh(a00, ahi), ahi, C.inv_d2z);
+        if (!VTI) {
+            const float2 qlo = ld2(Q, wi - 2), qmid = ld2(Q, wi), qhi = ld2(Q, wi + 2);
+            n0 = add2(n0, md1s2(tm2, qm2, tm1, qm1, tp1, qp1, tp2, qp2, C.adx));
+            n1 = add2(n1, md1s2(tlo, qlo, zsh(tlo, tmid), zsh(qlo, qmid), zsh(tmid, thi), zsh(qmid, qhi), thi, qhi,
+                                C.adz));
+        } else {
+            n0 = add2(n0, d1s2(tm2, tm1, tp1, tp2, C.sdx));
+            n1 = add2(n1, d1s2(tlo, zsh(tlo, tmid), zsh(tmid, thi), thi, C.sdz));
+        }
+        n1 = add2(n1, md1s2(cm2, mm2, cm1, mm1, cp1, mp1v, cp2, mp2v, C.adx));
+        n0 = add2(n0, md1s2(xlo, mlo, zsh(xlo, xmid), mz1, zsh(xmid, xhi), mzp, xhi, mhi, C.adz));
+        // sources, cell by cell in the reference's order
+        for (int e = e0; e < e1; e++) {
+            const InjEntry &E = Sp->inj[e];
+            if (E.gx == gx && (E.gz == gz0 || E.gz == gz0 + 1)) {
+                const float v = E.mt ? (E.wa * srcrow[E.ia] - E.wb * srcrow[E.ib]) : E.wa * srcrow[E.ia];
+                if (E.comp == 0) {
+                    if (E.gz == gz0) n0.x += v;
+                    else n0.y += v;
+                } else {
+                    if (E.gz == gz0) n1.x += v;
+                    else n1.y += v;
                 }
             }
-            const float tzv = pick(tzv2, c);
-            float p0 = pick(pv0, c), p1 = pick(pv1, c);
-            if (it > 0) {
-                p0 = p0 * tzv * txv;
-                p1 = p1 * tzv * txv;
-            }
-            const float rho = pick(rho2, c);
-            n0 = C.dt2 * n0 / rho + 2 * az.c - p0;
-            n1 = C.dt2 * n1 / rho + 2 * bz.c - p1;
-            n0 = n0 * tzv * txv;
-            n1 = n1 * tzv * txv;
-            if (c == 0) { out0.x = n0; out1.x = n1; } else { out0.y = n0; out1.y = n1; }
-            amax = fmaxf(amax, fmaxf(fabsf(n0), fabsf(n1)));
-            vax0[c] = d1s(pick(am2, c), pick(am1, c), pick(ap1, c), pick(ap2, c), C.sdx);
-            vaz1[c] = d1s(bz.m2, bz.m1, bz.p1, bz.p2, C.sdz);
         }
-        *reinterpret_cast<float2 *>(pn + cell0) = out0;
-        *reinterpret_cast<float2 *>(pn + nxz + cell0) = out1;
+        const float2 tzx = bc2(txv);
+        if (it > 0) {
+            pv0 = mul2(mul2(pv0, tzv2), tzx);
+            pv1 = mul2(mul2(pv1, tzv2), tzx);
+        }
+        // leapfrog: dt^2 n / rho + 2 curr - prev (one IEEE division per cell)
+        float2 q0 = mul2(bc2(C.dt2), n0), q1 = mul2(bc2(C.dt2), n1);
+        q0 = make_float2(q0.x / rho2.x, q0.y / rho2.y);
+        q1 = make_float2(q1.x / rho2.x, q1.y / rho2.y);
+        n0 = sub2(add2(q0, mul2(bc2(2.f), a00)), pv0);
+        n1 = sub2(add2(q1, mul2(bc2(2.f), b00)), pv1);
+        const float2 out0 = mul2(mul2(n0, tzv2), tzx);
+        const float2 out1 = mul2(mul2(n1, tzv2), tzx);
+        if (own0 && own1) {
+            *reinterpret_cast<float2 *>(pn + cell0) = out0;
+            *reinterpret_cast<float2 *>(pn + nxz + cell0) = out1;
+        } else {
+            if (own0) {
+                pn[cell0] = out0.x;
+                pn[nxz + cell0] = out1.x;
+            }
+            if (own1) {
+                pn[cell0 + 1] = out0.y;
+                pn[nxz + cell0 + 1] = out1.y;
+            }
+        }
+        if (own0) amax = fmaxf(amax, fmaxf(fabsf(out0.x), fabsf(out1.x)));
+        if (own1) amax = fmaxf(amax, fmaxf(fabsf(out0.y), fabsf(out1.y)));
 
-        if (GRAD && do_grad) {
+        if (GRAD && do_grad && (own0 || own1)) {
+            const float2 ax0 = d1s2(am2, am1, ap1, ap2, C.sdx);
+            const float2 az1 = d1s2(blo, zsh(blo, b00), zsh(b00, bhi), bhi, C.sdz);
             const float2 f0m2 = ld2(F0, wi - 2 * WZ), f0m1 = ld2(F0, wi - WZ), f0p1 = ld2(F0, wi + WZ), f0p2 = ld2(F0, wi + 2 * WZ);
             const float2 f1m2 = ld2(F1, wi - 2 * WZ), f1m1 = ld2(F1, wi - WZ), f1p1 = ld2(F1, wi + WZ), f1p2 = ld2(F1, wi + 2 * WZ);
             const float2 f0lo = ld2(F0, wi - 2), f0c = ld2(F0, wi), f0hi = ld2(F0, wi + 2);
@@ -501,62 +516,71 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 fm0 = snap_load2(snap, o, prec, inv);
                 fm1 = snap_load2(snap, o + nxz, prec, inv);
             }
-            float2 v2v = make_float2(0.f, 0.f), v3v = v2v, epsv = v2v;
-            if (VTI) {
+            const float2 t0 = d1s2(f0m2, f0m1, f0p1, f0p2, C.sdx);
+            const float2 t1 = d1s2(f1lo, zsh(f1lo, f1c), zsh(f1c, f1hi), f1hi, C.sdz);
+            const float2 t2 = d1s2(f1m2, f1m1, f1p1, f1p2, C.sdx);
+            const float2 t3 = d1s2(f0lo, zsh(f0lo, f0c), zsh(f0c, f0hi), f0hi, C.sdz);
+            const float2 az0 = ld2(CZ, wi), ax1 = xmid;
+            const float2 two = bc2(2.f);
+            float2 dl = make_float2(0.f, 0.f), dm;
+            if (!VTI) {
+                dm = add2(add2(mul2(add2(az0, ax1), add2(t2, t3)), mul2(mul2(two, ax0), t0)), mul2(mul2(two, az1), t1));
+            } else {
                 const long long mo = mofs + (long long)gx * mld + gz0;
-                v2v = *reinterpret_cast<const float2 *>(M.gv2 + mo);
-                v3v = *reinterpret_cast<const float2 *>(M.gv3 + mo);
-                epsv = *reinterpret_cast<const float2 *>(M.eps + mo);
+                const float2 v2v = *reinterpret_cast<const float2 *>(M.gv2 + mo);
+                const float2 v3v = *reinterpret_cast<const float2 *>(M.gv3 + mo);
+                const float2 epsv = *reinterpret_cast<const float2 *>(M.eps + mo);
+                const float2 e2 = add2(bc2(1.f), mul2(two, epsv));
+                const float2 cross = add2(mul2(ax0, t1), mul2(az1, t0));
+                dl = add2(add2(mul2(mul2(e2, ax0), t0), mul2(az1, t1)), mul2(v2v, cross));
+                dm = add2(add2(add2(mul2(add2(az0, ax1), add2(t2, t3)), mul2(mul2(mul2(two, e2), ax0), t0)),
+                               mul2(mul2(two, az1), t1)),
+                          mul2(v3v, cross));
             }
             float *g0 = Sp->grad + cell0, *g1 = g0 + nxz, *g2 = g1 + nxz;
             float2 G0 = *reinterpret_cast<float2 *>(g0), G1 = *reinterpret_cast<float2 *>(g1), G2 = *reinterpret_cast<float2 *>(g2);
             const float gw = Sp->gwt[itf];
             const double wdt = (double)gw * 1.0 / (double)dtg;
+            const float2 gd = bc2(gw * dtg);
+            if (itf > 0) {
+                // interior and last imaging times: FP32 terms (the density term below, in double)
+                if (!VTI) G0 = add2(G0, mul2(mul2(gd, add2(ax0, az1)), add2(t0, t1)));
+                else G0 = add2(G0, mul2(gd, dl));
+                G1 = add2(G1, mul2(gd, dm));
+            }
 #pragma unroll
             for (int c = 0; c < 2; c++) {
-                const float ax0 = vax0[c], az1 = vaz1[c];
-                const float az0 = pick(ld2(CZ, wi), c), ax1 = pick(xmid, c);
-                const Z5 f0z = zsel(f0lo, f0c, f0hi, c), f1z = zsel(f1lo, f1c, f1hi, c);
-                const float t0 = d1s(pick(f0m2, c), pick(f0m1, c), pick(f0p1, c), pick(f0p2, c), C.sdx);
-                const float t1 = d1s(f1z.m2, f1z.m1, f1z.p1, f1z.p2, C.sdz);
-                const float t2 = d1s(pick(f1m2, c), pick(f1m1, c), pick(f1p1, c), pick(f1p2, c), C.sdx);
-                const float t3 = d1s(f0z.m2, f0z.m1, f0z.p1, f0z.p2, C.sdz);
-                const float f0 = f0z.c, f1 = f1z.c;
+                const float f0 = pick(f0c, c), f1 = pick(f1c, c);
                 const float a0 = pick(out0, c), a1 = pick(out1, c);
-                float dl, dm;
-                if (!VTI) {
-                    dl = 0.f;
-                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
-                } else {
-                    const float e2 = 1 + 2 * pick(epsv, c);
-                    const float v2 = pick(v2v, c), v3 = pick(v3v, c);
-                    dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
-                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
-                }
                 float g0v = pick(G0, c), g1v = pick(G1, c), g2v = pick(G2, c);
                 const float fp0c = pick(fp0, c), fp1c = pick(fp1, c), fm0c = pick(fm0, c), fm1c = pick(fm1, c);
                 if (itf > 0 && itf < last) {
-                    if (!VTI) g0v = g0v + gw * dtg * (ax0 + az1) * (t0 + t1);
-                    else g0v = g0v + gw * dtg * dl;
-                    g1v = g1v + gw * dtg * dm;
                     g2v = (float)((double)g2v + wdt * (double)(a0 * (fp0c - 2 * f0 + fm0c) + a1 * (fp1c - 2 * f1 + fm1c)));
                 } else if (itf == 0) {
                     const double wh = (double)gw * 0.5 * (double)dtg;
-                    if (!VTI) g0v = (float)((double)g0v + wh * (double)(ax0 + az1) * (double)(t0 + t1));
-                    else g0v = (float)((double)g0v + wh * (double)dl);
-                    g1v = (float)((double)g1v + wh * (double)dm);
+                    const float ax0c = pick(ax0, c), az1c = pick(az1, c);
+                    if (!VTI) g0v = (float)((double)g0v + wh * (double)(ax0c + az1c) * (double)(pick(t0, c) + pick(t1, c)));
+                    else g0v = (float)((double)g0v + wh * (double)pick(dl, c));
+                    g1v = (float)((double)g1v + wh * (double)pick(dm, c));
                     g2v = (float)((double)g2v + wdt * (double)(a0 * (fp0c - f0) + a1 * (fp1c - f1)));
                 } else {
-                    if (!VTI) g0v = g0v + gw * dtg * (ax0 + az1) * (t0 + t1);
-                    else g0v = g0v + gw * dtg * dl;
-                    g1v = g1v + gw * dtg * dm;
                     g2v = (float)((double)g2v + wdt * (double)(a0 * (-f0 + fm0c) + a1 * (-f1 + fm1c)));
                 }
                 if (c == 0) { G0.x = g0v; G1.x = g1v; G2.x = g2v; } else { G0.y = g0v; G1.y = g1v; G2.y = g2v; }
             }
-            *reinterpret_cast<float2 *>(g0) = G0;
-            *reinterpret_cast<float2 *>(g1) = G1;
-            *reinterpret_cast<float2 *>(g2) = G2;
+            if (own0 && own1) {
+                *reinterpret_cast<float2 *>(g0) = G0;
+                *reinterpret_cast<float2 *>(g1) = G1;
+                *reinterpret_cast<float2 *>(g2) = G2;
+            } else if (own0) {
+                g0[0] = G0.x;
+                g1[0] = G1.x;
+                g2[0] = G2.x;
+            } else {
+                g0[1] = G0.y;
+                g1[1] = G1.y;
+                g2[1] = G2.y;
+            }
         }
     } else if (lean1) {
         // the general path's arithmetic in its interior forms (sbp.cuh d1i,
@@ -1007,24 +1031,29 @@ static constexpr size_t elastic_smem_bytes()
     return sizeof(float) * (2 * UX * UZ + (5 + ((VTI || AE) ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX);
 }
 
-template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false>
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false, bool CORE = false>
 static void launch_elastic_g(const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
                              const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
     constexpr size_t bytes = elastic_smem_bytes<VTI, RZ, TX, GRAD, AE>();
     static bool configured = false;   // per process; a kernel attribute applies to every device
     if (!configured) {
-        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD, AE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD, AE, CORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bytes);
         configured = true;
     }
-    elastic_step<VTI, RZ, TX, GRAD, AE><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags, dtg);
+    elastic_step<VTI, RZ, TX, GRAD, AE, CORE><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags, dtg);
 }
 
 template <bool VTI, int RZ, int TX>
 static void launch_elastic_t(const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M, const StepConst &C,
-                             int it, int flags, float dtg, cudaStream_t st)
+                             int it, int flags, float dtg, cudaStream_t st, bool core)
 {
+    if (core) {
+        if (flags & F_GRAD) launch_elastic_g<VTI, RZ, TX, true, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+        else launch_elastic_g<VTI, RZ, TX, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+        return;
+    }
     if (flags & F_GRAD) launch_elastic_g<VTI, RZ, TX, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
     else launch_elastic_g<VTI, RZ, TX, false>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
 }
@@ -1039,18 +1068,18 @@ void elastic_tile_shape(int i, int *tz, int *tx)
 }
 
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
-                         const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+                         const StepConst &C, int it, int flags, float dtg, cudaStream_t st, bool core)
 {
     if (ntiles <= 0) return;
     switch (shape) {
-    case 0: vti ? launch_elastic_t<true, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                : launch_elastic_t<false, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
-    case 1: vti ? launch_elastic_t<true, 2, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                : launch_elastic_t<false, 2, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
-    case 2: vti ? launch_elastic_t<true, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                : launch_elastic_t<false, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
-    default: vti ? launch_elastic_t<true, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st)
-                 : launch_elastic_t<false, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st); break;
+    case 0: vti ? launch_elastic_t<true, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core)
+                : launch_elastic_t<false, 2, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core); break;
+    case 1: vti ? launch_elastic_t<true, 2, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core)
+                : launch_elastic_t<false, 2, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core); break;
+    case 2: vti ? launch_elastic_t<true, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core)
+                : launch_elastic_t<false, 1, 16>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core); break;
+    default: vti ? launch_elastic_t<true, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core)
+                 : launch_elastic_t<false, 1, 8>(shots, tiles, ntiles, M, C, it, flags, dtg, st, core); break;
     }
 }
 

@@ -11,8 +11,10 @@ void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const 
 
 int elastic_tile_count();
 void elastic_tile_shape(int i, int *tz, int *tx);
+// core: interior windows of a framed plan (the tile kernel's lean paths only)
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
-                         const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+                         const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st,
+                         bool core = false);
 // x-marching kernel for the cells clear of all four boundary bands; nth
 // threads per unit (one z cell each), a width march_threads_ok accepts
 bool march_threads_ok(int nth);

@@ -225,3 +225,71 @@ __device__ __forceinline__ float d2s(float acc, const Brk &b, float um2, float u
 }
 
 }  // namespace fwi2d
+
+namespace fwi2d {
+
+// ---------------------------------------------------------------------------
+// Packed pairs of samples (sm_100 FADD2 / FMUL2 through __fadd2_rn /
+// __fmul2_rn): each lane is rounded to nearest on its own, exactly as the
+// scalar operation on that lane, so a pair of neighbouring cells evaluated
+// with these forms gives the scalar forms' results bit for bit with half the
+// floating-point instructions.  The operation order of every form is that of
+// its scalar counterpart above.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b == a + (-b) exactly in IEEE arithmetic
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
+// the pair shifted by one cell: (a.y, b.x) from the pairs (a) and (b) that follow each other
+__device__ __forceinline__ float2 zsh(float2 a, float2 b) { return make_float2(a.y, b.x); }
+
+__device__ __forceinline__ float2 d1s2(float2 vm2, float2 vm1, float2 vp1, float2 vp2, float scale)
+{
+    return mul2(bc2(scale), add2(mul2(bc2(kC1[0]), sub2(vp1, vm1)), mul2(bc2(kC1[1]), sub2(vp2, vm2))));
+}
+
+__device__ __forceinline__ float2 md1s2(float2 pm2, float2 qm2, float2 pm1, float2 qm1, float2 pp1, float2 qp1,
+                                        float2 pp2, float2 qp2, float ad)
+{
+    return mul2(bc2(ad), add2(mul2(bc2(kC1[0]), sub2(mul2(pp1, qp1), mul2(pm1, qm1))),
+                              mul2(bc2(kC1[1]), sub2(mul2(pp2, qp2), mul2(pm2, qm2)))));
+}
+
+struct Brk2 {
+    float2 b0, bm1, bp1, bm2, bp2;
+};
+
+__device__ __forceinline__ Brk2 brk52(float2 fm2, float2 fm1, float2 f0, float2 fp1, float2 fp2)
+{
+    Brk2 b;
+    b.b0 = add2(add2(mul2(bc2(kC2[0]), f0), mul2(bc2(kC2[1]), add2(fm1, fp1))), mul2(bc2(kC2[2]), add2(fm2, fp2)));
+    b.bm1 = add2(add2(add2(mul2(bc2(kC2[3]), fm2), mul2(bc2(kC2[4]), fm1)), mul2(bc2(kC2[5]), f0)),
+                 mul2(bc2(kC2[6]), fp1));
+    b.bp1 = add2(add2(add2(mul2(bc2(kC2[3]), fp2), mul2(bc2(kC2[4]), fp1)), mul2(bc2(kC2[5]), f0)),
+                 mul2(bc2(kC2[6]), fm1));
+    b.bm2 = add2(add2(mul2(bc2(kC2[7]), fm2), mul2(bc2(kC2[8]), fm1)), mul2(bc2(kC2[9]), f0));
+    b.bp2 = add2(add2(mul2(bc2(kC2[7]), fp2), mul2(bc2(kC2[8]), fp1)), mul2(bc2(kC2[9]), f0));
+    return b;
+}
+
+__device__ __forceinline__ Brk2 twice2(const Brk2 &a)
+{
+    Brk2 b;
+    b.b0 = mul2(bc2(2.f), a.b0);
+    b.bm1 = mul2(bc2(2.f), a.bm1);
+    b.bp1 = mul2(bc2(2.f), a.bp1);
+    b.bm2 = mul2(bc2(2.f), a.bm2);
+    b.bp2 = mul2(bc2(2.f), a.bp2);
+    return b;
+}
+
+__device__ __forceinline__ float2 d2s2(float2 acc, const Brk2 &b, float2 um2, float2 um1, float2 u0, float2 up1,
+                                       float2 up2, float invd2)
+{
+    const float2 s = add2(add2(add2(add2(mul2(b.b0, u0), mul2(b.bm1, um1)), mul2(b.bp1, up1)), mul2(b.bm2, um2)),
+                          mul2(b.bp2, up2));
+    return add2(acc, mul2(bc2(invd2), s));
+}
+
+}  // namespace fwi2d

@@ -45,7 +45,7 @@ def run_gpu(kind, mc, src, pd, nx, nz, d, src_locs, rcv_locs, adj_src=None, mt=0
                                         (0, (120, 200)), (1, (120, 200)),
                                         (4, (72, 80)), (6, (120, 200)), (7, (120, 200)), (11, (120, 200)),
                                         (11, (60, 251)), (14, (72, 80)), (15, (72, 80)), (14, (120, 200)),
-                                        (15, (60, 251))])
+                                        (15, (60, 251)), (16, (120, 200)), (17, (120, 200)), (17, (60, 251))])
 def test_forward_adjoint_vs_oracle(kind, mt, bc, shape, grid):
     """Shapes 0-3 run the tile kernel over the whole grid: small grids exercise
     the boundary path only; the 120 x 200 grid has interior tiles, which take
@@ -53,10 +53,12 @@ def test_forward_adjoint_vs_oracle(kind, mt, bc, shape, grid):
     marching kernel on the rows clear of the x boundary bands (one z window
     on 80 rows, two on 200; on 251 rows with 128-cell windows the last
     window is shifted up so that it owns the whole bottom band) and runs of
-    64 or 32 rows.  Shapes 14 and 15 are framed plans: 32 x 8 and 32 x 16
-    tiles on the tile kernel's interior path over the cells clear of the
-    bands (the last window of each axis flush with the band, owning part of
-    its cells), the bands on the band kernels."""
+    64 or 32 rows.  Shapes 14 to 17 are framed plans: 32 x 8, 32 x 16, 64 x 8
+    and 64 x 16 tiles on the tile kernel's interior paths (one cell, or a
+    z-pair in packed FP32x2 arithmetic, per thread) over the cells clear of
+    the bands (the last window of each axis flush with the band, owning part
+    of its cells), the bands on the band kernels.  Tile shapes 0 and 1 on the
+    200-row grid also run z-pair windows that own part of their cells."""
     nx, nz = grid
     d, nt = 0.01, 220 if nz < 100 else 160
     m = K.model_case(kind, nx, nz, d, seed=3)
