@@ -1022,6 +1022,8 @@ void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const 
     cudaMemcpyToSymbol(kC1, c1, sizeof(float) * 2);
     cudaMemcpyToSymbol(kSC, sc, sizeof(float) * 4);
     cudaMemcpyToSymbol(kHC, hc, sizeof(float) * 4);
+    const float2 one = make_float2(1.f, 1.f);
+    cudaMemcpyToSymbol(kOne2, &one, sizeof(one));
 }
 
 template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false>

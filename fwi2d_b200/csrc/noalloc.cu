@@ -211,6 +211,12 @@ extern "C" int fwi2d_propagate_noalloc(const float *model, const float *allsrc, 
     NA_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(FWI2D_ERR_ARG, "device index beyond 63");
     if (!g_addr[dev]) {
+        // once per device: the SBP coefficient tables the step kernels read
+        // (copies into the kernels' constant memory, no allocation), then the
+        // scratch array's device address
+        const SbpTables &t = sbp_tables();
+        upload_sbp_tables(&t.b1[0][0], &t.b2[0][0][0], t.c2, t.c1, t.sc, t.hc);
+        NA_CK(cudaGetLastError());
         void *ptr = nullptr;
         NA_CK(cudaGetSymbolAddress(&ptr, g_scratch));
         g_addr[dev] = (unsigned char *)ptr;

@@ -24,6 +24,7 @@ static __constant__ float kC2[10];        // its interior weights
 static __constant__ float kC1[2];         // 2/3, -1/12
 static __constant__ float kSC[4];         // one-sided boundary derivative 11/6, -3, 3/2, -1/3
 static __constant__ float kHC[4];         // H-norm boundary weights 17/48, 59/48, 43/48, 49/48
+static __constant__ float2 kOne2;         // (1, 1), set at run time: the packed sums' multiplier (add2)
 
 __device__ __forceinline__ float d1(const float *p, int st, int g, int n, float d, float scale)
 {
@@ -229,17 +230,40 @@ __device__ __forceinline__ float d2s(float acc, const Brk &b, float um2, float u
 namespace fwi2d {
 
 // ---------------------------------------------------------------------------
-// Packed pairs of samples (sm_100 FADD2 / FMUL2 through __fadd2_rn /
-// __fmul2_rn): each lane is rounded to nearest on its own, exactly as the
-// scalar operation on that lane, so a pair of neighbouring cells evaluated
-// with these forms gives the scalar forms' results bit for bit with half the
-// floating-point instructions.  The operation order of every form is that of
-// its scalar counterpart above.
+// Packed pairs of samples (sm_100 f32x2 arithmetic): each lane is rounded to
+// nearest on its own, exactly as the scalar operation on that lane, so a pair
+// of neighbouring cells evaluated with these forms gives the scalar forms'
+// results bit for bit with half the floating-point instructions.  The
+// operation order of every form is that of its scalar counterpart above.
+//
+// The assembler fuses a packed multiply into a packed add that consumes it
+// (one rounding instead of two) even with an explicit .rn and --fmad=false,
+// which would break the bitwise match with the reference.  A packed sum is
+// therefore an fma.rn.f32x2 with the multiplier kOne2, which is (1, 1) at run
+// time but unknown to the assembler: 1 * x + y rounds once, to x + y, and
+// there is no product left to fuse.  It costs one instruction, as the add.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    float2 r;
+    const float2 one = kOne2;
+    asm("{\n .reg .b64 po, pa, pb, pd;\n mov.b64 po, {%2, %3};\n mov.b64 pa, {%4, %5};\n"
+        " mov.b64 pb, {%6, %7};\n fma.rn.f32x2 pd, po, pa, pb;\n mov.b64 {%0, %1}, pd;\n}\n"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(one.x), "f"(one.y), "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n .reg .b64 pa, pb, pd;\n mov.b64 pa, {%2, %3};\n mov.b64 pb, {%4, %5};\n"
+        " mul.rn.f32x2 pd, pa, pb;\n mov.b64 {%0, %1}, pd;\n}\n"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
 // a - b == a + (-b) exactly in IEEE arithmetic
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return add2(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
 // the pair shifted by one cell: (a.y, b.x) from the pairs (a) and (b) that follow each other
 __device__ __forceinline__ float2 zsh(float2 a, float2 b) { return make_float2(a.y, b.x); }

@@ -85,6 +85,36 @@ def test_forward_adjoint_vs_oracle(kind, mt, bc, shape, grid):
         assert K.rel_l2(g_g[c], g_o[c]) <= GRAD_TOL, "gradient component %d" % c
 
 
+@pytest.mark.parametrize("kind", [O.KIND_ELASTIC, O.KIND_VTI])
+@pytest.mark.parametrize("shape", [0, 1, 3, 16, 17])
+def test_deep_source_vs_oracle(kind, shape):
+    """Source and receivers deep inside a 120 x 240 grid, so that the wave
+    crosses the interior windows of every shape from the first steps: the
+    z-pair windows of the 64-row shapes (packed FP32x2 arithmetic) and the
+    framed plans' interior tiles, against the oracle over 200 steps."""
+    nx, nz = 120, 240
+    d, nt = 0.01, 200
+    m = K.model_case(kind, nx, nz, d, seed=9)
+    mc = K.converted(kind, m)
+    sl, rl = K.geometry(nx, nz, d, nr=24, sz=(100 + 0.3) * d, rz=70 * d)
+    pd = K.par_dict(nt=nt, dt=1e-3, bc=(1, 2, 2, 2))
+    src = K.sources(2, nt, 1e-3)
+    port = O.Port(32)
+    par = O.make_par(**pd, ns=1, nr=len(rl[0]))
+    rcv_o, full_o = K.oracle_forward(port, kind, mc, src, par, nx, nz, d, sl, rl)
+    adj = np.ascontiguousarray(rcv_o[:, :, ::-1])
+    g_o = K.oracle_adjoint(port, kind, mc, adj, par, nx, nz, d, sl, rl, full_o)
+    rcv_g, g_g, snaps = run_gpu(kind, mc, src, pd, nx, nz, d, sl, rl, adj_src=adj, shape=shape)
+    idx = list(range(0, nt, max(1, nt // 5)))
+    e_tr, e_sn, e_gr = K.rel_l2(rcv_g, rcv_o), K.rel_l2(snaps, full_o[idx]), K.rel_l2(g_g, g_o)
+    print("deep source kind %d shape %d: traces %.3e (bitwise %.4f) snapshots %.3e gradient %.3e (bitwise %.4f)" % (
+        kind, shape, e_tr, np.mean(rcv_g == rcv_o), e_sn, e_gr, np.mean(g_g == g_o)))
+    assert e_tr <= TRACE_TOL
+    assert e_sn <= TRACE_TOL
+    for c in range(3):
+        assert K.rel_l2(g_g[c], g_o[c]) <= GRAD_TOL, "gradient component %d" % c
+
+
 @pytest.mark.parametrize("bc", [(1, 2, 2, 2), (3, 3, 2, 2), (2, 2, 2, 2), (1, 1, 3, 3)])
 @pytest.mark.parametrize("shape,grid", [(2, (72, 80)), (3, (72, 80)), (2, (120, 200)), (3, (60, 251))])
 def test_acoustic_forward_adjoint_vs_oracle(bc, shape, grid):

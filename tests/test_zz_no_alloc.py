@@ -12,6 +12,8 @@ The checks:
   practice bitwise), over several boundary-condition sets, a top taper and a
   receiver buffer that already holds data (the entry point accumulates into
   it), so the shared array leaves nothing behind from the previous call;
+* as the first library call of a fresh process it sets up the device itself
+  and gives the same receivers;
 * after a first call has reserved the array, a further call leaves the
   device's free memory unchanged: it allocates nothing;
 * incomplete injector tables and problems larger than the array are
@@ -85,6 +87,43 @@ def test_noalloc_matches_propagate_twice(seed, nx, nz, nt, nr, bc, taper):
         assert rc == 0, L.fwi2d_noalloc_last_error().decode()
         err = K.rel_l2(out - base, ref - base)
         assert err <= TRACE_TOL, "call %d: rel-L2 %.3e" % (call, err)
+
+
+FRESH = r'''
+import ctypes, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import fwi2d_b200 as F
+from fwi2d_b200 import _capi as C
+from tests import test_zz_no_alloc as T
+L = T._bind(F.load())
+seed, nx, nz, nt, nr, bc, taper = T.CASES[0]
+mc, src, inj, ext, params, d = T._case(seed, nx, nz, nt, nr, bc, taper)
+out = np.zeros((2, nr, nt), np.float32)
+rc = T._noalloc(L, mc, src, out, T._injector(inj), T._injector(ext), params, nr, nx, nz, d)
+assert rc == 0, L.fwi2d_noalloc_last_error().decode()
+np.save(sys.argv[2], out)
+'''
+
+
+def test_noalloc_first_call_in_fresh_process(tmp_path):
+    """The entry point is the first library call of a fresh process (no
+    context was ever created there): it must set up the device itself."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = str(tmp_path / "rcv.npy")
+    subprocess.run([sys.executable, "-c", FRESH, root, path], check=True, timeout=600)
+    out = np.load(path)
+    L = _bind(F.load())
+    seed, nx, nz, nt, nr, bc, taper = CASES[0]
+    mc, src, inj, ext, params, d = _case(seed, nx, nz, nt, nr, bc, taper)
+    ref = np.zeros((2, nr, nt), np.float32)
+    C.check(L.fwi2d_propagate(0, 0, C.ptr(mc), C.ptr(src), C.ptr(ref), ctypes.byref(_injector(inj)),
+                              ctypes.byref(_injector(ext)), None, None, None, None, ctypes.byref(params), 1, nr, nx, nz,
+                              d, d))
+    assert K.rel_l2(out, ref) <= TRACE_TOL
 
 
 def test_noalloc_call_allocates_no_device_memory():
