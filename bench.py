@@ -157,8 +157,9 @@ def build_workload(name, rank, world):
             wl["shots"] = [sh]
     else:
         wl = W.vti_batch()
-        if world > 1:
-            wl["shots"] = wl["shots"][rank::world]
+        if world > 1:   # cost-balanced shot lists (longest processing time first)
+            from fwi2d_b200.distributed import shard_shots
+            wl["shots"] = [wl["shots"][i] for i in shard_shots(wl["shots"], rank, world, wl["nz"])]
     return wl
 
 

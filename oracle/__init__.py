@@ -114,6 +114,14 @@ def have_reference_gpu():
     return os.path.exists(reference_gpu_path())
 
 
+def reference_b200_path():
+    return os.path.join(HERE, "_ref", "libfwi2d_ref32_b200.so")
+
+
+def have_reference_b200():
+    return os.path.exists(reference_b200_path())
+
+
 class Port(_Lib):
     """The C restatement."""
 
@@ -420,3 +428,35 @@ class ReferenceGPU(Reference):
                        len(ex), _ptr(ex), _ptr(ez), _ptr(full), _ptr(grad), ctypes.byref(par), nx, nz, dx, dz, ox, oz)
         if rc != 0:
             raise RuntimeError("reference GPU propagate failed with status %d" % rc)
+
+
+class ReferenceB200(Reference):
+    """The reference built as its maintainer would switch it to fwi2d_b200:
+    its own sources with -DCUDA and fwi2d_b200/integration/we_op_b200.cpp as
+    the propagate_gpu hook (oracle/_ref/libfwi2d_ref32_b200.so, linked with
+    libfwi2d_b200.so).  misfit_grad / misfit_grad_ae run the reference's
+    operator classes and solver steps, which call the hook; propagate runs
+    the hook directly (ref_propagate_gpu)."""
+
+    def __init__(self):
+        path = reference_b200_path()
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " (built by oracle/build_ref.sh where the reference is present)")
+        _Lib.__init__(self, path, 32, "reference-b200")
+        self._resample_symbol = "ref_resample"
+        self._gpu = self.lib.ref_propagate_gpu
+        self._gpu.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int,
+                              ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+
+    def propagate(self, kind, adj, model, src, rcv, par, nx, nz, dx, dz, ox, oz, inj_locs, ext_locs,
+                  inj_type=0, full=None, grad=None, water_inj_locs=None, water_ext_locs=None):
+        assert kind in (KIND_ELASTIC, KIND_VTI) and water_inj_locs is None and water_ext_locs is None
+        ix, iz = self.arr(inj_locs[0]), self.arr(inj_locs[1])
+        ex, ez = self.arr(ext_locs[0]), self.arr(ext_locs[1])
+        rc = self._gpu(kind, adj, _ptr(model), _ptr(src), _ptr(rcv), inj_type, len(ix), _ptr(ix), _ptr(iz),
+                       len(ex), _ptr(ex), _ptr(ez), _ptr(full), _ptr(grad), ctypes.byref(par), nx, nz, dx, dz, ox, oz)
+        if rc != 0:
+            raise RuntimeError("reference propagate_gpu hook failed with status %d" % rc)

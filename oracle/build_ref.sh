@@ -59,4 +59,22 @@ if [ -x "$CUDA_HOME/bin/nvcc" ]; then
     g++ -shared -fopenmp -o "$OUT/libfwi2d_ref32_cuda.so" $OBJS -L"$CUDA_HOME/lib64" -lcudart_static -ldl -lrt -lpthread \
         -Wl,--no-undefined
 fi
+# The reference built as its maintainer would switch it to this library:
+# the same -DCUDA objects, with fwi2d_b200/integration/we_op_b200.cpp (its
+# propagate_gpu hook on fwi2d_propagate) in place of src/cuda, linked with
+# libfwi2d_b200.so: libfwi2d_ref32_b200.so.  The tests run the reference's own
+# operator classes and solver gradient through it.
+LIB="$HERE/../fwi2d_b200/libfwi2d_b200.so"
+if [ -x "$CUDA_HOME/bin/nvcc" ] && [ -f "$LIB" ] && [ -d "$OUT/objcuda" ]; then
+    B="$OUT/objcuda"
+    INC="-I$HERE/ref_shim -I$REF/src/include -I$REF/src/cuda -I$CUDA_HOME/include -I$HERE/../include"
+    g++ -std=c++11 -O3 -fopenmp -fPIC -w -DCUDA $INC -c "$HERE/../fwi2d_b200/integration/we_op_b200.cpp" \
+        -o "$B/we_op_b200.o"
+    OBJS=""
+    for s in we_op spatial_operators injector misc operator ispc_loops stubs ref_driver; do
+        OBJS="$OBJS $B/$s.o"
+    done
+    g++ -shared -fopenmp -o "$OUT/libfwi2d_ref32_b200.so" $OBJS "$B/we_op_b200.o" \
+        -L"$HERE/../fwi2d_b200" -lfwi2d_b200 -Wl,-rpath,'$ORIGIN/../../fwi2d_b200' -Wl,--no-undefined
+fi
 echo "reference oracle built in $OUT"

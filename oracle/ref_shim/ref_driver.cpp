@@ -289,9 +289,11 @@ int ref_bin_read(const char *header, int ndim0, data_t *out, long cap, int *ndim
 }
 
 #ifdef CUDA
-// The reference's own GPU path (src/cuda/cudaWeOp.cpp, built with -DCUDA):
 // nl_we_op_e / nl_we_op_vti::propagate_gpu with ref_propagate's arguments
-// (kind 0 or 1).  Used only to time the reference's GPU implementation.
+// (kind 0 or 1), in the builds with -DCUDA: the reference's own GPU path
+// (src/cuda/cudaWeOp.cpp; timed beside this library) or the hook on
+// fwi2d_b200 (fwi2d_b200/integration/we_op_b200.cpp; tested against the CPU
+// build).
 int ref_propagate_gpu(int kind, int adj, const data_t *model, const data_t *allsrc, data_t *allrcv,
                       int inj_type, int ninj, const data_t *ix, const data_t *iz,
                       int next, const data_t *ex, const data_t *ez,
