@@ -2601,8 +2601,13 @@ int fwi2d_ctx_create(int device, fwi2d_ctx **out)
     c->device = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking));
+    // the band kernels' few CTAs are on the critical path of a step: their
+    // streams take the highest priority, so that the block scheduler starts
+    // them before the core launch fills the SMs
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CK(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&c->side2, cudaStreamNonBlocking, prio_hi));
     CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->join2, cudaEventDisableTiming));
