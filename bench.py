@@ -80,11 +80,42 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# the adjoint tile kernel on the single-shot grid, from the ncu capture
-# summarised in profiles/elastic_step_adjoint_single_shot_401x801.md
-# (cold caches: ncu flushes L2 before each pass).
-ADJ_TILE_TRAFFIC_BYTES = 21.756928e6
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one adjoint
+# step of the single-shot grid on the framed tile plan (shape 16): the core
+# launch and the x-band launch from the capture summarised in
+# profiles/elastic_step_framed_single_shot_401x801.md, the z-band launch from
+# profiles/elastic_zband_single_shot_401x801.md (cold caches: ncu flushes L2
+# before each pass); and the core launch's L1-to-L2 bytes.
+FRAMED_SHAPE = 16
+ADJ_STEP_TRAFFIC_BYTES = {"core": 21.133312e6, "x_bands": 0.554496e6, "z_bands": None}
+ADJ_CORE_L2_BYTES, ADJ_CORE_COLD_US = 1447280 * 32, 28.576
+
+
+def roof_kernel(shape, config):
+    if config == "single" and shape == FRAMED_SHAPE:
+        return ("adjoint + imaging step of the framed plan: interior elastic_step<RZ=2, CORE> with the x-band "
+                "elastic_step and elastic_zband overlapped on two side streams (one step = one launch of each)")
+    if config == "single":
+        return "adjoint + imaging step (tile shape %d)" % shape
+    return "adjoint loop: interior, band and imaging kernels"
+
+
+def step_traffic(shape, config):
+    """DRAM bytes of one adjoint step from the committed ncu summaries, or
+    None when a part is not captured for this plan."""
+    if config != "single" or shape != FRAMED_SHAPE or None in ADJ_STEP_TRAFFIC_BYTES.values():
+        return None
+    return sum(ADJ_STEP_TRAFFIC_BYTES.values())
+
+
+def l2_note(shape, config):
+    """L2 figures of the L2-resident single-shot case, from the committed ncu
+    capture of the core launch (cold caches)."""
+    if config != "single" or shape != FRAMED_SHAPE:
+        return None
+    return {"kernel": "elastic_step<RZ=2, CORE> adjoint", "l1_to_l2_bytes_per_launch": ADJ_CORE_L2_BYTES,
+            "achieved_gbs": ADJ_CORE_L2_BYTES / (ADJ_CORE_COLD_US * 1e-6) / 1e9, "lts_throughput_pct": 7.0,
+            "source": "ncu capture, cold caches (profiles/elastic_step_framed_single_shot_401x801.md)"}
 
 
 # ---------------------------------------------------------------------------
@@ -507,15 +538,15 @@ def run_ours(args):
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "shots_per_s": total_shots / (e2e_ms / 1e3)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": ("elastic_step (adjoint + imaging)" if args.config == "single" else
-                                                    "adjoint loop: marching, band and imaging kernels"),
+            "roofline": {"bound": "hbm", "kernel": roof_kernel(info["tile_shape"], args.config),
                          "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": ADJ_TILE_TRAFFIC_BYTES if args.config == "single" else None,
+                         "traffic": step_traffic(info["tile_shape"], args.config),
                          "algorithmic_bytes_per_launch": bytes_adj * cells_launch,
                          "launch_ms": adj_launch_s * 1e3,
                          "forward_launch_ms": fwd_launch_s * 1e3,
                          "forward_achieved": BYTES_FWD * cells_launch / fwd_launch_s / 1e9},
+            "l2": l2_note(info["tile_shape"], args.config),
             "clocks": clocks,
         }
         if world == 1 and args.config == "single":

@@ -242,6 +242,7 @@ struct ShotPlan {
     int nbuf = 0;                  // slots held on the device (nslot, or the replay window)
     size_t snap_need = 0;          // bytes of its snapshot store
     int u_t0 = 0, u_m0 = 0, u_b0 = 0, u_i0 = 0;   // first tile / marching / band / interior unit in the plan
+    int u_w0 = 0;                                 // acoustic-elastic: first fluid-layer tile in the plan
     void *snap_base = nullptr;     // its snapshot store: `snap`, or its place in the plan's wave pool
     std::vector<InjEntry> inj_f, inj_a;
     std::vector<int> inj_f_off, inj_a_off, inj_f_roff, inj_a_roff;
@@ -284,6 +285,7 @@ struct Plan {
     struct Wave {
         int s0 = 0, s1 = 0, nt_max = 0;
         int t0 = 0, t1 = 0, m0 = 0, m1 = 0, b0 = 0, b1 = 0, i0 = 0, i1 = 0;   // unit ranges
+        int w0 = 0, w1 = 0;                                                   // fluid-layer tiles
         cudaGraphExec_t graph[2] = {nullptr, nullptr};                        // forward + snapshots, adjoint
         cudaEvent_t ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
         long long launches[2] = {0, 0};
@@ -1064,17 +1066,20 @@ static void plan_waves(Plan &P, bool one_wave)
         w.m0 = a.u_m0;
         w.b0 = a.u_b0;
         w.i0 = a.u_i0;
+        w.w0 = a.u_w0;
         if (s1 < n) {
             const ShotPlan &b = *P.shots[s1];
             w.t1 = b.u_t0;
             w.m1 = b.u_m0;
             w.b1 = b.u_b0;
             w.i1 = b.u_i0;
+            w.w1 = b.u_w0;
         } else {
             w.t1 = (int)P.tiles.size();
             w.m1 = (int)P.marches.size();
             w.b1 = (int)P.bands.size();
             w.i1 = (int)P.itiles.size();
+            w.w1 = (int)P.wtiles.size();
         }
     };
     P.waves.clear();
@@ -1319,6 +1324,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             W->den.upload(wden, ctx->st);
             W->tz.upload(wtz, ctx->st);
             W->tx.upload(wtx, ctx->st);
+            S->u_w0 = (int)P->wtiles.size();
             P->wtiles.insert(P->wtiles.end(), UW.tiles.begin(), UW.tiles.end());
             S->halo.alloc((size_t)sh.nx * sizeof(float));
             S->fluid = std::move(W);
@@ -1389,7 +1395,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         P->shots.push_back(std::move(S));
     }
     P->have_snapshots = p.sub > 0;
-    plan_waves(*P, p.checkpoint_every > 0 || ae || acoustic);
+    plan_waves(*P, p.checkpoint_every > 0);
     P->d_tiles.upload(P->tiles, ctx->st);
     P->d_march.upload(P->marches, ctx->st);
     P->d_bands.upload(P->bands, ctx->st);
@@ -1499,17 +1505,15 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
         // fluid layer, elastic grid, then the implicit interface coupling
         const bool adj = (flags & STEP_GRAD) != 0;
         const ShotDev *wshots = (adj ? P.d_wshots_a : P.d_wshots_f).as<ShotDev>();
-        launch_ae_fluid_step(P.tshape, wshots, P.d_wtiles.as<TileRef>(), (int)P.wtiles.size(), P.wdev(), P.Cw, it,
+        launch_ae_fluid_step(P.tshape, wshots, P.d_wtiles.as<TileRef>() + R.w0, R.w1 - R.w0, P.wdev(), P.Cw, it,
                              flags & STEP_EXTRACT, st);
-        launch_ae_elastic_step(P.tshape, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C, it, flags,
-                               P.dtg, st);
-        launch_ae_couple(shots, wshots, (int)P.shots.size(), P.nx_max, md, P.C, it, flags, P.dtg, P.Kw, P.val0,
+        launch_ae_elastic_step(P.tshape, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, st);
+        launch_ae_couple(shots + R.s0, wshots + R.s0, R.s1 - R.s0, P.nx_max, md, P.C, it, flags, P.dtg, P.Kw, P.val0,
                          adj ? -1 : 1, st);
         return 3;
     }
     if (P.kind == KIND_ACOUSTIC) {
-        launch_acoustic_step(P.tshape, shots, P.d_tiles.as<TileRef>(), (int)P.tiles.size(), md, P.C, it, flags, P.dtg,
-                             st);
+        launch_acoustic_step(P.tshape, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, st);
         return 1;
     }
     if (!P.march && !P.framed) {
@@ -1928,7 +1932,7 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode, int w = 0)
     // source is in the water, else to the elastic grid, in both directions
     // (we_op.cpp:2220-2236)
     if (P.ae && P.ae_src_fluid)
-        launch_init_state(wshots, nshots, P.d_wicells[im].as<InitCell>(), P.d_wioff[im].as<int>(),
+        launch_init_state(wshots + R.s0, nshots, P.d_wicells[im].as<InitCell>(), P.d_wioff[im].as<int>() + R.s0,
                           P.d_wiidx[im].as<int>(), cst);
     else
         launch_init_state(shots + R.s0, nshots, P.d_icells[im].as<InitCell>(), P.d_ioff[im].as<int>() + R.s0,
@@ -1956,7 +1960,7 @@ static void capture(fwi2d_ctx *ctx, Plan &P, int mode, int w = 0)
             launch_finalize(shots + R.s0, nshots, P.C, ncomp, STEP_EXTRACT | (store ? STEP_STORE : 0), cst);
             n++;
             if (P.ae) {
-                launch_finalize(wshots, nshots, P.Cw, 1, STEP_EXTRACT, cst);
+                launch_finalize(wshots + R.s0, nshots, P.Cw, 1, STEP_EXTRACT, cst);
                 n++;
             }
         } else if (P.kind == KIND_ACOUSTIC) {

@@ -16,6 +16,13 @@ value distributions the configurations describe, in the reference's units
   km receiver aperture on its own cropped grid and a 1.2-2.0 s record.
 * elastic_batch   -- the batch geometry of vti_batch on the isotropic model
   of elastic_single (batched elastic gradients).
+* ae_fwi          -- acoustic-elastic FWI: a 200 m water layer (vp 1.5,
+  vs 0, rho 1.0) over a flat seabed on four elastic layers with seeded
+  velocities in [2.2, 4.0] km/s and a Gaussian low-velocity lens; 601 x 1601
+  cells at 5 m in all (the water rows are the fluid layer above the elastic
+  grid), Ricker 8 Hz, dt 0.4 ms, 6001 samples, 96 shots in the water; or the
+  same model on a coarser, smaller grid (scale) for solver runs that the
+  reference's CPU build finishes in minutes.
 """
 import math
 
@@ -172,3 +179,55 @@ def elastic_batch(nshots=64, nt_max=5001, seed=2, every=1, snapshot_precision=C.
     wl["shots"] = shots
     wl["params"] = dict(wl["params"], snapshot_precision=snapshot_precision)
     return wl
+
+
+def ae_model(nx=1601, nz=561, d=0.005, seed=4):
+    """Raw (vp, vs, rho) of the elastic part of the acoustic-elastic model (the
+    grid below the seabed): four flat layers whose velocities are drawn from
+    [2.2, 4.0] km/s and sorted to increase with depth, at seeded depths, and a
+    Gaussian lens 15 % slower than its layer (width a tenth of the line, height
+    a quarter of the grid) in the second layer; vs = vp/1.73,
+    rho = 0.31 (1000 vp)^0.25."""
+    rng = np.random.default_rng(seed)
+    vel = np.sort(rng.uniform(2.2, 4.0, 4))
+    cuts = np.sort(rng.uniform(0.15, 0.85, 3)) * nz
+    z = np.arange(nz)[None, :] * np.ones((nx, 1))
+    layer = (z >= cuts[0]).astype(int) + (z >= cuts[1]) + (z >= cuts[2])
+    vp = vel[layer]
+    x = np.arange(nx)[:, None] * np.ones((1, nz))
+    xc, zc = rng.uniform(0.35, 0.65) * nx, 0.5 * (cuts[0] + cuts[1])
+    sx, sz = 0.1 * nx / 2.355, 0.25 * nz / 2.355
+    vp = vp * (1 - 0.15 * np.exp(-0.5 * (((x - xc) / sx) ** 2 + ((z - zc) / sz) ** 2)))
+    vs = vp / 1.73
+    rho = 0.31 * (1000 * vp) ** 0.25
+    return np.stack([vp, vs, rho]).astype(np.float32)
+
+
+def ae_fwi(nx=1601, nz=561, nza=41, d=0.005, dt=4e-4, nt=6001, nshots=96, seed=4):
+    """Acoustic-elastic FWI workload: a fluid layer of nza rows (200 m at the
+    defaults) over an elastic grid of nz x nx cells (ae_model), dt, nt
+    samples of a Ricker 8 Hz source delayed 0.15 s, nshots sources 10 m below
+    the sea surface spread over the line, receivers every 10 m from 10 m,
+    10 m below the seabed on the elastic grid and 10 m below the sea surface
+    in the fluid.  Free sea surface, absorbing elsewhere with 20-cell tapers.
+    The starting model is the true model smoothed over 150 m."""
+    oz = (nza - 1) * d
+    true = ae_model(nx, nz, d, seed)
+    start = smoothed(true, max(1.0, 0.15 / d))
+    w = ricker(nt, dt, 8.0, 0.15)
+    width = (nx - 1) * d
+    sxs = [width * (0.05 + 0.9 * k / max(1, nshots - 1)) for k in range(nshots)]
+    rx = np.arange(0.01, width - 0.005, 0.01, dtype=np.float32)
+    params = dict(nt=nt, sub=1, dt=dt, bc_top=1, bc_bottom=2, bc_left=2, bc_right=2, taper_top=0,
+                  taper_bottom=20, taper_left=20, taper_right=20, taper_strength=0.05, nza=nza, acoustic_source=1)
+    return dict(kind=C.ACOUSTIC_ELASTIC, nx=nx, nz=nz, nza=nza, oz=oz, d=d, dt=dt, nt=nt, true=true, start=start,
+                src=w[None, :], sx=np.array(sxs, np.float32), sz=np.full(nshots, 0.01, np.float32), rx=rx,
+                rz=np.full(len(rx), oz + 0.01, np.float32), rzw=np.full(len(rx), 0.01, np.float32), params=params,
+                seismotype=1)
+
+
+def ae_fwi_small(nshots=6, nt=1201):
+    """The acoustic-elastic FWI model on a grid the reference's CPU build
+    inverts in minutes: 10 m cells, a 2 km line (201 cells), the 200 m water
+    layer (21 fluid rows) over 600 m of elastic grid (61 rows), dt 1 ms."""
+    return ae_fwi(nx=201, nz=61, nza=21, d=0.01, dt=1e-3, nt=nt, nshots=nshots)

@@ -379,6 +379,30 @@ class Reference(_Lib):
             raise RuntimeError("reference acoustic-elastic misfit/gradient failed")
         return syn, g
 
+    def fwi_lbfgs(self, kind, par, nx, nz, d, oz, nt, dt, sx, sz, rx, rz, rzw, src, obs, model_raw, niter,
+                  ls_a1=0.0):
+        """The reference's FWI solver stack (nlls_fwi_eco + lbfgs with the
+        regular Wolfe line search, ref_fwi_lbfgs) for niter iterations from
+        model_raw [npar][nx][nz].  sx, sz: one source position per shot; rx,
+        rz (and rzw, the fluid-layer depths for kind 3): the receivers every
+        shot records; src [ncs][ns][nt]; obs [nc][ns * nr][nt].  Returns (the
+        final model, the objective function per iteration)."""
+        vp = ctypes.c_void_p
+        f = self.lib.ref_fwi_lbfgs
+        f.argtypes = [ctypes.c_int, ctypes.POINTER(Par), ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                      ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, vp,
+                      vp, vp, vp, ctypes.c_int, ctypes.c_double, vp]
+        sx, sz, rx, rz = self.arr(sx), self.arr(sz), self.arr(rx), self.arr(rz)
+        rzw = self.arr(rz if rzw is None else rzw)
+        m = self.arr(model_raw).copy()
+        s, o = self.arr(src), self.arr(obs)
+        func = np.zeros(niter + 1, self.dtype)
+        n = f(kind, ctypes.byref(par), nx, nz, d, d, oz, nt, dt, len(sx), _ptr(sx), _ptr(sz), len(rx), _ptr(rx),
+              _ptr(rz), _ptr(rzw), _ptr(s), _ptr(o), _ptr(m), niter, float(ls_a1), _ptr(func))
+        if n < 0:
+            raise RuntimeError("reference FWI solver run failed")
+        return m, func[:n].copy()
+
     def _real(self):
         return ctypes.c_float if self.dtype == np.float32 else ctypes.c_double
 

@@ -13,7 +13,7 @@ if [ ! -d "$REF/src/cpp" ]; then
     exit 0
 fi
 mkdir -p "$OUT"
-SRCS="we_op.cpp spatial_operators.cpp injector.cpp misc.cpp operator.cpp dummy.cpp"
+SRCS="we_op.cpp spatial_operators.cpp injector.cpp misc.cpp operator.cpp nlsolver.cpp dummy.cpp"
 for prec in 32 64; do
     B="$OUT/obj$prec"
     mkdir -p "$B"
@@ -42,7 +42,7 @@ if [ -x "$CUDA_HOME/bin/nvcc" ]; then
     mkdir -p "$B"
     INC="-I$HERE/ref_shim -I$REF/src/include -I$REF/src/cuda -I$CUDA_HOME/include"
     OBJS=""
-    for s in we_op.cpp spatial_operators.cpp injector.cpp misc.cpp operator.cpp; do
+    for s in we_op.cpp spatial_operators.cpp injector.cpp misc.cpp operator.cpp nlsolver.cpp; do
         o="$B/${s%.cpp}.o"
         g++ -std=c++11 -O3 -fopenmp -fPIC -fpermissive -w -DCUDA $INC -c "$REF/src/cpp/$s" -o "$o"
         OBJS="$OBJS $o"
@@ -71,7 +71,7 @@ if [ -x "$CUDA_HOME/bin/nvcc" ] && [ -f "$LIB" ] && [ -d "$OUT/objcuda" ]; then
     g++ -std=c++11 -O3 -fopenmp -fPIC -w -DCUDA $INC -c "$HERE/../fwi2d_b200/integration/we_op_b200.cpp" \
         -o "$B/we_op_b200.o"
     OBJS=""
-    for s in we_op spatial_operators injector misc operator ispc_loops stubs ref_driver; do
+    for s in we_op spatial_operators injector misc operator nlsolver ispc_loops stubs ref_driver; do
         OBJS="$OBJS $B/$s.o"
     done
     g++ -shared -fopenmp -o "$OUT/libfwi2d_ref32_b200.so" $OBJS "$B/we_op_b200.o" \

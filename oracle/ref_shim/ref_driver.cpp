@@ -3,11 +3,13 @@
 // spatial_operators.cpp, injector.cpp, misc.cpp, operator.cpp, dummy.cpp) by
 // oracle/build_ref.sh into oracle/_ref/.  Used to generate tests/golden/ and
 // to pin the restatement in oracle/fwi2d_oracle.c.
+#include <algorithm>
 #include <vector>
 #include <memory>
 #include <cstdio>
 #include <cstring>
 #include "we_op.hpp"
+#include "nlsolver.hpp"
 #include "IO.hpp"
 
 struct ref_param {
@@ -450,6 +452,78 @@ int ref_propagate(int kind, int adj, const data_t *model, const data_t *allsrc, 
         return -1;
     }
     return 0;
+}
+
+
+// A full-waveform inversion run of the reference's own solver stack, as
+// main/fwi2d.cpp:234-356 assembles it with no model preconditioner,
+// regularization, mask, weights or filter: nlls_fwi_eco
+// (optimization.hpp:462-915) over the wave-equation operator of `kind`
+// (0 elastic, 1 VTI, 2 acoustic, 3 acoustic-elastic) and the lbfgs solver
+// (nlsolver.hpp:308-335, nlsolver.cpp:1207-1345) with the regular_wolfe line
+// search, the parameter defaults of param.hpp:58-73 (c1 = 1e-4, c2 = 0.9,
+// a0 = 1, max step 1e6, 10 trials, 5 pairs) and the initial step fraction
+// ls_a1 of the model norm, for niter iterations.  ns shots at (sx[s], sz[s]);
+// every shot records the same nr receivers at (rx, rz) -- for kind 3 also at
+// (rx, rzw) in the fluid layer above the grid, whose first row lies at depth
+// oz.  src is the reference's allsrc [ncs][ns][nt]; obs [nc][ns * nr][nt] (the
+// operator's range: component, then shot-major traces); model
+// [npar][nx][nz] holds the starting model (vp, vs, rho ...) on input and the
+// final model on output; func receives the objective function of every
+// iteration (at most niter + 1 values).  Returns the number of values, or -1.
+int ref_fwi_lbfgs(int kind, const ref_param *rp, int nx, int nz, double dx, double dz, double oz, int nt, double dt,
+                  int ns, const data_t *sx, const data_t *sz, int nr, const data_t *rx, const data_t *rz,
+                  const data_t *rzw, const data_t *src, const data_t *obs, data_t *model, int niter, double ls_a1,
+                  data_t *func)
+{
+    try {
+        param par = to_param(rp);
+        par.nt = nt;
+        par.dt = (data_t)dt;
+        par.sub = rp->sub > 0 ? rp->sub : 1;
+        par.ns = ns;
+        par.nr = ns * nr;
+        par.nmodels = kind == 1 ? 5 : (kind == 2 ? 2 : 3);
+        par.acoustic_elastic = kind == 3;
+        par.seismotype = 1;
+        par.resampling = "linear";
+        par.niter = niter;
+        par.verbose = 0;
+        par.sxz.clear();
+        par.rxz.clear();
+        par.rxza.clear();
+        for (int s = 0; s < ns; s++) {
+            par.sxz.push_back({sx[s], sz[s], 0});
+            par.rxz.push_back(locs(nr, rx, rz));
+            if (kind == 3) par.rxza.push_back(locs(nr, rx, rzw));
+        }
+        const int ncs = (kind == 2 || (kind == 3 && par.acoustic_source)) ? 1 : 2;
+        hypercube<data_t> dom(axis<data_t>(nz, (data_t)oz, (data_t)dz), axis<data_t>(nx, 0, (data_t)dx),
+                              axis<data_t>(par.nmodels, 0, 1));
+        auto allsrc = std::make_shared<vecReg<data_t> >(
+            hypercube<data_t>(axis<data_t>(nt, 0, (data_t)dt), axis<data_t>(ns, 0, 1), axis<data_t>(ncs, 0, 1)));
+        std::memcpy(allsrc->getVals(), src, (size_t)ncs * ns * nt * sizeof(data_t));
+        std::unique_ptr<nl_we_op> L;
+        if (kind == 0) L.reset(new nl_we_op_e(dom, allsrc, par));
+        else if (kind == 1) L.reset(new nl_we_op_vti(dom, allsrc, par));
+        else if (kind == 2) L.reset(new nl_we_op_a(dom, allsrc, par));
+        else L.reset(new nl_we_op_ae(dom, allsrc, par));
+        auto m = std::make_shared<vecReg<data_t> >(dom);
+        std::memcpy(m->getVals(), model, m->getN123() * sizeof(data_t));
+        auto d = std::make_shared<vecReg<data_t> >(*L->getRange());
+        std::memcpy(d->getVals(), obs, d->getN123() * sizeof(data_t));
+        nlls_fwi_eco prob(L.get(), m, d);
+        regular_wolfe ls(par.ls_c1, par.ls_c2, par.ls_a0, (data_t)ls_a1, par.ls_max_step, par.ls_version);
+        lbfgs solver(niter, par.max_trial, par.threshold, &ls, nullptr, par.lbfgs_m);
+        solver.run(&prob, false, "none", par.isave, par.format, "none");
+        std::memcpy(model, m->getCVals(), m->getN123() * sizeof(data_t));
+        const int nf = (int)std::min<size_t>(solver._func.size(), (size_t)niter + 1);
+        for (int i = 0; i < nf; i++) func[i] = solver._func[i];
+        return nf;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "ref_fwi_lbfgs: %s\n", e.what());
+        return -1;
+    }
 }
 
 }

@@ -97,3 +97,37 @@ def rel_l2(a, b):
     b = np.asarray(b, np.float64)
     nb = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0))
+
+
+def ae_fwi_par(wl):
+    """The reference's param of an acoustic-elastic FWI workload
+    (fwi2d_b200.workloads.ae_fwi), for one shot."""
+    p = wl["params"]
+    keys = ("nt", "sub", "dt", "bc_top", "bc_bottom", "bc_left", "bc_right", "taper_top", "taper_bottom",
+            "taper_left", "taper_right", "taper_strength")
+    return O.make_par(**{k: p[k] for k in keys}, ns=1, nr=len(wl["rx"]), nza=p["nza"],
+                      acoustic_source=p["acoustic_source"])
+
+
+def ae_fwi_observed(lib, wl):
+    """Observed data of an acoustic-elastic FWI workload, modelled shot by shot
+    on its true model by the reference's operator (ref_misfit_grad_ae) in the
+    layout of its multi-shot range: [3][ns * nr][nt] (fluid, x, z)."""
+    par = ae_fwi_par(wl)
+    nr, ns, nt = len(wl["rx"]), len(wl["sx"]), wl["nt"]
+    obs = np.zeros((3, ns * nr, nt), np.float32)
+    for s in range(ns):
+        syn, _ = lib.misfit_grad_ae(par, wl["nx"], wl["nz"], wl["d"], wl["oz"], nt, wl["dt"],
+                                    (wl["sx"][s], wl["sz"][s]), wl["rx"], wl["rz"], wl["rzw"], wl["true"], wl["src"])
+        obs[:, s * nr:(s + 1) * nr] = syn
+    return obs
+
+
+def ae_fwi_lbfgs(lib, wl, obs, niter, ls_a1):
+    """The reference's L-BFGS FWI (ref_fwi_lbfgs) of an acoustic-elastic
+    workload from its starting model; returns (final model, misfit per
+    iteration)."""
+    ns, nt = len(wl["sx"]), wl["nt"]
+    src = np.ascontiguousarray(np.broadcast_to(wl["src"][:, None, :], (1, ns, nt)), np.float32)
+    return lib.fwi_lbfgs(O.KIND_AE, ae_fwi_par(wl), wl["nx"], wl["nz"], wl["d"], wl["oz"], nt, wl["dt"], wl["sx"],
+                         wl["sz"], wl["rx"], wl["rz"], wl["rzw"], src, obs, wl["start"], niter, ls_a1)

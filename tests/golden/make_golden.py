@@ -6,7 +6,7 @@ seeded cases and stores inputs and outputs.  The tests check the oracle's C
 restatement and the library's host tables against these files; they never
 need the reference tree.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--lbfgs-only]
 """
 import os
 import sys
@@ -345,9 +345,29 @@ def fwi_case_ae_resampled():
                 true=true, start=start, src=src, obs_sinc=obs, grad_sinc=g, misfit_sinc=0.5 * np.sum(w * r * r))
 
 
+LBFGS_ITERS, LBFGS_A1 = 20, 0.01
+
+
+def fwi_lbfgs_ae_case():
+    """The reference's L-BFGS FWI (main/fwi2d.cpp's solver stack through
+    ref_fwi_lbfgs) on the small acoustic-elastic FWI workload, 20 iterations,
+    initial step 1 % of the model norm: the objective function per iteration
+    and the final model.  The observed data are not stored: the tests model
+    them again with the reference build (tests/cases.py ae_fwi_observed)."""
+    from fwi2d_b200 import workloads as W
+    lib = O.Reference(32)
+    wl = W.ae_fwi_small()
+    obs = K.ae_fwi_observed(lib, wl)
+    m, f = K.ae_fwi_lbfgs(lib, wl, obs, LBFGS_ITERS, LBFGS_A1)
+    return dict(niter=LBFGS_ITERS, ls_a1=LBFGS_A1, func=f, model=m, obs_norm=np.linalg.norm(obs.astype(np.float64)))
+
+
 def main():
     if not O.have_reference(32):
         sys.exit("oracle/_ref is not built (oracle/build_ref.sh needs the reference tree)")
+    if "--lbfgs-only" in sys.argv:   # the solver run alone takes minutes
+        np.savez_compressed(os.path.join(HERE, "fwi_lbfgs_ae_f32.npz"), **fwi_lbfgs_ae_case())
+        return
     for prec in (32, 64):
         for name, kind, mt, bc, nx, nz, nt in CASES:
             out = elastic_like(name, kind, mt, bc, nx, nz, nt, prec)
@@ -366,6 +386,7 @@ def main():
                         **fwi_case_resampled(O.KIND_VTI, ("sinc",)))
     np.savez_compressed(os.path.join(HERE, "fwi_gradient_acoustic_resampled_f32.npz"),
                         **fwi_case_resampled(O.KIND_ACOUSTIC, ("linear",)))
+    np.savez_compressed(os.path.join(HERE, "fwi_lbfgs_ae_f32.npz"), **fwi_lbfgs_ae_case())
     print("golden fixtures written to", HERE)
 
 

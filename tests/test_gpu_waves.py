@@ -8,7 +8,8 @@ forward, residual and adjoint wave by wave, summing the gradient over all
 shots.  FWI2D_SNAPSHOT_BUDGET replaces the budget so that a small batch
 splits here.
 
-Checks, for the elastic and VTI propagators, on the tile and the marching
+Checks, for the elastic and VTI propagators on the tile and the marching
+plans, and for the acoustic and acoustic-elastic propagators on their tile
 plans: a batch of uneven shots (cropped grids, uneven record lengths) split
 into three or more waves gives the same gradient and misfit as the same
 batch in one wave, bitwise; its plan holds the snapshots of one wave only;
@@ -35,10 +36,16 @@ SHOTS = [  # x0, nx, nt, source x offset (cells), receivers
 ]
 
 
+NZA = 14   # fluid rows of the acoustic-elastic batch
+
+
 def _batch(kind):
     nxm, nz, d, dt = 160, 72, 2.0 ** -7, 1e-3
-    raw = K.model_case(kind, nxm, nz, d, seed=21)
-    true = K.model_case(kind, nxm, nz, d, seed=22)
+    ae = kind == O.KIND_AE
+    mkind = O.KIND_ELASTIC if ae else kind
+    raw = K.model_case(mkind, nxm, nz, d, seed=21)
+    true = K.model_case(mkind, nxm, nz, d, seed=22)
+    oz = (NZA - 1) * d
     specs, srcs = [], []
     for x0, nx, nt, sxo, nr in SHOTS:
         sx = np.array([(x0 + sxo + 0.25) * d], np.float32)
@@ -46,25 +53,34 @@ def _batch(kind):
         step = (nx - 8) // nr
         rx = ((x0 + 3.25 + step * np.arange(nr)) * d).astype(np.float32)
         rz = np.full(nr, 2.25 * d, np.float32)
-        specs.append(F.ShotSpec(x0, nx, nt, sx, sz, rx, rz))
-        srcs.append(K.sources(2, nt, dt))
-    pd = K.par_dict(nt=max(s[2] for s in SHOTS), dt=dt, bc=(1, 2, 2, 2), taper=(0, 8, 8, 8))
+        if ae:
+            # source in the water; receivers below the seabed and in the water
+            specs.append(F.ShotSpec(x0, nx, nt, [0.0], [oz], rx, rz + oz, water_src_x=sx, water_src_z=sz,
+                                    water_rcv_x=rx, water_rcv_z=rz + d))
+        else:
+            specs.append(F.ShotSpec(x0, nx, nt, sx, sz, rx, rz))
+        srcs.append(K.sources(1 if kind in (O.KIND_ACOUSTIC, O.KIND_AE) else 2, nt, dt))
+    extra = dict(nza=NZA, acoustic_source=1) if ae else {}
+    pd = K.par_dict(nt=max(s[2] for s in SHOTS), dt=dt, bc=(2, 2, 2, 2) if ae else (1, 2, 2, 2),
+                    taper=(4, 8, 8, 8) if ae else (0, 8, 8, 8), **extra)
     return raw, true, specs, srcs, pd, d
 
 
 def _gradient(kind, raw, true, specs, srcs, pd, d, shape):
     P = F.Propagator(0)
-    P.set_model(kind, K.converted(kind, true), d, d)
+    mkind = O.KIND_ELASTIC if kind == O.KIND_AE else kind
+    oz = (NZA - 1) * d if kind == O.KIND_AE else 0.0
+    P.set_model(kind, K.converted(mkind, true), d, d, 0.0, oz)
     P.set_shots(F.make_params(**pd, tile_shape=shape), specs)
     obs = P.forward(srcs, store=False)
-    mc = K.converted(kind, raw)
+    mc = K.converted(mkind, raw)
     g, phi = P.fwi_gradient(mc, srcs, obs)
     info = P.plan_info()
     return P, g, phi, info
 
 
-@pytest.mark.parametrize("kind", [O.KIND_ELASTIC, O.KIND_VTI])
-@pytest.mark.parametrize("shape", [3, 8])
+@pytest.mark.parametrize("kind,shape", [(O.KIND_ELASTIC, 3), (O.KIND_ELASTIC, 8), (O.KIND_VTI, 3), (O.KIND_VTI, 8),
+                                        (O.KIND_ACOUSTIC, 3), (O.KIND_AE, 3)])
 def test_waves_match_one_wave(kind, shape, monkeypatch):
     raw, true, specs, srcs, pd, d = _batch(kind)
     P1, g1, phi1, info1 = _gradient(kind, raw, true, specs, srcs, pd, d, shape)

@@ -16,7 +16,8 @@ from tests import cases as K
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FILES = sorted(f for f in glob.glob(os.path.join(GOLD, "*.npz"))
-               if not os.path.basename(f).startswith(("fwi_gradient_", "resample_", "analyze_model_", "dipole_")))
+               if not os.path.basename(f).startswith(("fwi_gradient_", "fwi_lbfgs_", "resample_", "analyze_model_",
+                                                      "dipole_")))
 FWI_FILES = sorted(glob.glob(os.path.join(GOLD, "fwi_gradient_*.npz")))
 
 
