@@ -82,12 +82,11 @@ def peaks():
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one adjoint
 # step of the single-shot grid on the framed tile plan (shape 16): the core
-# launch and the x-band launch from the capture summarised in
-# profiles/elastic_step_framed_single_shot_401x801.md, the z-band launch from
-# profiles/elastic_zband_single_shot_401x801.md (cold caches: ncu flushes L2
-# before each pass); and the core launch's L1-to-L2 bytes.
+# launch, the x-band launch and the z-band launch from the captures summarised
+# in profiles/elastic_step_framed_single_shot_401x801.md (cold caches: ncu
+# flushes L2 before each pass); and the core launch's L1-to-L2 bytes.
 FRAMED_SHAPE = 16
-ADJ_STEP_TRAFFIC_BYTES = {"core": 21.133312e6, "x_bands": 0.554496e6, "z_bands": None}
+ADJ_STEP_TRAFFIC_BYTES = {"core": 21.133312e6, "x_bands": 0.554496e6, "z_bands": 3.61984e6}
 ADJ_CORE_L2_BYTES, ADJ_CORE_COLD_US = 1447280 * 32, 28.576
 
 

@@ -1524,7 +1524,7 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
     CK(cudaEventRecord(ctx->fork, st));
     CK(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
     CK(cudaStreamWaitEvent(ctx->side2, ctx->fork, 0));
-    launch_elastic_step(P.tshape, P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
+    launch_elastic_xband(P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
     launch_elastic_zband(P.kind == KIND_VTI, P.d_bands.as<BandRef>() + R.b0, R.b1 - R.b0, shots, md, P.C, it, flags,
                          P.dtg, ctx->side2);
     n += 2;

@@ -126,9 +126,15 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 #ifndef CORE_MIN_BLOCKS
 #define CORE_MIN_BLOCKS 2
 #endif
-template <bool VTI, int RZ, int TX, bool GRAD, bool AE, bool CORE = false>
-__global__ void __launch_bounds__(32 * TX, TX == 8 ? (RZ == 1 ? TILE_MIN_BLOCKS : (CORE ? CORE_MIN_BLOCKS : 1))
-                                                   : (CORE && RZ == 1 ? 2 : 1))
+// BAND: the instantiation for the full-height x-band windows of framed and
+// marching plans.  Few CTAs run it and it sets the step's critical path, so
+// it is compiled without the occupancy bound (no register spills) and, in
+// the imaging condition, loads its snapshot and gradient operands before the
+// stencil arithmetic so that their latency overlaps it.
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE, bool CORE = false, bool BAND = false>
+__global__ void __launch_bounds__(32 * TX, BAND ? 1
+                                               : (TX == 8 ? (RZ == 1 ? TILE_MIN_BLOCKS : (CORE ? CORE_MIN_BLOCKS : 1))
+                                                          : (CORE && RZ == 1 ? 2 : 1)))
 elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C,
              int it, int flags, float dtg)
 {
@@ -706,6 +712,27 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             const int wi = (tx + 2) * WZ + (tz + 2);
             const int cell = gx * ldz + gz;
             const int mcell = gx * mld + gz;
+            // BAND: the imaging condition's global operands, loaded ahead
+            float hfp0 = 0.f, hfp1 = 0.f, hfm0 = 0.f, hfm1 = 0.f, hg0 = 0.f, hg1 = 0.f, hg2 = 0.f;
+            if (BAND && GRAD && do_grad) {
+                const int last = nt / C.sub;
+                if (itf + 1 <= last) {
+                    const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf + 1);
+                    const long long o = (long long)(itf + 1) * slot_elems + cell;
+                    hfp0 = snap_load(snap, o, prec, inv);
+                    hfp1 = snap_load(snap, o + nxz, prec, inv);
+                }
+                if (itf > 0) {
+                    const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
+                    const long long o = (long long)(itf - 1) * slot_elems + cell;
+                    hfm0 = snap_load(snap, o, prec, inv);
+                    hfm1 = snap_load(snap, o + nxz, prec, inv);
+                }
+                const float *g = Sp->grad + cell;
+                hg0 = g[0];
+                hg1 = g[nxz];
+                hg2 = g[2 * nxz];
+            }
             if (store) {
                 const int slot = it / C.sub;
                 const float sc = prec == SNAP_FP32 ? 1.f : snap_scale(Sp->snap_amax, slot);
@@ -839,14 +866,14 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 const float az0 = CZ[wi], ax1 = BX[wi];
                 const int last = nt / C.sub;
                 const float f0 = F0[wi], f1 = F1[wi];
-                float fp0 = 0.f, fp1 = 0.f, fm0 = 0.f, fm1 = 0.f;
-                if (itf + 1 <= last) {
+                float fp0 = hfp0, fp1 = hfp1, fm0 = hfm0, fm1 = hfm1;
+                if (!BAND && itf + 1 <= last) {
                     const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf + 1);
                     const long long o = (long long)(itf + 1) * slot_elems + cell;
                     fp0 = snap_load(snap, o, prec, inv);
                     fp1 = snap_load(snap, o + nxz, prec, inv);
                 }
-                if (itf > 0) {
+                if (!BAND && itf > 0) {
                     const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
                     const long long o = (long long)(itf - 1) * slot_elems + cell;
                     fm0 = snap_load(snap, o, prec, inv);
@@ -868,23 +895,26 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 const double wdt = (double)gw * 1.0 / (double)dtg;
                 // acoustic-elastic interface row: the density term needs the coupled uz (ae_couple)
                 const bool rho_here = !AE || gz != 0;
+                const float G0 = BAND ? hg0 : *g0, G1 = BAND ? hg1 : *g1;
                 if (itf > 0 && itf < last) {
-                    if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
-                    else *g0 = *g0 + gw * dtg * dl;
-                    *g1 = *g1 + gw * dtg * dm;
+                    if (!VTI) *g0 = G0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                    else *g0 = G0 + gw * dtg * dl;
+                    *g1 = G1 + gw * dtg * dm;
                     if (rho_here)
-                        *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
+                        *g2 = (float)((double)(BAND ? hg2 : *g2) +
+                                      wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
                 } else if (itf == 0) {
                     const double wh = (double)gw * 0.5 * (double)dtg;
-                    if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
-                    else *g0 = (float)((double)*g0 + wh * (double)dl);
-                    *g1 = (float)((double)*g1 + wh * (double)dm);
-                    *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
+                    if (!VTI) *g0 = (float)((double)G0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
+                    else *g0 = (float)((double)G0 + wh * (double)dl);
+                    *g1 = (float)((double)G1 + wh * (double)dm);
+                    *g2 = (float)((double)(BAND ? hg2 : *g2) + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
                 } else {
-                    if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
-                    else *g0 = *g0 + gw * dtg * dl;
-                    *g1 = *g1 + gw * dtg * dm;
-                    if (rho_here) *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
+                    if (!VTI) *g0 = G0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                    else *g0 = G0 + gw * dtg * dl;
+                    *g1 = G1 + gw * dtg * dm;
+                    if (rho_here)
+                        *g2 = (float)((double)(BAND ? hg2 : *g2) + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
                 }
             }
         }
@@ -1033,18 +1063,19 @@ static constexpr size_t elastic_smem_bytes()
     return sizeof(float) * (2 * UX * UZ + (5 + ((VTI || AE) ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX);
 }
 
-template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false, bool CORE = false>
+template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false, bool CORE = false, bool BAND = false>
 static void launch_elastic_g(const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
                              const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
     constexpr size_t bytes = elastic_smem_bytes<VTI, RZ, TX, GRAD, AE>();
     static bool configured = false;   // per process; a kernel attribute applies to every device
     if (!configured) {
-        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD, AE, CORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)bytes);
+        cudaFuncSetAttribute(elastic_step<VTI, RZ, TX, GRAD, AE, CORE, BAND>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         configured = true;
     }
-    elastic_step<VTI, RZ, TX, GRAD, AE, CORE><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags, dtg);
+    elastic_step<VTI, RZ, TX, GRAD, AE, CORE, BAND><<<ntiles, 32 * TX, bytes, st>>>(shots, tiles, M, C, it, flags,
+                                                                                    dtg);
 }
 
 template <bool VTI, int RZ, int TX>
@@ -1067,6 +1098,20 @@ void elastic_tile_shape(int i, int *tz, int *tx)
     static const int s[4][2] = {{64, 16}, {64, 8}, {32, 16}, {32, 8}};
     *tz = s[i][0];
     *tx = s[i][1];
+}
+
+void launch_elastic_xband(bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    if (ntiles <= 0) return;
+    const bool grad = (flags & F_GRAD) != 0;
+    if (vti) {
+        if (grad) launch_elastic_g<true, 1, 8, true, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+        else launch_elastic_g<true, 1, 8, false, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+    } else {
+        if (grad) launch_elastic_g<false, 1, 8, true, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+        else launch_elastic_g<false, 1, 8, false, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
+    }
 }
 
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,

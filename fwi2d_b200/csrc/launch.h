@@ -12,6 +12,9 @@ void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const 
 int elastic_tile_count();
 void elastic_tile_shape(int i, int *tz, int *tx);
 // core: interior windows of a framed plan (the tile kernel's lean paths only)
+// the x-band windows (32 x 8, full height) of framed and marching plans
+void launch_elastic_xband(bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
+                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st,
                          bool core = false);

@@ -80,7 +80,9 @@ __device__ __forceinline__ void d2acc(float &acc, const float *pu, int su, const
         float fk[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) fk[k] = fs * bf[dir * k * sf];
-#pragma unroll
+        // rolled over the eight samples (the unrolled closure overflows the
+        // instruction cache of the latency-bound band kernels)
+#pragma unroll 1
         for (int jj = 0; jj < 8; jj++) {
             float val = 0.f;
 #pragma unroll

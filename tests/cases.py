@@ -123,11 +123,27 @@ def ae_fwi_observed(lib, wl):
     return obs
 
 
+LBFGS_OMP_THREADS = 8
+
+
+def set_omp_threads(n):
+    """Thread count of the OpenMP parallel regions this process starts from
+    now on (libgomp's omp_set_num_threads, shared by the reference builds).
+    The reference sums its FP32 objective function with an OpenMP reduction
+    whose partial sums follow the thread count: runs that compare misfits to
+    1e-4 use the same count."""
+    import ctypes
+    import ctypes.util
+    name = ctypes.util.find_library("gomp") or "libgomp.so.1"
+    ctypes.CDLL(name).omp_set_num_threads(int(n))
+
+
 def ae_fwi_lbfgs(lib, wl, obs, niter, ls_a1):
     """The reference's L-BFGS FWI (ref_fwi_lbfgs) of an acoustic-elastic
-    workload from its starting model; returns (final model, misfit per
-    iteration)."""
+    workload from its starting model, on LBFGS_OMP_THREADS OpenMP threads;
+    returns (final model, misfit per iteration)."""
     ns, nt = len(wl["sx"]), wl["nt"]
     src = np.ascontiguousarray(np.broadcast_to(wl["src"][:, None, :], (1, ns, nt)), np.float32)
+    set_omp_threads(LBFGS_OMP_THREADS)
     return lib.fwi_lbfgs(O.KIND_AE, ae_fwi_par(wl), wl["nx"], wl["nz"], wl["d"], wl["oz"], nt, wl["dt"], wl["sx"],
                          wl["sz"], wl["rx"], wl["rz"], wl["rzw"], src, obs, wl["start"], niter, ls_a1)
