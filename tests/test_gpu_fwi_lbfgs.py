@@ -23,10 +23,12 @@ the CPU build's on every shot.  The reference sums its FP32 objective
 function with an OpenMP reduction whose partial sums follow the thread
 count (a different count moved the first misfit by 1.7e-4), so both runs use
 8 threads (tests/cases.py set_omp_threads); the order in which the threads'
-partial sums combine still varies, at the level of rounding.  Checks: the
-objective function of every iteration agrees with the CPU run's to 1e-4
-relative, the final models to 1e-4 relative L2 (the north-star gradient
-bar), and both runs reduce the misfit by more than half.
+partial sums combine still varies, at the level of rounding, and two CPU
+runs differ by up to 6e-6 of the starting misfit at some iterations.
+Checks: the objective function of every iteration agrees with the CPU
+run's to 1e-4 of the starting misfit (measured: at most 2e-5), the final
+models to 1e-4 relative L2 (the north-star gradient bar; measured 9e-6),
+and both runs reduce the misfit by more than half.
 """
 import os
 import time
@@ -66,7 +68,7 @@ def test_ae_lbfgs_fwi_through_hook_matches_reference_cpu_run():
           "final models rel L2 %.2e" % (f[-1] / f[0], fc[-1] / fc[0], err(wl["start"]), err(m), err(mc),
                                         K.rel_l2(m, mc)))
     assert len(f) == len(fc)
-    assert np.all(np.abs(f - fc) <= TOL * np.abs(fc))
+    assert np.all(np.abs(f - fc) <= TOL * fc[0])
     assert K.rel_l2(m, mc) <= TOL
     assert f[-1] < 0.5 * f[0] and fc[-1] < 0.5 * fc[0]
     assert err(m) < err(wl["start"])
