@@ -59,6 +59,37 @@ __device__ __forceinline__ float snap_load(const void *base, long long idx, int 
 }
 
 
+// 4-byte asynchronous copy global -> shared (cp.async, no register staging)
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The 4-byte word holding snapshot sample idx: the sample itself (FP32), or
+// the pair of 16-bit samples that contains it.
+__device__ __forceinline__ const void *snap_word(const void *base, long long idx, int prec)
+{
+    if (prec == SNAP_FP32) return (const float *)base + idx;
+    return (const unsigned short *)base + (idx & ~1LL);
+}
+// snap_load on a word copied by snap_word
+__device__ __forceinline__ float snap_from_word(float w, long long idx, int prec, float inv)
+{
+    if (prec == SNAP_FP32) return w;
+    const unsigned u = __float_as_uint(w);
+    const unsigned short h = (unsigned short)((idx & 1) ? (u >> 16) : (u & 0xffffu));
+    if (prec == SNAP_BF16) return __bfloat162float(__ushort_as_bfloat16(h)) * inv;
+    return __half2float(__ushort_as_half(h)) * inv;
+}
+
+// Per-thread slots of the scalar interior path: the operands of the thread's
+// own cell, copied into shared memory at the start of the step.
+enum OwnSlot { OS_P0 = 0, OS_P1, OS_RHO, OS_FP0, OS_FP1, OS_FM0, OS_FM1, OS_G0, OS_G1, OS_G2, OS_EPS, OS_V2, OS_V3 };
+template <bool VTI, bool GRAD>
+constexpr int own_slots() { return GRAD ? (VTI ? 13 : 10) : 3; }
+
 // ---------------------------------------------------------------------------
 // Elastic isotropic / VTI step.
 // ---------------------------------------------------------------------------
@@ -155,6 +186,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     float *F0 = T1 + ((VTI || AE) ? WX * WZ : 0);
     float *F1 = F0 + (GRAD ? WX * WZ : 0);
     float *red = F1 + (GRAD ? WX * WZ : 0);
+    float *OWN = red + TX;         // scalar interior path: own_slots() x NT per-thread slots
 
     const TileRef tr = tiles[blockIdx.x];
     const ShotDev *__restrict__ Sp = shots + tr.shot;
@@ -188,6 +220,43 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     if (GRAD && do_grad && prec != SNAP_FP32) finv = 1.f / snap_scale(Sp->snap_amax, itf);
     const long long slot_elems = Sp->snap_slot;
     const void *snap = Sp->snap;
+
+    // scalar interior path: start the copies of the own cell's operands (prev,
+    // rho; for the imaging condition the neighbouring snapshots, the gradient
+    // and the VTI coefficients) so that their latency overlaps phases 1 and 2;
+    // each thread waits for its own copies in phase 3
+    if (RZ == 1 && !AE && lean1) {
+        const int gx = wx0 + (int)(threadIdx.x >> 5), gz = wz0 + (int)(threadIdx.x & 31);
+        if (gx >= tr.ox0 && gx < tr.ox1 && gz >= tr.oz0 && gz < tr.oz1) {
+            float *own = OWN + threadIdx.x;
+            const long long cell = (long long)gx * ldz + gz, mcell = (long long)gx * mld + gz;
+            cp_async4(own + OS_P0 * NT, pn + cell);
+            cp_async4(own + OS_P1 * NT, pn + nxz + cell);
+            cp_async4(own + OS_RHO * NT, mp2 + mcell);
+            if (GRAD && do_grad) {
+                const int last = nt / C.sub;
+                if (itf + 1 <= last) {
+                    const long long o = (long long)(itf + 1) * slot_elems + cell;
+                    cp_async4(own + OS_FP0 * NT, snap_word(snap, o, prec));
+                    cp_async4(own + OS_FP1 * NT, snap_word(snap, o + nxz, prec));
+                }
+                if (itf > 0) {
+                    const long long o = (long long)(itf - 1) * slot_elems + cell;
+                    cp_async4(own + OS_FM0 * NT, snap_word(snap, o, prec));
+                    cp_async4(own + OS_FM1 * NT, snap_word(snap, o + nxz, prec));
+                }
+                const float *g = Sp->grad + cell;
+                cp_async4(own + OS_G0 * NT, g);
+                cp_async4(own + OS_G1 * NT, g + nxz);
+                cp_async4(own + OS_G2 * NT, g + 2 * (long long)nxz);
+                if (VTI) {
+                    cp_async4(own + OS_EPS * NT, M.eps + mofs + mcell);
+                    cp_async4(own + OS_V2 * NT, M.gv2 + mofs + mcell);
+                    cp_async4(own + OS_V3 * NT, M.gv3 + mofs + mcell);
+                }
+            }
+        }
+    }
 
     // ---- phase 1: curr with a 4-cell halo, coefficients (and snapshot) with a 2-cell halo
     // (vector loads for interior tiles that start on a multiple of 4 cells)
@@ -596,7 +665,6 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
         const int ui = (warp + 4) * UZ + (lane + 4);
         const int wi = (warp + 2) * WZ + (lane + 2);
         const int cell = gx * ldz + gz;
-        const int mcell = gx * mld + gz;
         if (store) {
             const int slot = it / C.sub;
             const float sc = prec == SNAP_FP32 ? 1.f : snap_scale(Sp->snap_amax, slot);
@@ -632,12 +700,14 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             }
         }
         const float tzv = Sp->tz[gz], txv = Sp->tx[gx];
-        float p0 = pn[cell], p1 = pn[nxz + cell];
+        cp_async_wait_all();
+        const float *own = OWN + threadIdx.x;
+        float p0 = own[OS_P0 * NT], p1 = own[OS_P1 * NT];
         if (it > 0) {
             p0 = p0 * tzv * txv;
             p1 = p1 * tzv * txv;
         }
-        const float rho = mp2[mcell];
+        const float rho = own[OS_RHO * NT];
         n0 = C.dt2 * n0 / rho + 2 * U0[ui] - p0;
         n1 = C.dt2 * n1 / rho + 2 * U1[ui] - p1;
         n0 = n0 * tzv * txv;
@@ -659,45 +729,45 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             if (itf + 1 <= last) {
                 const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf + 1);
                 const long long o = (long long)(itf + 1) * slot_elems + cell;
-                fp0 = snap_load(snap, o, prec, inv);
-                fp1 = snap_load(snap, o + nxz, prec, inv);
+                fp0 = snap_from_word(own[OS_FP0 * NT], o, prec, inv);
+                fp1 = snap_from_word(own[OS_FP1 * NT], o + nxz, prec, inv);
             }
             if (itf > 0) {
                 const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
                 const long long o = (long long)(itf - 1) * slot_elems + cell;
-                fm0 = snap_load(snap, o, prec, inv);
-                fm1 = snap_load(snap, o + nxz, prec, inv);
+                fm0 = snap_from_word(own[OS_FM0 * NT], o, prec, inv);
+                fm1 = snap_from_word(own[OS_FM1 * NT], o + nxz, prec, inv);
             }
             float dl, dm;
             if (!VTI) {
                 dl = 0.f;
                 dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
             } else {
-                const long long mo = mofs + mcell;
-                const float e2 = 1 + 2 * M.eps[mo];
-                const float v2 = M.gv2[mo], v3 = M.gv3[mo];
+                const float e2 = 1 + 2 * own[OS_EPS * NT];
+                const float v2 = own[OS_V2 * NT], v3 = own[OS_V3 * NT];
                 dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
                 dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
             }
             float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
+            const float G0 = own[OS_G0 * NT], G1 = own[OS_G1 * NT], G2 = own[OS_G2 * NT];
             const float gw = Sp->gwt[itf];
             const double wdt = (double)gw * 1.0 / (double)dtg;
             if (itf > 0 && itf < last) {
-                if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
-                else *g0 = *g0 + gw * dtg * dl;
-                *g1 = *g1 + gw * dtg * dm;
-                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
+                if (!VTI) *g0 = G0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                else *g0 = G0 + gw * dtg * dl;
+                *g1 = G1 + gw * dtg * dm;
+                *g2 = (float)((double)G2 + wdt * (double)(n0 * (fp0 - 2 * f0 + fm0) + n1 * (fp1 - 2 * f1 + fm1)));
             } else if (itf == 0) {
                 const double wh = (double)gw * 0.5 * (double)dtg;
-                if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
-                else *g0 = (float)((double)*g0 + wh * (double)dl);
-                *g1 = (float)((double)*g1 + wh * (double)dm);
-                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
+                if (!VTI) *g0 = (float)((double)G0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
+                else *g0 = (float)((double)G0 + wh * (double)dl);
+                *g1 = (float)((double)G1 + wh * (double)dm);
+                *g2 = (float)((double)G2 + wdt * (double)(n0 * (fp0 - f0) + n1 * (fp1 - f1)));
             } else {
-                if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
-                else *g0 = *g0 + gw * dtg * dl;
-                *g1 = *g1 + gw * dtg * dm;
-                *g2 = (float)((double)*g2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
+                if (!VTI) *g0 = G0 + gw * dtg * (ax0 + az1) * (t0 + t1);
+                else *g0 = G0 + gw * dtg * dl;
+                *g1 = G1 + gw * dtg * dm;
+                *g2 = (float)((double)G2 + wdt * (double)(n0 * (-f0 + fm0) + n1 * (-f1 + fm1)));
             }
         }
         }
@@ -1060,7 +1130,8 @@ template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false>
 static constexpr size_t elastic_smem_bytes()
 {
     constexpr int TZ = 32 * RZ, UZ = TZ + 8, UX = TX + 8, WZ = TZ + 4, WX = TX + 4;
-    return sizeof(float) * (2 * UX * UZ + (5 + ((VTI || AE) ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX);
+    constexpr int own = (RZ == 1 && !AE) ? own_slots<VTI, GRAD>() * 32 * TX : 0;   // scalar interior path
+    return sizeof(float) * (2 * UX * UZ + (5 + ((VTI || AE) ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX + own);
 }
 
 template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false, bool CORE = false, bool BAND = false>
