@@ -80,20 +80,27 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one adjoint
-# step of the single-shot grid on the framed tile plan (shape 16): the core
-# launch, the x-band launch and the z-band launch from the captures summarised
-# in profiles/elastic_step_framed_single_shot_401x801.md (cold caches: ncu
-# flushes L2 before each pass); and the core launch's L1-to-L2 bytes.
-FRAMED_SHAPE = 16
-ADJ_STEP_TRAFFIC_BYTES = {"core": 21.133312e6, "x_bands": 0.554496e6, "z_bands": 3.61984e6}
-ADJ_CORE_L2_BYTES, ADJ_CORE_COLD_US = 1447280 * 32, 28.576
+# Per framed plan of the single-shot grid: DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) of the core, x-band and z-band launches of one
+# adjoint step, and the core launch's L1-to-L2 bytes, cold duration and L2
+# throughput, from the captures summarised in
+# profiles/elastic_step_framed_single_shot_401x801.md (cold caches: ncu
+# flushes L2 before each pass).
+FRAMED_CAPTURES = {
+    16: dict(core="elastic_step<RZ=2, CORE> (64 x 8 z-pair windows)",
+             traffic={"core": 21.133312e6, "x_bands": 0.554496e6, "z_bands": 3.61984e6},
+             l2_bytes=1447280 * 32, core_cold_us=28.576, lts_pct=7.0),
+    14: dict(core="elastic_step<RZ=1, CORE> (32 x 8 windows)",
+             traffic={"core": 21.152256e6, "x_bands": 0.534016e6, "z_bands": 3.607808e6},
+             l2_bytes=1651721 * 32, core_cold_us=21.312, lts_pct=10.4),
+}
 
 
 def roof_kernel(shape, config):
-    if config == "single" and shape == FRAMED_SHAPE:
-        return ("adjoint + imaging step of the framed plan: interior elastic_step<RZ=2, CORE> with the x-band "
-                "elastic_step and elastic_zband overlapped on two side streams (one step = one launch of each)")
+    if config == "single" and shape in FRAMED_CAPTURES:
+        return ("adjoint + imaging step of the framed plan: interior %s with the x-band elastic_step and "
+                "elastic_zband overlapped on two side streams (one step = one launch of each)"
+                % FRAMED_CAPTURES[shape]["core"])
     if config == "single":
         return "adjoint + imaging step (tile shape %d)" % shape
     return "adjoint loop: interior, band and imaging kernels"
@@ -101,19 +108,21 @@ def roof_kernel(shape, config):
 
 def step_traffic(shape, config):
     """DRAM bytes of one adjoint step from the committed ncu summaries, or
-    None when a part is not captured for this plan."""
-    if config != "single" or shape != FRAMED_SHAPE or None in ADJ_STEP_TRAFFIC_BYTES.values():
+    None when the plan's launches are not captured."""
+    cap = FRAMED_CAPTURES.get(shape) if config == "single" else None
+    if not cap or not cap["traffic"]:
         return None
-    return sum(ADJ_STEP_TRAFFIC_BYTES.values())
+    return sum(cap["traffic"].values())
 
 
 def l2_note(shape, config):
     """L2 figures of the L2-resident single-shot case, from the committed ncu
     capture of the core launch (cold caches)."""
-    if config != "single" or shape != FRAMED_SHAPE:
+    cap = FRAMED_CAPTURES.get(shape) if config == "single" else None
+    if not cap or not cap["l2_bytes"]:
         return None
-    return {"kernel": "elastic_step<RZ=2, CORE> adjoint", "l1_to_l2_bytes_per_launch": ADJ_CORE_L2_BYTES,
-            "achieved_gbs": ADJ_CORE_L2_BYTES / (ADJ_CORE_COLD_US * 1e-6) / 1e9, "lts_throughput_pct": 7.0,
+    return {"kernel": cap["core"] + " adjoint", "l1_to_l2_bytes_per_launch": cap["l2_bytes"],
+            "achieved_gbs": cap["l2_bytes"] / (cap["core_cold_us"] * 1e-6) / 1e9, "lts_throughput_pct": cap["lts_pct"],
             "source": "ncu capture, cold caches (profiles/elastic_step_framed_single_shot_401x801.md)"}
 
 
