@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-ae", action="store_true")
     return ap.parse_args()
 
 
@@ -576,6 +577,11 @@ def run_ours(args):
                 line["large"] = run_large(local)
             except Exception as e:   # the large-grid leg never blocks the main line
                 line["large"] = {"error": str(e)}
+        if world == 1 and args.config == "single" and not args.no_ae:
+            try:
+                line["acoustic_elastic"] = run_ae(local)
+            except Exception as e:   # the acoustic-elastic leg never blocks the main line
+                line["acoustic_elastic"] = {"error": str(e)}
         if world == 1 and args.config == "single":
             try:
                 rg = reference_gpu_sample(wl)
@@ -679,6 +685,82 @@ def run_batched(local, steps, warmup):
 # cells x 32 rows), pinned so that the bench does not rerun the tuner's
 # whole-pass stage, whose passes take tens of seconds on this grid
 LARGE_TILE_SHAPE = 8
+
+
+def run_ae(local, nshots=8):
+    """FWI gradients of the acoustic-elastic configuration at full size (601 x
+    1601 cells at 5 m: 41 fluid rows over 561 elastic rows, nt = 6001, FP32
+    snapshots), nshots of its 96 shots in one plan on one GPU (in waves: one
+    shot's snapshots take 44 GB); returns a dict with the time of one gradient
+    of 96 shots and of 20 L-BFGS iterations projected from it (lower bound)."""
+    import ctypes
+    import torch
+    import fwi2d_b200 as F
+    from fwi2d_b200 import _capi as C
+    from fwi2d_b200 import workloads as W
+    wl = W.ae_fwi(nshots=96)
+    pick = np.linspace(0, 95, nshots).round().astype(int)
+    nt, d, oz = wl["nt"], wl["d"], wl["oz"]
+    prm = dict(wl["params"])
+
+    def shots():
+        return [F.ShotSpec(0, wl["nx"], nt, [0.0], [oz], wl["rx"], wl["rz"], water_src_x=[float(wl["sx"][k])],
+                           water_src_z=[float(wl["sz"][k])], water_rcv_x=wl["rx"], water_rcv_z=wl["rzw"])
+                for k in pick]
+    src = np.ascontiguousarray(wl["src"].reshape(1, 1, nt))
+    srcs = [src] * nshots
+    # observed data: the true model's forward, as particle velocity / -d(potential)/dt (seismotype 1)
+    Q = F.Propagator(local)
+    Q.set_model(C.ACOUSTIC_ELASTIC, W.convert(C.ELASTIC, wl["true"]), d, d, 0.0, oz)
+    Q.set_shots(F.make_params(**dict(prm, sub=0)), shots())
+    raw = Q.forward(srcs, store=False)
+    Q.close()
+    obs = []
+    for u in raw:
+        v = np.empty_like(u)
+        v[..., 0] = (u[..., 1] - u[..., 0]) / np.float32(wl["dt"])
+        v[..., -1] = (u[..., -1] - u[..., -2]) / np.float32(wl["dt"])
+        v[..., 1:-1] = (u[..., 2:] - u[..., :-2]) / np.float32(2 * wl["dt"])
+        v[0] = -v[0]
+        obs.append(v.astype(np.float32))
+    P = F.Propagator(local)
+    P.set_model(C.ACOUSTIC_ELASTIC, W.convert(C.ELASTIC, wl["start"]), d, d, 0.0, oz)
+    P.set_shots(F.make_params(**prm), shots())
+    stream = torch.cuda.Stream()
+    P.set_stream(stream.cuda_stream)
+    P.set_observed(obs)
+    P.upload(srcs, adjoint=False)
+    L = F.load()
+    mis = ctypes.c_double(0.0)
+
+    def step():
+        C.check(L.fwi2d_fwi_gradient(P.h, None, None, None, 1, None, ctypes.byref(mis)))
+    with torch.cuda.stream(stream):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        step()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    fwd_ms, adj_ms = P.last_timing()
+    info = P.plan_info()
+    nwaves, snap_all = P.plan_waves()
+    P.close()
+    cells = nshots * 2 * (nt - 1) * wl["nx"] * (wl["nz"] + wl["nza"])
+    per96 = ms * 96 / nshots / 1e3
+    return {"workload": "acoustic-elastic FWI gradient, %d of the 96 shots of the 601 x 1601 model at 5 m (41 fluid "
+                        "rows over 561 elastic rows), nt = %d, FP32 snapshots" % (nshots, nt),
+            "shots": nshots, "ms_per_step": ms, "shots_per_s": nshots / (ms / 1e3),
+            "value": cells / (ms / 1e3) / 1e9, "unit": "Gcell-updates/s (fluid and elastic cells)",
+            "cell_updates_per_step": cells, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
+            "tile_shape": info["tile_shape"], "waves": nwaves, "snapshot_bytes_all_shots": snap_all,
+            "misfit": mis.value, "projected_96_shot_gradient_s": per96,
+            "projected_20_lbfgs_iterations_s": per96 * 21,
+            "projection": "20 L-BFGS iterations at one gradient evaluation each plus the initial one (a lower "
+                          "bound: every further line-search trial adds one evaluation)"}
 
 
 def run_large(local, nshots=4):
