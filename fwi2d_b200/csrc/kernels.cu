@@ -142,7 +142,9 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 // Dz(lambda ux_x)), the top edge is the fluid interface (traction-free SAT,
 // applied after the other sides), and the interface row of uz is left
 // untapered, with its prev saved in halo_save, for ae_couple.  No imaging
-// term at snapshot 0.  General path only.
+// term at snapshot 0.  Windows clear of the bands take the scalar interior
+// path with the same split; the others, the interface row among them, the
+// general path.
 // Resident CTAs per SM asked of the compiler for the 32 x 8 tiles (a cap of
 // 51 registers a thread): the kernel is latency-bound, and five resident
 // tiles instead of four cut its single-shot time by about 20 % on B200.
@@ -201,7 +203,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     // one cell per thread: tiles clear of the boundary bands take the scalar
     // interior forms (no closure code, which keeps the hot loop small); a
     // thread whose cell the tile does not own computes nothing in phase 3
-    const bool lean1 = CORE ? RZ == 1 : (!AE && RZ == 1 && interior);
+    const bool lean1 = CORE ? RZ == 1 : (RZ == 1 && interior);
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];              // prev in, next out
@@ -225,7 +227,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
     // rho; for the imaging condition the neighbouring snapshots, the gradient
     // and the VTI coefficients) so that their latency overlaps phases 1 and 2;
     // each thread waits for its own copies in phase 3
-    if (RZ == 1 && !AE && lean1) {
+    if (RZ == 1 && lean1) {
         const int gx = wx0 + (int)(threadIdx.x >> 5), gz = wz0 + (int)(threadIdx.x & 31);
         if (gx >= tr.ox0 && gx < tr.ox1 && gz >= tr.oz0 && gz < tr.oz1) {
             float *own = OWN + threadIdx.x;
@@ -392,7 +394,10 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
             const float ux_x = d1i(U0 + ui, UZ, C.sdx);
             const float uz_z = d1i(U1 + ui, 1, C.sdz);
             float t0, t1 = 0.f;
-            if (!VTI) {
+            if (AE) {
+                t0 = ux_x;
+                t1 = uz_z;
+            } else if (!VTI) {
                 t0 = ux_x + uz_z;
             } else {
                 const long long o = mofs + (long long)(wx0 - 2 + sx) * mld + wz0 - 2 + sz;
@@ -401,7 +406,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
                 t1 = lam * uz_z + c13 * ux_x;
             }
             T0[i] = t0;
-            if (VTI) T1[i] = t1;
+            if (VTI || AE) T1[i] = t1;
             BX[i] = d1i(U1 + ui, UZ, C.sdx);
             CZ[i] = d1i(U0 + ui, 1, C.sdz);
         }
@@ -682,7 +687,13 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
         }
         n1 = d2i(n1, brackets(MU + wi, WZ), U1 + ui, UZ, C.inv_d2x);
         n0 = d2i(n0, brackets(MU + wi, 1), U0 + ui, 1, C.inv_d2z);
-        if (!VTI) {
+        if (AE) {
+            // the acoustic-elastic propagator's version-1 split, in the general path's order
+            n0 += md1i(T0 + wi, Q + wi, WZ, C.adx);
+            n1 += md1i(T1 + wi, Q + wi, 1, C.adz);
+            n0 += md1i(T1 + wi, Q + wi, WZ, C.adx);
+            n1 += md1i(T0 + wi, Q + wi, 1, C.adz);
+        } else if (!VTI) {
             n0 += md1i(T0 + wi, Q + wi, WZ, C.adx);
             n1 += md1i(T0 + wi, Q + wi, 1, C.adz);
         } else {
@@ -1130,7 +1141,7 @@ template <bool VTI, int RZ, int TX, bool GRAD, bool AE = false>
 static constexpr size_t elastic_smem_bytes()
 {
     constexpr int TZ = 32 * RZ, UZ = TZ + 8, UX = TX + 8, WZ = TZ + 4, WX = TX + 4;
-    constexpr int own = (RZ == 1 && !AE) ? own_slots<VTI, GRAD>() * 32 * TX : 0;   // scalar interior path
+    constexpr int own = RZ == 1 ? own_slots<VTI, GRAD>() * 32 * TX : 0;   // scalar interior path
     return sizeof(float) * (2 * UX * UZ + (5 + ((VTI || AE) ? 1 : 0) + (GRAD ? 2 : 0)) * WX * WZ + TX + own);
 }
 
