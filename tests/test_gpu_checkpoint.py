@@ -54,6 +54,9 @@ CASES = [
     (O.KIND_VTI, 4, F.SNAP_FP16, (72, 80)),
     (O.KIND_ACOUSTIC, 2, F.SNAP_FP32, (72, 80)),
     (O.KIND_ACOUSTIC, 3, F.SNAP_FP16, (72, 80)),
+    (O.KIND_ELASTIC, 14, F.SNAP_FP16, (72, 80)),     # framed plans: interior windows + frame kernels
+    (O.KIND_VTI, 14, F.SNAP_FP32, (72, 80)),
+    (O.KIND_ELASTIC, 16, F.SNAP_FP32, (72, 100)),
 ]
 
 
