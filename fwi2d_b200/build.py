@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfwi2d_b200.so")
 SOURCES = ["kernels.cu", "engine.cu", "noalloc.cu", "host_tables.cpp"]
-HEADERS = ["engine.h", "launch.h", "sbp.cuh", "march.cuh", "zband.cuh", "acoustic.cuh", "resample.cuh", "host_tables.h",
+HEADERS = ["engine.h", "launch.h", "sbp.cuh", "march.cuh", "zband.cuh", "xband.cuh", "acoustic.cuh", "resample.cuh", "host_tables.h",
            "d2_closure.inc", "../../include/fwi2d_b200.h"]
 
 NVCC_FLAGS = [

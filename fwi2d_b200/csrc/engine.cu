@@ -266,6 +266,7 @@ struct Plan {
     int tshape = 0, TZ = 32, TX = 16;   // tile shape of the tile kernel's units
     bool march = false;            // interior rows on the marching kernel
     bool framed = false;           // interior on the tile kernel's interior path, frame on the band kernels
+    bool band_split = false;       // frame on the band kernels that split a cell's components over two warps
     int ishape = 0;                // framed: tile shape of the interior tiles
     int nth = 0, lx = 0;           // marching: threads (z window) per unit, rows per unit
     int nt_max = 0;
@@ -497,6 +498,23 @@ static const int kBand = 6;
 static const int kFramedShapes[] = {3, 2, 1, 0};
 static const int kNumFramed = sizeof(kFramedShapes) / sizeof(kFramedShapes[0]);
 
+// The band kernels of framed and marching plans come in two forms: one
+// thread per cell, or the two field components of a cell in two warps
+// (split), which halves the serial closure chain of a thread.  The frame's
+// few CTAs set the time of a step when the plan has few band windows (one
+// 401 x 801 shot on B200: forward step 18.8 -> 16.4 us, adjoint unchanged);
+// with many, the split kernels' larger CTAs take registers from the interior
+// kernel on their SMs (eight such shots: 3-6 % slower per gradient).  So the
+// split form is taken up to kSplitMaxBandWindows x-band windows (32 rows of
+// one side of one shot each); FWI2D_BAND_SPLIT=0 or 1 forces either form.
+static const int kSplitMaxBandWindows = 32;
+static bool band_split_for(int nshots, int nz)
+{
+    const char *e = std::getenv("FWI2D_BAND_SPLIT");
+    if (e && *e) return std::atoi(e) != 0;
+    return (long long)nshots * 2 * ((nz + 31) / 32) <= kSplitMaxBandWindows;
+}
+
 static int shape_count() { return elastic_tile_count() + kNumMarch + kNumFramed; }
 static bool is_march_shape(int s) { return s >= elastic_tile_count() && s < elastic_tile_count() + kNumMarch; }
 static bool is_framed_shape(int s) { return s >= elastic_tile_count() + kNumMarch && s < shape_count(); }
@@ -511,6 +529,7 @@ struct ShotUnits {
     int TX = 0, TZ = 0, tiles_x = 0, tiles_z = 0;
     int lx = 0, nseg = 0, nwin = 0;
     int ITX = 0, ITZ = 0, itiles_x = 0;   // framed: interior tile shape and tiles along x
+    int zrows = 64;                        // rows per top / bottom band unit (zband_rows)
     int itiles_z = 0, izlast = 0;          // framed: tiles along z, first row of the last (interior coordinates)
     std::vector<int> zo;           // marching: owned z starts of the core windows, plus nz - 6
     std::vector<TileRef> tiles;    // marching and framed plans: the x-band tiles
@@ -524,7 +543,7 @@ struct ShotUnits {
         if (x < kBand) return owner_tile(z, nz, TZ);
         if (x >= nx - kBand) return tiles_z + owner_tile(z, nz, TZ);
         const int nt = (int)tiles.size();
-        if (z < kBand || z >= nz - kBand) return nt + 2 * ((x - kBand) / zband_rows()) + (z < kBand ? 0 : 1);
+        if (z < kBand || z >= nz - kBand) return nt + 2 * ((x - kBand) / zrows) + (z < kBand ? 0 : 1);
         if (framed) {
             const int zi = z - kBand;
             const int kz = zi >= izlast ? itiles_z - 1 : zi / ITZ;
@@ -590,11 +609,12 @@ static bool shape_fits(int shape, int nx, int nz)
     return frame && march_threads_ok(kMarchShapes[shape - elastic_tile_count()].nth);
 }
 
-static ShotUnits make_units(int shape, int shot, int nx, int nz)
+static ShotUnits make_units(int shape, int shot, int nx, int nz, bool band_split)
 {
     ShotUnits U;
     U.nx = nx;
     U.nz = nz;
+    U.zrows = zband_rows(band_split);
     const bool framed = is_framed_shape(shape);
     const bool march = is_march_shape(shape);
     U.march = march;
@@ -626,13 +646,13 @@ static ShotUnits make_units(int shape, int shot, int nx, int nz)
             U.tiles.push_back(r);
         }
     int roff = 0;
-    for (int a = kBand; a < nx - kBand; a += zband_rows())
+    for (int a = kBand; a < nx - kBand; a += U.zrows)
         for (int side = 0; side < 2; side++) {
             BandRef b;
             b.shot = shot;
             b.unit = (int)(U.tiles.size() + U.bands.size());
             b.xb = a;
-            b.xe = std::min(a + zband_rows(), nx - kBand);
+            b.xe = std::min(a + U.zrows, nx - kBand);
             b.side = side;
             b.roff = roff;
             roff += b.xe - b.xb + 1;
@@ -1199,7 +1219,8 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         const int m0 = elastic_tile_count();
         if (!acoustic && !ae && shape_ok(m0)) {
             long long units = 0;
-            for (int s = 0; s < nshots; s++) units += (long long)make_units(m0, s, shots[s].nx, M.nz).marches.size();
+            for (int s = 0; s < nshots; s++)
+                units += (long long)make_units(m0, s, shots[s].nx, M.nz, false).marches.size();
             if (units >= 148) shape = m0;
         }
         for (int i = 0; i < elastic_tile_count() && shape < 0; i++)
@@ -1212,6 +1233,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
     P->framed = is_framed_shape(shape);
     P->tshape = P->march || P->framed ? kBandTile : shape;
     if (P->framed) P->ishape = framed_tile_shape(shape);
+    P->band_split = (P->march || P->framed) && band_split_for(nshots, M.nz);
     elastic_tile_shape(P->tshape, &P->TZ, &P->TX);
     if (P->march) {
         P->nth = kMarchShapes[shape - elastic_tile_count()].nth;
@@ -1248,7 +1270,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
         S->nx = sh.nx;
         S->nt = sh.nt;
         S->ncomp = acoustic ? 1 : 2;
-        const ShotUnits U = make_units(shape, s, sh.nx, M.nz);
+        const ShotUnits U = make_units(shape, s, sh.nx, M.nz, P->band_split);
         const int nunits = U.nunits();
         S->ntr_src = src_fluid ? sh.src_water.ntr : sh.src.ntr;
         S->ncomp_src = acoustic || src_fluid ? 1 : (p.mt ? 3 : 2);
@@ -1298,7 +1320,7 @@ static void set_shots_impl(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, 
             W->nt = sh.nt;
             W->ncomp = 1;
             W->nr = sh.rcv_water.ntr;
-            const ShotUnits UW = make_units(shape, s, sh.nx, p.nza);
+            const ShotUnits UW = make_units(shape, s, sh.nx, p.nza, P->band_split);
             int wa[2] = {0, 0}, wb[2] = {0, 0};
             build_inj(src_fluid ? sh.src_water : none, 1, wa, wb, UW, W->inj_f, W->inj_f_off, W->inj_f_roff);
             build_inj(sh.rcv_water, 1, wa, wb, UW, W->inj_a, W->inj_a_off, W->inj_a_roff);
@@ -1524,8 +1546,9 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
     CK(cudaEventRecord(ctx->fork, st));
     CK(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
     CK(cudaStreamWaitEvent(ctx->side2, ctx->fork, 0));
-    launch_elastic_xband(P.kind == KIND_VTI, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
-    launch_elastic_zband(P.kind == KIND_VTI, P.d_bands.as<BandRef>() + R.b0, R.b1 - R.b0, shots, md, P.C, it, flags,
+    launch_elastic_xband(P.kind == KIND_VTI, P.band_split, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
+    launch_elastic_zband(P.kind == KIND_VTI, P.band_split, P.d_bands.as<BandRef>() + R.b0, R.b1 - R.b0, shots, md, P.C,
+                         it, flags,
                          P.dtg, ctx->side2);
     n += 2;
     CK(cudaEventRecord(ctx->join, ctx->side));
@@ -1724,7 +1747,7 @@ static void set_shots(fwi2d_ctx *ctx, const fwi2d_params *par, int nshots, const
         const bool grad = p.sub > 0;
         std::string key = tune_build_key(ctx->device) + "/" + std::to_string(ctx->M.kind) + "/" +
                           std::to_string(ctx->M.nz) + "/" + (grad ? "g" + std::to_string(p.snapshot_precision) : "f") +
-                          "/" + std::to_string(nshots);
+                          "/" + std::to_string(nshots) + (band_split_for(nshots, ctx->M.nz) ? "/bs" : "");
         long long cells = 0;
         for (int i = 0; i < nshots; i++) {
             key += "/" + std::to_string(shots[i].nx);

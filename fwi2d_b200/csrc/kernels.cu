@@ -1027,6 +1027,7 @@ elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tile
 }  // namespace fwi2d
 #include "march.cuh"
 #include "zband.cuh"
+#include "xband.cuh"
 #include "acoustic.cuh"
 namespace fwi2d {
 
@@ -1189,11 +1190,21 @@ void elastic_tile_shape(int i, int *tz, int *tx)
     *tx = s[i][1];
 }
 
-void launch_elastic_xband(bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
-                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+void launch_elastic_xband(bool vti, bool split, const ShotDev *shots, const TileRef *tiles, int ntiles,
+                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
     if (ntiles <= 0) return;
     const bool grad = (flags & F_GRAD) != 0;
+    if (split) {
+        if (vti) {
+            if (grad) elastic_xband<true, true><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+            else elastic_xband<true, false><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        } else {
+            if (grad) elastic_xband<false, true><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+            else elastic_xband<false, false><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+        }
+        return;
+    }
     if (vti) {
         if (grad) launch_elastic_g<true, 1, 8, true, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
         else launch_elastic_g<true, 1, 8, false, false, false, true>(shots, tiles, ntiles, M, C, it, flags, dtg, st);
@@ -1260,21 +1271,29 @@ void launch_elastic_march(bool vti, const ShotDev *shots, const MarchRef *units,
     }
 }
 
-void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const ShotDev *shots, const ModelDev &M,
-                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+template <bool SPLIT>
+static void launch_zband_s(bool vti, const BandRef *units, int nunits, const ShotDev *shots, const ModelDev &M,
+                           const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
 {
-    if (nunits <= 0) return;
     const bool grad = (flags & F_GRAD) != 0;
     if (vti) {
-        if (grad) elastic_zband<true, true><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
-        else elastic_zband<true, false><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        if (grad) elastic_zband<true, true, SPLIT><<<nunits, kZbThreads, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        else elastic_zband<true, false, SPLIT><<<nunits, kZbThreads, 0, st>>>(shots, units, M, C, it, flags, dtg);
     } else {
-        if (grad) elastic_zband<false, true><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
-        else elastic_zband<false, false><<<nunits, 6 * kZbRows, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        if (grad) elastic_zband<false, true, SPLIT><<<nunits, kZbThreads, 0, st>>>(shots, units, M, C, it, flags, dtg);
+        else elastic_zband<false, false, SPLIT><<<nunits, kZbThreads, 0, st>>>(shots, units, M, C, it, flags, dtg);
     }
 }
 
-int zband_rows() { return kZbRows; }
+void launch_elastic_zband(bool vti, bool split, const BandRef *units, int nunits, const ShotDev *shots,
+                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st)
+{
+    if (nunits <= 0) return;
+    if (split) launch_zband_s<true>(vti, units, nunits, shots, M, C, it, flags, dtg, st);
+    else launch_zband_s<false>(vti, units, nunits, shots, M, C, it, flags, dtg, st);
+}
+
+int zband_rows(bool split) { return split ? kZbSplitRows : kZbRows; }
 
 // tile shapes of the acoustic kernel: (32, 16) and (32, 8), the elastic shapes 2 and 3
 bool acoustic_shape_ok(int shape) { return shape == 2 || shape == 3; }

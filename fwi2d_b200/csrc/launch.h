@@ -11,10 +11,11 @@ void upload_sbp_tables(const float *b1, const float *b2, const float *c2, const 
 
 int elastic_tile_count();
 void elastic_tile_shape(int i, int *tz, int *tx);
-// core: interior windows of a framed plan (the tile kernel's lean paths only)
-// the x-band windows (32 x 8, full height) of framed and marching plans
-void launch_elastic_xband(bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles, const ModelDev &M,
-                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+// the x-band windows (32 x 8, full height) of framed and marching plans:
+// split = true takes the band kernel that updates the two components of a
+// cell in two warps (xband.cuh), split = false the tile kernel's general path
+void launch_elastic_xband(bool vti, bool split, const ShotDev *shots, const TileRef *tiles, int ntiles,
+                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRef *tiles, int ntiles,
                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st,
                          bool core = false);
@@ -23,10 +24,11 @@ void launch_elastic_step(int shape, bool vti, const ShotDev *shots, const TileRe
 bool march_threads_ok(int nth);
 void launch_elastic_march(bool vti, const ShotDev *shots, const MarchRef *units, int nunits, int nth,
                           const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
-// top / bottom band kernel (rows clear of the x bands), zband_rows() rows per unit
-int zband_rows();
-void launch_elastic_zband(bool vti, const BandRef *units, int nunits, const ShotDev *shots, const ModelDev &M,
-                          const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
+// top / bottom band kernel (rows clear of the x bands), zband_rows(split)
+// rows per unit; split as for the x bands
+int zband_rows(bool split);
+void launch_elastic_zband(bool vti, bool split, const BandRef *units, int nunits, const ShotDev *shots,
+                          const ModelDev &M, const StepConst &C, int it, int flags, float dtg, cudaStream_t st);
 void launch_init_state(const ShotDev *shots, int nshots, const InitCell *cells, const int *off, const int *idx,
                        cudaStream_t st);
 // Receivers of the last sample and its snapshot (t_store < 0), or only the
