@@ -13,8 +13,10 @@
 // of a step on a single shot.  Each component keeps the reference's own
 // operation order (the terms of ux and of uz never mix until the density
 // term of the imaging condition, whose float sum the ux warp forms from the
-// uz warp's product, passed through shared memory).  Elastic isotropic and
-// VTI, not the acoustic-elastic propagator (which runs on tile plans).
+// uz warp's product, passed through shared memory; the ux warp also takes
+// the lambda term of the imaging condition and the uz warp the mu term).
+// Elastic isotropic and VTI, not the acoustic-elastic propagator (which runs
+// on tile plans).
 //
 // The arithmetic is the tile kernel's general path (src/cpp/we_op.cpp:667-871
 // elastic, :1640-1840 VTI, closures of src/include/spatial_operators.hpp,
@@ -42,6 +44,7 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     __shared__ float T1[VTI ? WX * WZ : 1];     // VTI: tmp_z
     __shared__ float F0[GRAD ? WX * WZ : 1], F1[GRAD ? WX * WZ : 1];
     __shared__ float XP[GRAD ? 6 * TZ : 1];     // uz warp's density-term product per cell
+    __shared__ float GD[4][GRAD ? 6 * TZ : 1];  // ux warp's first derivatives of the lambda term per cell
     __shared__ float red[NT / 32];
 
     const TileRef tr = tiles[blockIdx.x];
@@ -94,9 +97,9 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
             }
             const float *g = Sp->grad + cell;
             if (comp == 0) {
+                hg0 = g[0];
                 hg2 = g[2 * nxz];
             } else {
-                hg0 = g[0];
                 hg1 = g[nxz];
             }
         }
@@ -293,52 +296,68 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     }
 
     if (GRAD && do_grad) {
-        // density term: each component's product (the reference's float sum
-        // of the two is formed by the ux warp, in its order)
+        // The ux warp takes the lambda term, whose four first derivatives it
+        // passes to the uz warp for the mu term, and the density term, whose
+        // float sum of one product per component it forms in the reference's
+        // order from the uz warp's product; the uz warp adds the two further
+        // derivatives of the mu term.  Each value is the general path's.
         const float f = comp == 0 ? F0[wi] : F1[wi];
-        float prod = 0.f;
+        const float gw = Sp->gwt[itf];
+        const double wdt = (double)gw * 1.0 / (double)dtg;
+        const double wh = (double)gw * 0.5 * (double)dtg;
+        const long long mo = mofs + mcell;
+        const int xi = c * TZ + lane;
+        float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
+        float prod = 0.f, t2 = 0.f, t3 = 0.f;
         if (owned) {
             if (itf > 0 && itf < last) prod = n * (hfp - 2 * f + hfm);
             else if (itf == 0) prod = n * (hfp - f);
             else prod = n * (-f + hfm);
-        }
-        if (comp == 1) XP[c * TZ + lane] = prod;
-        __syncthreads();
-        if (owned) {
-            const float gw = Sp->gwt[itf];
-            const double wdt = (double)gw * 1.0 / (double)dtg;
-            float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
             if (comp == 0) {
-                *g2 = (float)((double)hg2 + wdt * (double)(prod + XP[c * TZ + lane]));
-            } else {
                 const float ax0 = d1(U0 + ui, UZ, gx, nx, C.dx, C.sdx);
                 const float az1 = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
                 const float t0 = d1(F0 + wi, WZ, gx, nx, C.dx, C.sdx);
                 const float t1 = d1(F1 + wi, 1, gz, nz, C.dz, C.sdz);
-                const float t2 = d1(F1 + wi, WZ, gx, nx, C.dx, C.sdx);
-                const float t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
-                const float az0 = CZ[wi], ax1 = BX[wi];
-                float dl, dm;
-                if (!VTI) {
-                    dl = 0.f;
-                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
-                } else {
-                    const long long mo = mofs + mcell;
+                GD[0][xi] = ax0;
+                GD[1][xi] = az1;
+                GD[2][xi] = t0;
+                GD[3][xi] = t1;
+                float dl = 0.f;
+                if (VTI) {
                     const float e2 = 1 + 2 * M.eps[mo];
-                    const float v2 = M.gv2[mo], v3 = M.gv3[mo];
+                    const float v2 = M.gv2[mo];
                     dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
-                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
                 }
                 if (itf == 0) {
-                    const double wh = (double)gw * 0.5 * (double)dtg;
                     if (!VTI) *g0 = (float)((double)hg0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
                     else *g0 = (float)((double)hg0 + wh * (double)dl);
-                    *g1 = (float)((double)hg1 + wh * (double)dm);
                 } else {
                     if (!VTI) *g0 = hg0 + gw * dtg * (ax0 + az1) * (t0 + t1);
                     else *g0 = hg0 + gw * dtg * dl;
-                    *g1 = hg1 + gw * dtg * dm;
                 }
+            } else {
+                XP[xi] = prod;
+                t2 = d1(F1 + wi, WZ, gx, nx, C.dx, C.sdx);
+                t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
+            }
+        }
+        __syncthreads();
+        if (owned) {
+            if (comp == 0) {
+                *g2 = (float)((double)hg2 + wdt * (double)(prod + XP[xi]));
+            } else {
+                const float ax0 = GD[0][xi], az1 = GD[1][xi], t0 = GD[2][xi], t1 = GD[3][xi];
+                const float az0 = CZ[wi], ax1 = BX[wi];
+                float dm;
+                if (!VTI) {
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
+                } else {
+                    const float e2 = 1 + 2 * M.eps[mo];
+                    const float v3 = M.gv3[mo];
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
+                }
+                if (itf == 0) *g1 = (float)((double)hg1 + wh * (double)dm);
+                else *g1 = hg1 + gw * dtg * dm;
             }
         }
     }

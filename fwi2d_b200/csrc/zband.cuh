@@ -15,7 +15,8 @@
 //     of many shots keep SPLIT = false.  Each component keeps the
 //     reference's operation order; the density term of the imaging
 //     condition, which sums one product of each component, is formed by the
-//     ux warp from the uz warp's product passed through shared memory.
+//     ux warp from the uz warp's product passed through shared memory, and
+//     the ux warp takes the lambda term and the uz warp the mu term.
 // Every lane of a warp sits on the same closure row (the same k) and the
 // same component, so the SBP closure coefficients are uniform reads and no
 // lane diverges.  The arithmetic is the tile kernel's general path
@@ -44,6 +45,7 @@ elastic_zband(const ShotDev *__restrict__ shots, const BandRef *__restrict__ uni
     __shared__ float BX[XB * ZW], T1[VTI ? XB * ZW : 1];    // uz_x; VTI: lambda uz_z + c13 ux_x (own rows)
     __shared__ float F0[GRAD ? NR2 * ZW : 1], F1[GRAD ? NR2 * ZW : 1];
     __shared__ float XP[GRAD && SPLIT ? 6 * XB : 1];        // uz warp's density-term product per cell
+    __shared__ float GD[4][GRAD && SPLIT ? 6 * XB : 1];     // ux warp's first derivatives of the lambda term
     __shared__ float red[NT / 32];
 
     const BandRef U = units[blockIdx.x];
@@ -229,9 +231,17 @@ elastic_zband(const ShotDev *__restrict__ shots, const BandRef *__restrict__ uni
             }
         }
         if (GRAD && do_grad) {
-            // density term: each component's product; the ux warp forms their
-            // float sum in the reference's order
-            float prod = 0.f;
+            // The ux warp takes the lambda term, whose four first derivatives
+            // it passes to the uz warp for the mu term, and the density term,
+            // whose float sum of one product per component it forms in the
+            // reference's order from the uz warp's product; the uz warp adds
+            // the two further derivatives of the mu term.
+            const float gw = Sp->gwt[itf];
+            const double wdt = (double)gw * 1.0 / (double)dtg;
+            const double wh = (double)gw * 0.5 * (double)dtg;
+            const int xi = k * XB + tr;
+            float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
+            float prod = 0.f, t2 = 0.f, t3 = 0.f;
             if (owned) {
                 const float f = comp == 0 ? F0[wi] : F1[wi];
                 float fp = 0.f, fm = 0.f;
@@ -246,43 +256,51 @@ elastic_zband(const ShotDev *__restrict__ shots, const BandRef *__restrict__ uni
                 if (itf > 0 && itf < last) prod = n * (fp - 2 * f + fm);
                 else if (itf == 0) prod = n * (fp - f);
                 else prod = n * (-f + fm);
-            }
-            if (comp == 1) XP[k * XB + tr] = prod;
-            __syncthreads();
-            if (owned) {
-                const float gw = Sp->gwt[itf];
-                const double wdt = (double)gw * 1.0 / (double)dtg;
-                float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
                 if (comp == 0) {
-                    *g2 = (float)((double)*g2 + wdt * (double)(prod + XP[k * XB + tr]));
-                } else {
-                    const double wh = (double)gw * 0.5 * (double)dtg;
                     const float ax0 = d1(U0 + ui, ZW, gx, nx, C.dx, C.sdx);
                     const float az1 = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
                     const float t0 = d1(F0 + wi, ZW, gx, nx, C.dx, C.sdx);
                     const float t1 = d1(F1 + wi, 1, gz, nz, C.dz, C.sdz);
-                    const float t2 = d1(F1 + wi, ZW, gx, nx, C.dx, C.sdx);
-                    const float t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
-                    const float az0 = CZ[wi], ax1 = BX[bi];
-                    float dl, dm;
-                    if (!VTI) {
-                        dl = 0.f;
-                        dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
-                    } else {
+                    GD[0][xi] = ax0;
+                    GD[1][xi] = az1;
+                    GD[2][xi] = t0;
+                    GD[3][xi] = t1;
+                    float dl = 0.f;
+                    if (VTI) {
                         const float e2 = 1 + 2 * M.eps[mcell];
-                        const float v2 = M.gv2[mcell], v3 = M.gv3[mcell];
+                        const float v2 = M.gv2[mcell];
                         dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
-                        dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
                     }
                     if (itf == 0) {
                         if (!VTI) *g0 = (float)((double)*g0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
                         else *g0 = (float)((double)*g0 + wh * (double)dl);
-                        *g1 = (float)((double)*g1 + wh * (double)dm);
                     } else {
                         if (!VTI) *g0 = *g0 + gw * dtg * (ax0 + az1) * (t0 + t1);
                         else *g0 = *g0 + gw * dtg * dl;
-                        *g1 = *g1 + gw * dtg * dm;
                     }
+                } else {
+                    XP[xi] = prod;
+                    t2 = d1(F1 + wi, ZW, gx, nx, C.dx, C.sdx);
+                    t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
+                }
+            }
+            __syncthreads();
+            if (owned) {
+                if (comp == 0) {
+                    *g2 = (float)((double)*g2 + wdt * (double)(prod + XP[xi]));
+                } else {
+                    const float ax0 = GD[0][xi], az1 = GD[1][xi], t0 = GD[2][xi], t1 = GD[3][xi];
+                    const float az0 = CZ[wi], ax1 = BX[bi];
+                    float dm;
+                    if (!VTI) {
+                        dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
+                    } else {
+                        const float e2 = 1 + 2 * M.eps[mcell];
+                        const float v3 = M.gv3[mcell];
+                        dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
+                    }
+                    if (itf == 0) *g1 = (float)((double)*g1 + wh * (double)dm);
+                    else *g1 = *g1 + gw * dtg * dm;
                 }
             }
         }
