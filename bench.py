@@ -85,23 +85,27 @@ def peaks():
 # dram__bytes_write.sum) of the core, x-band and z-band launches of one
 # adjoint step, and the core launch's L1-to-L2 bytes, cold duration and L2
 # throughput, from the captures summarised in
-# profiles/elastic_step_framed_single_shot_401x801.md (cold caches: ncu
-# flushes L2 before each pass).
+# profiles/elastic_step_framed_single_shot_401x801.md and, for the split band
+# kernels that one shot takes, profiles/elastic_band_split_single_shot_401x801.md
+# (cold caches: ncu flushes L2 before each pass).
 FRAMED_CAPTURES = {
     16: dict(core="elastic_step<RZ=2, CORE> (64 x 8 z-pair windows)",
              traffic={"core": 21.133312e6, "x_bands": 0.554496e6, "z_bands": 3.61984e6},
              l2_bytes=1447280 * 32, core_cold_us=28.576, lts_pct=7.0),
     14: dict(core="elastic_step<RZ=1, CORE> (32 x 8 windows)",
-             traffic={"core": 21.152256e6, "x_bands": 0.534016e6, "z_bands": 3.607808e6},
+             traffic={"core": 21.152256e6, "x_bands": 0.499712e6, "z_bands": 3.606528e6},
              l2_bytes=1651721 * 32, core_cold_us=21.312, lts_pct=10.4),
+    15: dict(core="elastic_step<RZ=1, CORE> (32 x 16 windows)",
+             traffic={"core": 21.128704e6, "x_bands": 0.498688e6, "z_bands": 3.606784e6},
+             l2_bytes=1548000 * 32, core_cold_us=25.95, lts_pct=8.1),
 }
 
 
 def roof_kernel(shape, config):
     if config == "single" and shape in FRAMED_CAPTURES:
-        return ("adjoint + imaging step of the framed plan: interior %s with the x-band elastic_step and "
-                "elastic_zband overlapped on two side streams (one step = one launch of each)"
-                % FRAMED_CAPTURES[shape]["core"])
+        return ("adjoint + imaging step of the framed plan: interior %s with the band kernels elastic_xband and "
+                "elastic_zband<SPLIT> (a cell's two components in two warps) overlapped on two side streams "
+                "(one step = one launch of each)" % FRAMED_CAPTURES[shape]["core"])
     if config == "single":
         return "adjoint + imaging step (tile shape %d)" % shape
     return "adjoint loop: interior, band and imaging kernels"
@@ -124,7 +128,8 @@ def l2_note(shape, config):
         return None
     return {"kernel": cap["core"] + " adjoint", "l1_to_l2_bytes_per_launch": cap["l2_bytes"],
             "achieved_gbs": cap["l2_bytes"] / (cap["core_cold_us"] * 1e-6) / 1e9, "lts_throughput_pct": cap["lts_pct"],
-            "source": "ncu capture, cold caches (profiles/elastic_step_framed_single_shot_401x801.md)"}
+            "source": "ncu capture, cold caches (profiles/elastic_step_framed_single_shot_401x801.md, "
+                      "profiles/elastic_band_split_single_shot_401x801.md)"}
 
 
 # ---------------------------------------------------------------------------
