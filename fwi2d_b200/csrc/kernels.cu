@@ -1196,12 +1196,13 @@ void launch_elastic_xband(bool vti, bool split, const ShotDev *shots, const Tile
     if (ntiles <= 0) return;
     const bool grad = (flags & F_GRAD) != 0;
     if (split) {
+        constexpr int nf = xband_threads<false>(), ng = xband_threads<true>();
         if (vti) {
-            if (grad) elastic_xband<true, true><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
-            else elastic_xband<true, false><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+            if (grad) elastic_xband<true, true><<<ntiles, ng, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+            else elastic_xband<true, false><<<ntiles, nf, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
         } else {
-            if (grad) elastic_xband<false, true><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
-            else elastic_xband<false, false><<<ntiles, kXbThreads, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+            if (grad) elastic_xband<false, true><<<ntiles, ng, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
+            else elastic_xband<false, false><<<ntiles, nf, 0, st>>>(shots, tiles, M, C, it, flags, dtg);
         }
         return;
     }

@@ -6,15 +6,16 @@
 // columns next to them, owned cells [ox0, ox1) x [oz0, oz1)).  The window is
 // staged and differentiated as in the tile kernel's general path.  The two
 // field components of a cell are then updated by two different warps: warps
-// 0-5 take ux of columns 0-5 of the band, warps 6-11 take uz.  Every one of
-// these cells sits in the x closure of the SBP operators, so the stencil
-// arithmetic of one cell is long and serial; two warps per cell halve the
-// instruction chain that sets the band's time, and the band sets the time
-// of a step on a single shot.  Each component keeps the reference's own
-// operation order (the terms of ux and of uz never mix until the density
-// term of the imaging condition, whose float sum the ux warp forms from the
-// uz warp's product, passed through shared memory; the ux warp also takes
-// the lambda term of the imaging condition and the uz warp the mu term).
+// 0-5 take ux of columns 0-5 of the band, warps 6-11 take uz; in the adjoint,
+// warps 12-17 take the lambda and mu terms of the imaging condition, which
+// need first derivatives only.  Every one of these cells sits in the x
+// closure of the SBP operators, so the arithmetic of one cell is long and
+// serial; spreading it over warps shortens the instruction chain that sets
+// the band's time, and the band sets the time of a step on a single shot.
+// Each component keeps the reference's own operation order (the terms of ux
+// and of uz never mix until the density term of the imaging condition,
+// whose float sum the ux warp forms from the uz warp's product, passed
+// through shared memory behind a barrier of those two warp groups only).
 // Elastic isotropic and VTI, not the acoustic-elastic propagator (which runs
 // on tile plans).
 //
@@ -26,16 +27,18 @@
 
 namespace fwi2d {
 
-constexpr int kXbThreads = 384;   // 2 components x 6 band columns x 32 z cells
+// threads per CTA: 2 components (and, in the adjoint, the imaging terms) x 6 band columns x 32 z cells
+template <bool GRAD>
+__host__ __device__ constexpr int xband_threads() { return GRAD ? 576 : 384; }
 
 template <bool VTI, bool GRAD>
-__global__ void __launch_bounds__(kXbThreads, 1)
+__global__ void __launch_bounds__(xband_threads<GRAD>(), 1)
 elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C, int it,
               int flags, float dtg)
 {
     constexpr int TZ = 32, TX = 8;
     constexpr int UZ = TZ + 8, UX = TX + 8, WZ = TZ + 4, WX = TX + 4;
-    constexpr int NT = kXbThreads;
+    constexpr int NT = xband_threads<GRAD>();
     __shared__ __align__(16) float U0[UX * UZ];
     __shared__ __align__(16) float U1[UX * UZ];
     __shared__ float MU[WX * WZ], Q[WX * WZ];   // mu; lambda (iso) or (1+2eps)2mu (VTI)
@@ -44,7 +47,6 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     __shared__ float T1[VTI ? WX * WZ : 1];     // VTI: tmp_z
     __shared__ float F0[GRAD ? WX * WZ : 1], F1[GRAD ? WX * WZ : 1];
     __shared__ float XP[GRAD ? 6 * TZ : 1];     // uz warp's density-term product per cell
-    __shared__ float GD[4][GRAD ? 6 * TZ : 1];  // ux warp's first derivatives of the lambda term per cell
     __shared__ float red[NT / 32];
 
     const TileRef tr = tiles[blockIdx.x];
@@ -55,7 +57,8 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     const int nxz = nx * ldz;
     const int wx0 = tr.wx0, wz0 = tr.wz0;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int comp = warp / 6, c = warp - 6 * comp;
+    const int comp = warp / 6, c = warp - 6 * comp;   // comp 0: ux, 1: uz, 2: imaging terms (adjoint)
+    const bool stencil = comp < 2;
 
     const float *__restrict__ curr = Sp->u[(it + 1) & 1];
     float *__restrict__ pn = Sp->u[it & 1];   // prev in, next out
@@ -81,7 +84,7 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     const int cell = gx * ldz + gz, mcell = gx * mld + gz;
     float p = 0.f, rho = 1.f, tzv = 0.f, txv = 0.f;
     float hfp = 0.f, hfm = 0.f, hg0 = 0.f, hg1 = 0.f, hg2 = 0.f;
-    if (owned) {
+    if (owned && stencil) {
         p = pn[comp * nxz + cell];
         rho = mp2[mcell];
         tzv = Sp->tz[gz];
@@ -95,14 +98,12 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
                 const float inv = prec == SNAP_FP32 ? 1.f : 1.f / snap_scale(Sp->snap_amax, itf - 1);
                 hfm = snap_load(snap, (long long)(itf - 1) * slot_elems + comp * nxz + cell, prec, inv);
             }
-            const float *g = Sp->grad + cell;
-            if (comp == 0) {
-                hg0 = g[0];
-                hg2 = g[2 * nxz];
-            } else {
-                hg1 = g[nxz];
-            }
+            if (comp == 0) hg2 = Sp->grad[cell + 2 * (long long)nxz];
         }
+    }
+    if (GRAD && do_grad && owned && comp == 2) {
+        hg0 = Sp->grad[cell];
+        hg1 = Sp->grad[cell + (long long)nxz];
     }
     float finv = 1.f;
     if (GRAD && do_grad && prec != SNAP_FP32) finv = 1.f / snap_scale(Sp->snap_amax, itf);
@@ -198,7 +199,7 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     const int wi = (tx + 2) * WZ + (lane + 2);
     const float *Uc = comp == 0 ? U0 : U1;
     float n = 0.f, amax = 0.f;
-    if (owned) {
+    if (owned && stencil) {
         const bool store = (flags & F_STORE) && (it % C.sub == 0);
         if (store) {
             const int slot = it / C.sub;
@@ -296,68 +297,57 @@ elastic_xband(const ShotDev *__restrict__ shots, const TileRef *__restrict__ til
     }
 
     if (GRAD && do_grad) {
-        // The ux warp takes the lambda term, whose four first derivatives it
-        // passes to the uz warp for the mu term, and the density term, whose
-        // float sum of one product per component it forms in the reference's
-        // order from the uz warp's product; the uz warp adds the two further
-        // derivatives of the mu term.  Each value is the general path's.
-        const float f = comp == 0 ? F0[wi] : F1[wi];
-        const float gw = Sp->gwt[itf];
-        const double wdt = (double)gw * 1.0 / (double)dtg;
-        const double wh = (double)gw * 0.5 * (double)dtg;
-        const long long mo = mofs + mcell;
-        const int xi = c * TZ + lane;
         float *g0 = Sp->grad + cell, *g1 = g0 + nxz, *g2 = g1 + nxz;
-        float prod = 0.f, t2 = 0.f, t3 = 0.f;
-        if (owned) {
-            if (itf > 0 && itf < last) prod = n * (hfp - 2 * f + hfm);
-            else if (itf == 0) prod = n * (hfp - f);
-            else prod = n * (-f + hfm);
-            if (comp == 0) {
+        const float gw = Sp->gwt[itf];
+        if (comp == 2) {
+            // lambda and mu terms: first derivatives of curr and of the snapshot
+            if (owned) {
                 const float ax0 = d1(U0 + ui, UZ, gx, nx, C.dx, C.sdx);
                 const float az1 = d1(U1 + ui, 1, gz, nz, C.dz, C.sdz);
                 const float t0 = d1(F0 + wi, WZ, gx, nx, C.dx, C.sdx);
                 const float t1 = d1(F1 + wi, 1, gz, nz, C.dz, C.sdz);
-                GD[0][xi] = ax0;
-                GD[1][xi] = az1;
-                GD[2][xi] = t0;
-                GD[3][xi] = t1;
-                float dl = 0.f;
-                if (VTI) {
+                const float t2 = d1(F1 + wi, WZ, gx, nx, C.dx, C.sdx);
+                const float t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
+                const float az0 = CZ[wi], ax1 = BX[wi];
+                float dl, dm;
+                if (!VTI) {
+                    dl = 0.f;
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
+                } else {
+                    const long long mo = mofs + mcell;
                     const float e2 = 1 + 2 * M.eps[mo];
-                    const float v2 = M.gv2[mo];
+                    const float v2 = M.gv2[mo], v3 = M.gv3[mo];
                     dl = e2 * ax0 * t0 + az1 * t1 + v2 * (ax0 * t1 + az1 * t0);
+                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
                 }
                 if (itf == 0) {
+                    const double wh = (double)gw * 0.5 * (double)dtg;
                     if (!VTI) *g0 = (float)((double)hg0 + wh * (double)(ax0 + az1) * (double)(t0 + t1));
                     else *g0 = (float)((double)hg0 + wh * (double)dl);
+                    *g1 = (float)((double)hg1 + wh * (double)dm);
                 } else {
                     if (!VTI) *g0 = hg0 + gw * dtg * (ax0 + az1) * (t0 + t1);
                     else *g0 = hg0 + gw * dtg * dl;
+                    *g1 = hg1 + gw * dtg * dm;
                 }
-            } else {
-                XP[xi] = prod;
-                t2 = d1(F1 + wi, WZ, gx, nx, C.dx, C.sdx);
-                t3 = d1(F0 + wi, 1, gz, nz, C.dz, C.sdz);
             }
-        }
-        __syncthreads();
-        if (owned) {
-            if (comp == 0) {
+        } else {
+            // density term: each component's product; the ux warp forms their
+            // float sum in the reference's order, behind a barrier of the 12
+            // stencil warps only (named barrier 1)
+            float prod = 0.f;
+            if (owned) {
+                const float f = comp == 0 ? F0[wi] : F1[wi];
+                if (itf > 0 && itf < last) prod = n * (hfp - 2 * f + hfm);
+                else if (itf == 0) prod = n * (hfp - f);
+                else prod = n * (-f + hfm);
+            }
+            const int xi = c * TZ + lane;
+            if (comp == 1) XP[xi] = prod;
+            asm volatile("bar.sync 1, 384;" ::: "memory");
+            if (owned && comp == 0) {
+                const double wdt = (double)gw * 1.0 / (double)dtg;
                 *g2 = (float)((double)hg2 + wdt * (double)(prod + XP[xi]));
-            } else {
-                const float ax0 = GD[0][xi], az1 = GD[1][xi], t0 = GD[2][xi], t1 = GD[3][xi];
-                const float az0 = CZ[wi], ax1 = BX[wi];
-                float dm;
-                if (!VTI) {
-                    dm = (az0 + ax1) * (t2 + t3) + 2 * ax0 * t0 + 2 * az1 * t1;
-                } else {
-                    const float e2 = 1 + 2 * M.eps[mo];
-                    const float v3 = M.gv3[mo];
-                    dm = (az0 + ax1) * (t2 + t3) + 2 * e2 * ax0 * t0 + 2 * az1 * t1 + v3 * (ax0 * t1 + az1 * t0);
-                }
-                if (itf == 0) *g1 = (float)((double)hg1 + wh * (double)dm);
-                else *g1 = hg1 + gw * dtg * dm;
             }
         }
     }
