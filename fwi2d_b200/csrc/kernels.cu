@@ -165,6 +165,12 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 #ifndef CORE1_MIN_BLOCKS
 #define CORE1_MIN_BLOCKS 6
 #endif
+// resident CTAs per SM asked for the scalar (RZ = 1) 32 x 16 interior windows:
+// two (64 registers).  Three (40 registers) took the single-shot adjoint 8 %
+// slower on B200, and on 8-shot plans the 32 x 8 windows stayed ahead.
+#ifndef CORE16_MIN_BLOCKS
+#define CORE16_MIN_BLOCKS 2
+#endif
 // BAND: the instantiation for the full-height x-band windows of framed and
 // marching plans.  Few CTAs run it and it sets the step's critical path, so
 // it is compiled without the occupancy bound (no register spills) and, in
@@ -174,7 +180,7 @@ template <bool VTI, int RZ, int TX, bool GRAD, bool AE, bool CORE = false, bool 
 __global__ void __launch_bounds__(32 * TX, BAND ? 1
                                                : (TX == 8 ? (RZ == 1 ? (CORE ? CORE1_MIN_BLOCKS : TILE_MIN_BLOCKS)
                                                                      : (CORE ? CORE_MIN_BLOCKS : 1))
-                                                          : (CORE && RZ == 1 ? 2 : 1)))
+                                                          : (CORE && RZ == 1 ? CORE16_MIN_BLOCKS : 1)))
 elastic_step(const ShotDev *__restrict__ shots, const TileRef *__restrict__ tiles, ModelDev M, StepConst C,
              int it, int flags, float dtg)
 {
