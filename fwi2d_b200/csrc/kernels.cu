@@ -172,8 +172,10 @@ __device__ __forceinline__ float2 snap_load2(const void *base, long long idx, in
 #define CORE16_MIN_BLOCKS 2
 #endif
 // BAND: the instantiation for the full-height x-band windows of framed and
-// marching plans.  Few CTAs run it and it sets the step's critical path, so
-// it is compiled without the occupancy bound (no register spills) and, in
+// marching plans with many band windows (one thread per cell; plans with few
+// take elastic_xband, which splits a cell's components over two warps).  It
+// runs on few CTAs beside the interior, so it is compiled without the
+// occupancy bound (no register spills) and, in
 // the imaging condition, loads its snapshot and gradient operands before the
 // stencil arithmetic so that their latency overlaps it.
 template <bool VTI, int RZ, int TX, bool GRAD, bool AE, bool CORE = false, bool BAND = false>
