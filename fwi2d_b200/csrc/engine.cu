@@ -502,7 +502,8 @@ static const int kNumFramed = sizeof(kFramedShapes) / sizeof(kFramedShapes[0]);
 // thread per cell, or the two field components of a cell in two warps
 // (split), which halves the serial closure chain of a thread.  The frame's
 // few CTAs set the time of a step when the plan has few band windows (one
-// 401 x 801 shot on B200: forward step 18.8 -> 16.4 us, adjoint unchanged);
+// 401 x 801 shot on B200, same interior shape: forward 17 % and adjoint 4 %
+// faster);
 // with many, the split kernels' larger CTAs take registers from the interior
 // kernel on their SMs (eight such shots: 3-6 % slower per gradient).  So the
 // split form is taken up to kSplitMaxBandWindows x-band windows (32 rows of
@@ -1548,8 +1549,7 @@ static int launch_step(fwi2d_ctx *ctx, const Plan &P, const ShotDev *shots, cons
     CK(cudaStreamWaitEvent(ctx->side2, ctx->fork, 0));
     launch_elastic_xband(P.kind == KIND_VTI, P.band_split, shots, tiles, ntiles, md, P.C, it, flags, P.dtg, ctx->side);
     launch_elastic_zband(P.kind == KIND_VTI, P.band_split, P.d_bands.as<BandRef>() + R.b0, R.b1 - R.b0, shots, md, P.C,
-                         it, flags,
-                         P.dtg, ctx->side2);
+                         it, flags, P.dtg, ctx->side2);
     n += 2;
     CK(cudaEventRecord(ctx->join, ctx->side));
     CK(cudaEventRecord(ctx->join2, ctx->side2));
